@@ -1,0 +1,362 @@
+#!/usr/bin/env python
+"""Benchmark: plain forward TTI elastic RSG modelling on one B200 per rank.
+
+Workload (the demo shape of the reference, seeded synthetic salt-like model):
+nz=1126 nx=7872 dx=dz=10 m, ealThick=60 (E=65, padded grid 1256 x 8002 =
+10,050,512 cells), free surface, one 12 Hz Ricker source at the surface centre,
+7872 receivers at z=2, dt=0.8 ms. A "step" is one time step (velocity and
+stress half-steps over the padded grid); the metric is Gcell-updates/s over
+the padded grid (Nz * Nx per step), summed over ranks (one shot per GPU, weak
+scaling, no collective on the data path).
+
+Arms:
+  default            the CUDA library through the C ABI (inputs resident in HBM
+                     for `value`; host buffers and the whole public-API call
+                     sequence for `e2e`)
+  --impl reference   the reference's own OpenMP C build (oracle/_ref) on the
+                     host cores, a bounded number of steps of the same workload
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "tti-fdmodeling_b200"))
+import synthetic  # noqa: E402
+
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM = 6650.0
+# Compulsory bytes per cell-update with the reference storage layout (state
+# read+written once, per-cell parameters read once).
+ALG_BYTES_STEP = {"coordinate_rotation": 84, "tensor_rotation": 104, "bond_transformation": 76}
+# Compulsory bytes per cell of each half-step kernel when the two half-steps
+# run as separate kernels (each re-reads the state the other wrote).
+ALG_BYTES_HALF = {
+    "coordinate_rotation": {"velocity": 48, "stress": 64},   # v: 3 sig + 2 v + 5 par + 2 w; s: 2 v + 3 sig + 8 par + 3 w
+    "tensor_rotation": {"velocity": 40, "stress": 88},       # s: 2 v + 3 tau + 7 par + 6 w
+    "bond_transformation": {"velocity": 40, "stress": 68},   # s: 2 v + 3 sig + 9 par + 3 w
+}
+
+WORKLOAD = dict(nz=1126, nx=7872, dx=10.0, dz=10.0, dt=0.0008, fpeak=12.0, ealThick=60, freesurface=1, stype=1,
+                seistype=3, mt=1, wsave=2, savew=0, snap_sample=1250, mode=1, scalar=1.0, energy=0)
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def peaks():
+    try:
+        d = json.load(open(MEASURED_PEAKS))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- inputs
+_MODEL = None
+
+
+def model():
+    global _MODEL
+    if _MODEL is None:
+        _MODEL = synthetic.salt_model(WORKLOAD["nz"], WORKLOAD["nx"], seed=1)
+    return _MODEL
+
+
+def geometry(rank: int):
+    nx, nt = WORKLOAD["nx"], None
+    sx = nx // 2 + 12 * rank  # one shot per rank, 120 m apart
+    gx = np.arange(nx, dtype=np.int32)
+    gz = np.full(nx, 2, np.int32)
+    return sx, 2, gx, gz
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args, rank, world, local_rank):
+    import ttifd
+
+    variant = args.variant
+    K, W = args.steps, args.warmup
+    m = model()
+    pads = synthetic.padded(m, WORKLOAD["ealThick"])
+    sx, sz, gx, gz = geometry(rank)
+    cfg = dict(WORKLOAD, variant=variant, nt=W + K + args.profile_steps)
+    wav = synthetic.ricker(cfg["nt"], cfg["dt"], cfg["fpeak"])
+    h = ttifd.Modeling(device=local_rank, **cfg)
+    h.upload_model(*pads)
+    h.set_source([sx], [sz], wav[None, :])
+    for k in (0, 1, 2):
+        h.set_receivers(k, gx, gz)
+    cells = h.Nz * h.Nx
+    h.reset()
+    h.step(W)
+    dist_barrier()
+    l0 = h.kernel_launches
+    with ClockSampler(local_rank) as clk:
+        h.step(K)
+        ms = h.elapsed_ms
+    launches = h.kernel_launches - l0
+    ms_max = dist_max(ms)
+    # per-phase device time (events on the library's stream)
+    pv, ps, po = h.profile_steps(args.profile_steps)
+    h.close()
+    value = cells * K * world / (ms_max / 1e3) / 1e9
+
+    # e2e: the whole public-API sequence from host buffers (pinned by the
+    # library where it stages): upload + precompute, geometry, K steps with
+    # snapshots delivered to the host, traces fetched.
+    cfg_e = dict(WORKLOAD, variant=variant, nt=K)
+    wav_e = wav[:K]
+    dist_barrier()
+    t0 = time.perf_counter()
+    with ttifd.Modeling(device=local_rank, **cfg_e) as he:
+        he.upload_model(*pads)
+        he.set_source([sx], [sz], wav_e[None, :])
+        for k in (0, 1, 2):
+            he.set_receivers(k, gx, gz)
+        snaps = []
+        he.run(lambda it, kind, a: snaps.append(a.nbytes))
+        trs = [he.fetch_traces(k) for k in (0, 1, 2)]
+    t_e2e = dist_max(time.perf_counter() - t0)
+    h2d = sum(a.nbytes for a in pads) + wav_e.nbytes + 3 * 2 * gx.nbytes
+    d2h = sum(snaps) + sum(t.nbytes for t in trs)
+    e2e = {"value": cells * K * world / t_e2e / 1e9, "unit": "Gcell/s", "h2d_bytes_per_step": h2d / K,
+           "d2h_bytes_per_step": d2h / K, "wall_s": t_e2e,
+           "includes": "tti_create..tti_destroy: model upload + device precompute, geometry, K steps, snapshots to host, traces"}
+
+    # roofline of the dominant kernel (per-launch algorithmic bytes / event time)
+    n = args.profile_steps
+    interior = (h.Nx - 10) * (h.Nz - 5 - h.E)  # freesurface: rows [E, Nz-5)
+    halves = ALG_BYTES_HALF[variant]
+    dom = "stress" if ps >= pv else "velocity"
+    t_launch = (ps if dom == "stress" else pv) / n / 1e3
+    bytes_launch = halves[dom] * interior
+    peak, src = peaks()
+    achieved = bytes_launch / t_launch / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tfile):
+        try:
+            traffic = json.load(open(tfile)).get(variant, {}).get(dom)
+        except Exception:
+            traffic = None
+    roof = {"bound": "hbm", "kernel": f"k_{dom}<{variant}>", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": src, "traffic": traffic,
+            "alg_bytes_per_cell": halves[dom], "cells_per_launch": interior,
+            "step": {"alg_bytes_per_cell_update": ALG_BYTES_STEP[variant],
+                     "achieved_GBps": ALG_BYTES_STEP[variant] * cells * K / (ms / 1e3) / 1e9,
+                     "frac": ALG_BYTES_STEP[variant] * cells * K / (ms / 1e3) / 1e9 / peak},
+            "phase_ms_per_step": {"velocity": pv / n, "stress": ps / n, "other": po / n}}
+    line = {"metric": "Gcell-updates/s", "value": value, "unit": "Gcell/s", "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"plain forward, {variant}, salt-like synthetic 1126x7872 (padded 1256x8002), "
+                                   "freesurface, 12 Hz Ricker, 7872 receivers",
+                       "variant": variant, "nz": WORKLOAD["nz"], "nx": WORKLOAD["nx"], "Nz": h.Nz, "Nx": h.Nx,
+                       "cells": cells, "dt": WORKLOAD["dt"], "parallelism": f"shots x{world}",
+                       "l2": "inputs larger than L2 (>= 16 arrays x 41 MB per step)"},
+            "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary()}
+    return line
+
+
+# ---------------------------------------------------------------- reference arm
+def ref_program(variant: str):
+    for sub in ("bin", "strict"):
+        p = os.path.join(ROOT, "oracle", "_ref", sub, f"sufdmod2dTTIelastic_{variant}")
+        if os.path.exists(p):
+            return p, sub
+    return None, None
+
+
+def run_reference_cpu(variant: str, budget_s: float = 20.0, max_steps: int = 400):
+    """Times the reference's own OpenMP build on this host's cores on the bench
+    workload for a bounded number of steps; returns a cpu_baseline dict."""
+    prog, build = ref_program(variant)
+    if prog is None:
+        return None
+    m = model()
+    work = tempfile.mkdtemp(prefix="ttifd_ref_")
+    try:
+        files = synthetic.write_model(work, m)
+        sx, sz, gx, gz = geometry(0)
+        ncores = os.cpu_count() or 1
+        env = dict(os.environ, OMP_NUM_THREADS=str(ncores), OMP_PROC_BIND="close", OMP_PLACES="cores",
+                   SUSHIM_QUIET="1")
+
+        def once(nt):
+            wav = synthetic.ricker(nt, WORKLOAD["dt"], WORKLOAD["fpeak"])
+            synthetic.write_su_source(os.path.join(work, "src.su"), wav[None, :], [sx], [sz], WORKLOAD["dt"])
+            synthetic.write_su_receivers(os.path.join(work, "rec.su"), gx, gz)
+            a = [f"{k}={v}" for k, v in WORKLOAD.items() if k not in ("wsave",)] + [
+                f"nt={nt}", "wsave=0", "shotID=1", f"sourcefile={work}/src.su", f"recposfile={work}/rec.su"]
+            a += [f"{k}file={files[k]}" for k in ("vp", "vs", "rho", "epsilon", "delta", "theta")]
+            r = subprocess.run([prog] + a, cwd=work, env=env, capture_output=True, text=True)
+            mt = re.search(r"Finite difference modeling takes ([0-9.eE+-]+) s", r.stdout)
+            if r.returncode != 0 or not mt:
+                raise RuntimeError(f"reference run failed ({r.returncode}): {r.stderr[-500:]}")
+            return float(mt.group(1))
+
+        t = once(10)
+        steps = int(max(10, min(max_steps, 10 * budget_s / max(t, 1e-3))))
+        t = once(steps)
+        E = WORKLOAD["ealThick"] + 5
+        cells = (WORKLOAD["nz"] + 2 * E) * (WORKLOAD["nx"] + 2 * E)
+        return {"value": cells * steps / t / 1e9, "unit": "Gcell/s", "cores": ncores, "kind": "reference",
+                "sample": f"{steps} steps of the same workload ({variant}), reference OpenMP build ({build}), "
+                          f"loop time from its own 'Finite difference modeling takes' line: {t:.2f} s",
+                "steps": steps, "loop_s": t}
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+# ---------------------------------------------------------------- distributed
+_PG = None
+
+
+def dist_init():
+    global _PG
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+        _PG = dist
+    return int(os.environ.get("RANK", "0")), world, int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def dist_barrier():
+    if _PG is not None:
+        _PG.barrier()
+
+
+def dist_max(x: float) -> float:
+    if _PG is None:
+        return x
+    import torch
+
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    _PG.all_reduce(t, op=_PG.ReduceOp.MAX)
+    return float(t.item())
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--variant", default="coordinate_rotation",
+                    choices=["coordinate_rotation", "tensor_rotation", "bond_transformation"])
+    ap.add_argument("--profile-steps", type=int, default=50)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank, world, local_rank = dist_init()
+
+    if args.impl == "reference":
+        if rank == 0:
+            cb = run_reference_cpu(args.variant)
+            if cb is None:
+                print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built on this host"}))
+            else:
+                line = {"impl": "reference", "metric": "Gcell-updates/s", "value": cb["value"], "unit": "Gcell/s",
+                        "n_gpus": world, "steps": cb["steps"], "warmup": 0, "higher_is_better": True,
+                        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                        "config": {"workload": f"plain forward, {args.variant}, salt-like synthetic 1126x7872",
+                                   "variant": args.variant},
+                        "cpu_baseline": cb,
+                        "e2e": {"value": cb["value"], "unit": "Gcell/s", "h2d_bytes_per_step": 0,
+                                "d2h_bytes_per_step": 0}}
+                print(json.dumps(line), flush=True)
+        if _PG is not None:
+            _PG.destroy_process_group()
+        return
+
+    line = run_ours(args, rank, world, local_rank)
+    if rank == 0:
+        if not args.no_cpu_baseline:
+            try:
+                line["cpu_baseline"] = run_reference_cpu(args.variant)
+            except Exception as e:  # reported, not fatal
+                line["cpu_baseline"] = {"error": str(e)[:300]}
+        print(json.dumps(line), flush=True)
+    if _PG is not None:
+        _PG.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,176 @@
+/*
+ * ttifd.h -- C ABI of the B200 time-stepping library for 2D TTI elastic
+ * modelling on a rotated staggered grid (RSG).
+ *
+ * Each entry point replaces a region of the reference drivers'
+ * main() (wavetomo/TTI-FDModeling):
+ *   src/main/sufdmod2dTTIelastic/sufdmod2dTTIelastic_coordinate_rotation.c
+ *   src/main/sufdmod2dTTIelastic/sufdmod2dTTIelastic_tensor_rotation.c
+ *   src/main/sufdmod2dTTIelastic/sufdmod2dTTIelastic_bond_transformation.c
+ * (cited below as coord:, tensor:, bond: with line numbers). The caller keeps
+ * getpar, the model file reads, padModel2d, read2dsource / read2dreceiver and
+ * traces2d_output; everything from the stability check to the end of the time
+ * loop runs on the GPU behind these calls.
+ *
+ * Conventions
+ *  - Plain C types only. Every function returns an int status (TTI_OK = 0);
+ *    tti_last_error() gives the message. Callers that want the reference's
+ *    behaviour print it with err() and exit(1).
+ *  - Grids: Nz = nz + 2E, Nx = nx + 2E with E = ealThick + 5 (the reference
+ *    adds N = 5 to ealThick, coord:309-312). Host arrays are [Nx][Nz] FP32,
+ *    z fastest (the layout of CWP alloc2float(Nz, Nx); pass arr[0]).
+ *  - One handle = one shot on one device, one CUDA stream, one host thread.
+ *  - Host buffers are owned by the caller and copied; device memory is owned
+ *    by the handle.
+ */
+#ifndef TTIFD_H
+#define TTIFD_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define TTI_OK 0
+#define TTI_ERR_ARG 1       /* invalid argument or configuration            */
+#define TTI_ERR_UNSTABLE 2  /* dt above the RSG stability limit (stable.c:217-246) */
+#define TTI_ERR_RANGE 3     /* source / receiver position out of the model (obsinfo.c:69-80, 206-218) */
+#define TTI_ERR_CUDA 4      /* CUDA runtime error                           */
+#define TTI_ERR_NOMEM 5     /* device allocation failed                     */
+#define TTI_ERR_NONFINITE 6 /* NaN/Inf watchdog tripped in the wavefield    */
+#define TTI_ERR_STATE 7     /* call out of order (e.g. run before upload)   */
+#define TTI_ERR_CALLBACK 8  /* a host callback returned nonzero             */
+
+/* ---- formulations (the three reference drivers) ---- */
+#define TTI_COORDINATE 0 /* coordinate rotation, coord:611-926 */
+#define TTI_TENSOR 1     /* tensor rotation,     tensor:614-935 */
+#define TTI_BOND 2       /* Bond transformation, bond:651-954 */
+
+/* ---- receiver components (elastic2dReceiver, isoelastic.c:103-144) ---- */
+#define TTI_REC_VX 0
+#define TTI_REC_VZ 1
+#define TTI_REC_P 2
+
+/* ---- wavefield ids for tti_fetch_field ---- */
+#define TTI_F_VX 0
+#define TTI_F_VZ 1
+#define TTI_F_SXX 2
+#define TTI_F_SZZ 3
+#define TTI_F_SXZ 4
+#define TTI_F_TXX 5 /* tensor formulation only */
+#define TTI_F_TZZ 6
+#define TTI_F_TXZ 7
+
+/* ---- precomputed per-cell arrays for tti_fetch_param (the setup dumps
+ *      D_/Beta_/coef1_/coef2_/invrho_/c*_%05d_%05d.bin, coord:480-557) ---- */
+#define TTI_P_D 0
+#define TTI_P_BETA 1
+#define TTI_P_COEF1 2
+#define TTI_P_COEF2 3
+#define TTI_P_INVRHO 4
+#define TTI_P_C11 5
+#define TTI_P_C13 6
+#define TTI_P_C15 7 /* Bond only */
+#define TTI_P_C33 8
+#define TTI_P_C35 9 /* Bond only */
+#define TTI_P_C55 10
+#define TTI_P_SIN 11   /* coordinate: sin(theta) at stress nodes */
+#define TTI_P_COS 12   /* coordinate: cos(theta) at stress nodes */
+#define TTI_P_SIN_V 13 /* coordinate: sin(theta) averaged to velocity nodes */
+#define TTI_P_COS_V 14 /* coordinate: cos(theta) averaged to velocity nodes */
+#define TTI_P_SIN2 15  /* tensor: sin^2(theta) */
+#define TTI_P_COS2 16  /* tensor: cos^2(theta) */
+#define TTI_P_SIN_2T 17 /* tensor: sin(2 theta) */
+#define TTI_P_VP 18    /* vp after the MEAL rescale vp/Beta (meal.c:454-460) */
+#define TTI_P_VS 19    /* vs after vs/Beta */
+#define TTI_P_RHO 20   /* rho after rho*Beta */
+#define TTI_P_COUNT 21
+
+/* Run configuration: the getpar keys of the reference drivers (coord:134-294). */
+typedef struct tti_config {
+  int variant;      /* TTI_COORDINATE / TTI_TENSOR / TTI_BOND */
+  int nz, nx, nt;   /* physical grid and time samples */
+  float dx, dz, dt; /* sampling (m, m, s) */
+  int ealThick;     /* absorbing layers as given on the command line (default 30) */
+  float eal_alpha;  /* MEAL weight exponent, -1 = default 2.5 (meal.c:74-77) */
+  int freesurface;  /* 1 = stress-image free surface at z = E */
+  float fpeak;      /* peak frequency used by MEAL's Beta */
+  float scalar;     /* factor applied to theta (degrees) */
+  int stype;        /* source type 1..8 */
+  int seistype;     /* 0 none, 1 vx+vz, 2 p, 3 all */
+  int mt;           /* receiver decimation in time */
+  int wsave;        /* snapshot kind 0..5 */
+  int savew;        /* 0: physical area only, 1: whole padded grid */
+  int snap_sample;  /* snapshot every snap_sample steps (it % snap_sample == 0) */
+  int mode;         /* 1: it = 0..nt-1, 2: it = nt-1..0 (coord:611) */
+  int energy;       /* 1: record Ek/Ep per step (coord:898-924) */
+} tti_config;
+
+typedef struct tti_handle tti_handle;
+
+/* Snapshot sink: called on the host thread at every it % snap_sample == 0.
+ * `kind` is 1 (vx), 2 (vz), 3 (p), 4 (vxp), 5 (vzp), 6 (vxs), 7 (vzs),
+ * matching the file names of elastic2dSnapshot (isoelastic.c:240-289).
+ * `data` is nx_out records of nz_out floats (the raw-binary file body).
+ * Return 0 to continue, nonzero to abort the run with TTI_ERR_CALLBACK. */
+typedef int (*tti_snapshot_fn)(void *user, int it, int kind, const float *data, int nz_out, int nx_out);
+
+/* Creates a handle on CUDA device `device`; validates cfg. Replaces the
+ * allocation block coord:295-344 (device side). */
+int tti_create(tti_handle **out, const tti_config *cfg, int device);
+int tti_destroy(tti_handle *h);
+/* Last error message of h (or of the last failed tti_create when h is NULL). */
+const char *tti_last_error(const tti_handle *h);
+/* Padded grid sizes and E = ealThick + 5. */
+int tti_grid(const tti_handle *h, int *Nz, int *Nx, int *E);
+
+/* Uploads the padded model ([Nx][Nz], after padModel2d) and precomputes on the
+ * device: stability check (coord:476, stable.c:217-246), MEAL D/Beta
+ * (coord:478, meal.c:51-201), MEAL FD coefficients with the vp/vs/rho rescale
+ * (coord:479, meal.c:450-502) and the stiffness build of the selected
+ * formulation (coord:497-537, tensor:498-535, bond:492-568 incl. the
+ * free-surface stiffness rewrite). vs/rho must be given (defaults are the
+ * caller's, coord:362-415). */
+int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const float *rho, const float *epsilon,
+                     const float *delta, const float *theta);
+/* Copies one precomputed array ([Nx][Nz]) to host memory (setup dumps). */
+int tti_fetch_param(tti_handle *h, int which, float *out);
+
+/* Source geometry and wavelets, as read2dsource returns them
+ * (obsinfo.c:34-87): positions in cells of the physical grid,
+ * src is [ntrace][nt]. Replaces the Source2D argument of the loop. */
+int tti_set_source(tti_handle *h, int ntrace, const int *posx, const int *posz, const float *src);
+/* Receiver line for one component (read2dreceiver, obsinfo.c:175-230). */
+int tti_set_receivers(tti_handle *h, int kind, int ntrace, const int *posx, const int *posz);
+
+/* Runs the whole time loop (coord:611-926): zero wavefields, nt steps,
+ * snapshots through `snap` (may be NULL), receivers, energy. */
+int tti_run(tti_handle *h, tti_snapshot_fn snap, void *user);
+/* Lower-level stepping: zero the wavefields / advance `nsteps` steps from the
+ * current step index without snapshots. tti_run = reset + all steps. */
+int tti_reset(tti_handle *h);
+int tti_step(tti_handle *h, int nsteps);
+/* Device time in ms of the last tti_run / tti_step call (CUDA events). */
+int tti_elapsed_ms(const tti_handle *h, float *ms);
+/* Measurement aid (no counterpart in the reference, which only prints the
+ * loop wall time, coord:927-930): advances `nsteps` steps like tti_step with
+ * CUDA events on the handle's stream around each phase and returns the total
+ * device ms per phase: ms[0] velocity update, ms[1] stress update,
+ * ms[2] everything else (sources, free surface, receivers, energy). */
+int tti_profile_steps(tti_handle *h, int nsteps, float ms[3]);
+/* Number of kernels this handle has launched since tti_create. */
+int tti_kernel_launches(const tti_handle *h, long long *n);
+
+/* Recorded traces of one component, [ntrace][(nt-1)/mt+1] (Receiver2D.recv). */
+int tti_fetch_traces(tti_handle *h, int kind, float *out);
+/* Current wavefield ([Nx][Nz]). */
+int tti_fetch_field(tti_handle *h, int which, float *out);
+/* Energy per step (energy = 1): Ek[nt], Ep[nt] (coord:898-924, 942-968). */
+int tti_fetch_energy(tti_handle *h, float *ek, float *ep);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

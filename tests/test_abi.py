@@ -1,0 +1,52 @@
+"""The C-ABI library loads on a CPU-only host and exports every entry point
+include/ttifd.h declares (no compute calls: there may be no GPU here)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for fn in os.listdir(os.path.join(ROOT, "include")):
+        if fn.endswith(".h"):
+            src = open(os.path.join(ROOT, "include", fn)).read()
+            src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+            names.update(re.findall(r"\b(tti_\w+)\s*\(", src))
+    return sorted(names)
+
+
+def test_header_declares_the_boundary():
+    names = declared_symbols()
+    for must in ("tti_create", "tti_upload_model", "tti_set_source", "tti_set_receivers", "tti_run",
+                 "tti_fetch_traces", "tti_destroy", "tti_last_error"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol(gpu_lib):
+    lib = gpu_lib
+    missing = [n for n in declared_symbols() if not hasattr(lib, n)]
+    assert not missing, f"not exported: {missing}"
+
+
+def test_python_binding_covers_the_header():
+    import ttifd
+
+    names = set(declared_symbols())
+    assert set(ttifd.EXPORTS) <= names
+
+
+def test_create_without_gpu_fails_cleanly(gpu_lib):
+    """On a host without a GPU tti_create must return an error, not crash."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    import ttifd
+
+    with pytest.raises(ttifd.TTIError) as e:
+        ttifd.Modeling(nz=10, nx=10, nt=10, dx=10, dz=10, dt=0.001, fpeak=10)
+    assert e.value.code == ttifd.ERR_CUDA

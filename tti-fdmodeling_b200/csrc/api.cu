@@ -1,0 +1,625 @@
+// C ABI of the B200 TTI RSG library (include/ttifd.h).
+#include <cfloat>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "launch.cuh"
+
+using namespace ttifd;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+int set_err(tti_handle *h, int code, const char *fmt, ...)
+{
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (h) h->err = buf;
+  else g_create_error = buf;
+  return code;
+}
+
+#define CK(h, call)                                                                                     \
+  do {                                                                                                  \
+    cudaError_t e_ = (call);                                                                            \
+    if (e_ != cudaSuccess)                                                                              \
+      return set_err((h), e_ == cudaErrorMemoryAllocation ? TTI_ERR_NOMEM : TTI_ERR_CUDA, "%s: %s (%s:%d)", \
+                     #call, cudaGetErrorString(e_), __FILE__, __LINE__);                                \
+  } while (0)
+
+// Arrays each formulation needs on the device (beyond D/Beta/coef/vp/vs/rho
+// which every formulation keeps for the setup dumps).
+bool param_used(int variant, int p)
+{
+  switch (p) {
+  case TTI_P_C15:
+  case TTI_P_C35:
+    return variant == TTI_BOND;
+  case TTI_P_SIN:
+  case TTI_P_COS:
+  case TTI_P_SIN_V:
+  case TTI_P_COS_V:
+    return variant == TTI_COORDINATE;
+  case TTI_P_SIN2:
+  case TTI_P_COS2:
+  case TTI_P_SIN_2T:
+    return variant == TTI_TENSOR;
+  default:
+    return true;
+  }
+}
+
+int nfields(int variant) { return variant == TTI_TENSOR ? 8 : 5; }
+
+StepArgs step_args(const tti_handle *h)
+{
+  StepArgs a;
+  a.g = h->g;
+  a.f = Fields{h->fld[0], h->fld[1], h->fld[2], h->fld[3], h->fld[4], h->fld[5], h->fld[6], h->fld[7]};
+  const float *const *P = h->par;
+  a.p = Params{P[TTI_P_COEF1], P[TTI_P_COEF2], P[TTI_P_INVRHO], P[TTI_P_C11], P[TTI_P_C13], P[TTI_P_C15],
+               P[TTI_P_C33],   P[TTI_P_C35],   P[TTI_P_C55],    P[TTI_P_SIN], P[TTI_P_COS], P[TTI_P_SIN_V],
+               P[TTI_P_COS_V], P[TTI_P_SIN2],  P[TTI_P_COS2],   P[TTI_P_SIN_2T]};
+  a.invdx = h->invdx;
+  a.invdz = h->invdz;
+  a.variant = h->cfg.variant;
+  a.exact = h->exact;
+  return a;
+}
+
+// Host precompute of the source weight tables in the reference's float
+// expression order (coord:607, 684-691, 711-713, 733-734, 775-777, 880-882).
+void source_tables(const tti_handle *h, SourceTables *t)
+{
+  const float dx = h->cfg.dx, dz = h->cfg.dz, dt = h->cfg.dt;
+  const float alpha = logf(0.8f) / (dx * dx + dz * dz);
+  for (int a = 0; a < 11; ++a)
+    for (int b = 0; b < 11; ++b) {
+      const float rx = (a - NH) * dx, rz = (b - NH) * dz;
+      const float w = expf(alpha * (rx * rx + rz * rz)) * h->invdx * h->invdz * dt;
+      const int k = a * 11 + b;
+      t->k1[k] = 0.5f * w;
+      t->kx[k] = 2.0f * alpha * rx * w;
+      t->kz[k] = 2.0f * alpha * rz * w;
+      t->k5[k] = w;
+      t->k7[k] = 0.5f * sqrtf(2.0f) * w;
+    }
+  t->q8 = 0.125f * sqrtf(2.0f);
+}
+
+int check_cfg(const tti_config *c)
+{
+  if (c->variant < 0 || c->variant > 2) return set_err(nullptr, TTI_ERR_ARG, "variant must be 0, 1 or 2");
+  if (c->nz <= 0 || c->nx <= 0 || c->nt <= 0) return set_err(nullptr, TTI_ERR_ARG, "nz, nx, nt must be positive");
+  if (!(c->dx > 0) || !(c->dz > 0) || !(c->dt > 0)) return set_err(nullptr, TTI_ERR_ARG, "dx, dz, dt must be positive");
+  if (c->ealThick < 0) return set_err(nullptr, TTI_ERR_ARG, "ealThick must be >= 0");
+  if (!(c->fpeak > 0)) return set_err(nullptr, TTI_ERR_ARG, "fpeak must be positive");
+  if (c->freesurface != 0 && c->freesurface != 1) return set_err(nullptr, TTI_ERR_ARG, "freesurface must be 0 or 1");
+  if (c->stype < 1 || c->stype > 8) return set_err(nullptr, TTI_ERR_ARG, "stype must be 1..8");
+  if (c->seistype < 0 || c->seistype > 3) return set_err(nullptr, TTI_ERR_ARG, "seistype must be 0..3");
+  if (c->mt < 1) return set_err(nullptr, TTI_ERR_ARG, "mt must be >= 1");
+  if (c->wsave < 0 || c->wsave > 5) return set_err(nullptr, TTI_ERR_ARG, "wsave must be 0..5");
+  if (c->savew != 0 && c->savew != 1) return set_err(nullptr, TTI_ERR_ARG, "savew must be 0 or 1");
+  if (c->wsave > 0 && c->snap_sample < 1) return set_err(nullptr, TTI_ERR_ARG, "snap_sample must be >= 1");
+  if (c->mode != 1 && c->mode != 2) return set_err(nullptr, TTI_ERR_ARG, "mode must be 1 or 2");
+  return TTI_OK;
+}
+
+int current_it(const tti_handle *h) { return h->cfg.mode == 2 ? h->cfg.nt - 1 - h->step_index : h->step_index; }
+
+// Launches one time step (coord:611-926 body). With `ev` (5 events) the
+// phases are bracketed for tti_profile_steps: ev[0] | velocity | ev[1] |
+// velocity sources | ev[2] | stress | ev[3] | the rest | ev[4].
+int launch_one_step(tti_handle *h, const SourceTables &tab, cudaEvent_t *ev = nullptr)
+{
+  const tti_config &c = h->cfg;
+  const int it = current_it(h);
+  StepArgs a = step_args(h);
+  SourceSet s{h->nsrc, h->d_sx, h->d_sz, h->d_src, c.nt};
+  const bool vsrc = s.n > 0 && c.stype >= 2, ssrc = s.n > 0 && c.stype == 1;
+  if (ev) CK(h, cudaEventRecord(ev[0], h->stream));
+  launch_velocity(a, h->stream);
+  if (ev) CK(h, cudaEventRecord(ev[1], h->stream));
+  if (vsrc) launch_sources(a, s, &tab, c.stype, 0, it, h->stream);
+  if (ev) CK(h, cudaEventRecord(ev[2], h->stream));
+  launch_stress(a, h->stream);
+  if (ev) CK(h, cudaEventRecord(ev[3], h->stream));
+  h->launches += 2 + vsrc + ssrc;
+  if (c.freesurface == 1) {
+    launch_free_surface(a, h->stream);
+    h->launches++;
+  }
+  if (ssrc) launch_sources(a, s, &tab, c.stype, 1, it, h->stream);
+  if (c.seistype > 0 && it % c.mt == 0) {
+    ReceiverSet r;
+    for (int k = 0; k < 3; ++k) {
+      r.n[k] = h->nrec[k];
+      r.x[k] = h->d_rx[k];
+      r.z[k] = h->d_rz[k];
+      r.rec[k] = h->d_rec[k];
+    }
+    if (r.n[0] + r.n[1] + r.n[2] > 0) {
+      launch_receivers(a, r, c.seistype, it / c.mt, h->d_flag, h->stream);
+      h->launches++;
+    }
+  }
+  if (c.energy == 1) {
+    launch_energy(a, c.nz, c.nx, h->d_energy + 2 * (size_t)it, h->stream);
+    h->launches++;
+  }
+  if (ev) CK(h, cudaEventRecord(ev[4], h->stream));
+  CK(h, cudaGetLastError());
+  h->step_index++;
+  return TTI_OK;
+}
+
+int snapshot_kinds(int wsave, int *kinds)
+{
+  switch (wsave) {
+  case 1: kinds[0] = 1; kinds[1] = 2; return 2;
+  case 2: kinds[0] = 3; return 1;
+  case 3: kinds[0] = 1; kinds[1] = 2; kinds[2] = 3; return 3;
+  case 4: kinds[0] = 4; kinds[1] = 5; return 2;
+  case 5: kinds[0] = 6; kinds[1] = 7; return 2;
+  default: return 0;
+  }
+}
+
+int do_snapshot(tti_handle *h, tti_snapshot_fn fn, void *user, int it)
+{
+  const Grid &g = h->g;
+  const int nzo = h->cfg.savew == 0 ? g.Nz - 2 * g.E : g.Nz;
+  const int nxo = h->cfg.savew == 0 ? g.Nx - 2 * g.E : g.Nx;
+  const size_t n = (size_t)nzo * nxo;
+  if (h->snap_cap < n) {
+    cudaFree(h->d_snap);
+    cudaFreeHost(h->h_snap);
+    h->d_snap = nullptr;
+    h->h_snap = nullptr;
+    h->snap_cap = 0;
+    CK(h, cudaMalloc(&h->d_snap, n * sizeof(float)));
+    CK(h, cudaMallocHost(&h->h_snap, n * sizeof(float)));
+    h->snap_cap = n;
+  }
+  int kinds[3];
+  const int nk = snapshot_kinds(h->cfg.wsave, kinds);
+  StepArgs a = step_args(h);
+  for (int q = 0; q < nk; ++q) {
+    launch_snapshot(a, kinds[q], h->cfg.savew, h->d_snap, h->stream);
+    h->launches++;
+    CK(h, cudaMemcpyAsync(h->h_snap, h->d_snap, n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    if (fn(user, it, kinds[q], h->h_snap, nzo, nxo) != 0)
+      return set_err(h, TTI_ERR_CALLBACK, "snapshot callback aborted the run at it=%d", it);
+  }
+  return TTI_OK;
+}
+
+int check_flag(tti_handle *h)
+{
+  int flag = 0;
+  CK(h, cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  if (flag) return set_err(h, TTI_ERR_NONFINITE, "non-finite value recorded at a receiver (unstable run?)");
+  return TTI_OK;
+}
+
+int copy_out_pitched(tti_handle *h, const float *src, float *out)
+{
+  const Grid &g = h->g;
+  CK(h, cudaMemcpy2DAsync(out, (size_t)g.Nz * sizeof(float), src, (size_t)g.ldz * sizeof(float),
+                          (size_t)g.Nz * sizeof(float), g.Nx, cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  return TTI_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *tti_last_error(const tti_handle *h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+int tti_create(tti_handle **out, const tti_config *cfg, int device)
+{
+  if (!out || !cfg) return set_err(nullptr, TTI_ERR_ARG, "null argument");
+  *out = nullptr;
+  int rc = check_cfg(cfg);
+  if (rc) return rc;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return set_err(nullptr, TTI_ERR_CUDA, "no CUDA device available");
+  if (device < 0 || device >= ndev) return set_err(nullptr, TTI_ERR_ARG, "device %d out of range", device);
+  tti_handle *h = new tti_handle();
+  h->cfg = *cfg;
+  h->device = device;
+  const char *ex = getenv("TTIFD_EXACT");
+  h->exact = ex && ex[0] == '1';
+  Grid &g = h->g;
+  g.E = cfg->ealThick + NH;
+  g.Nz = cfg->nz + 2 * g.E;
+  g.Nx = cfg->nx + 2 * g.E;
+  g.ldz = (g.Nz + 31) / 32 * 32;
+  g.izStart = cfg->freesurface == 0 ? NH : g.E;
+  g.n = (size_t)g.ldz * g.Nx;
+  h->invdx = (float)(1.0 / cfg->dx);
+  h->invdz = (float)(1.0 / cfg->dz);
+  h->nts = (cfg->nt - 1) / cfg->mt + 1;
+  auto fail = [&](int code) {
+    std::string msg = h->err;
+    tti_destroy(h);
+    set_err(nullptr, code, "%s", msg.c_str());
+    return code;
+  };
+  if (cudaSetDevice(device) != cudaSuccess) {
+    set_err(h, TTI_ERR_CUDA, "cudaSetDevice(%d) failed", device);
+    return fail(TTI_ERR_CUDA);
+  }
+  auto alloc = [&](float **p) -> int {
+    cudaError_t e = cudaMalloc(p, g.n * sizeof(float));
+    if (e != cudaSuccess)
+      return set_err(h, TTI_ERR_NOMEM, "device allocation of %zu bytes failed: %s", g.n * sizeof(float),
+                     cudaGetErrorString(e));
+    e = cudaMemsetAsync(*p, 0, g.n * sizeof(float), h->stream);
+    if (e != cudaSuccess) return set_err(h, TTI_ERR_CUDA, "cudaMemset failed: %s", cudaGetErrorString(e));
+    return TTI_OK;
+  };
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
+    set_err(h, TTI_ERR_CUDA, "stream/event creation failed");
+    return fail(TTI_ERR_CUDA);
+  }
+  for (int f = 0; f < nfields(cfg->variant); ++f)
+    if ((rc = alloc(&h->fld[f]))) return fail(rc);
+  for (int p = 0; p < TTI_P_COUNT; ++p)
+    if (param_used(cfg->variant, p) && (rc = alloc(&h->par[p]))) return fail(rc);
+  if (cudaMalloc(&h->d_flag, sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&h->d_energy, sizeof(double) * 2 * (size_t)cfg->nt) != cudaSuccess) {
+    set_err(h, TTI_ERR_NOMEM, "device allocation failed");
+    return fail(TTI_ERR_NOMEM);
+  }
+  cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream);
+  cudaMemsetAsync(h->d_energy, 0, sizeof(double) * 2 * (size_t)cfg->nt, h->stream);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
+    set_err(h, TTI_ERR_CUDA, "initialisation failed");
+    return fail(TTI_ERR_CUDA);
+  }
+  *out = h;
+  return TTI_OK;
+}
+
+int tti_destroy(tti_handle *h)
+{
+  if (!h) return TTI_OK;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (auto &p : h->fld) cudaFree(p);
+  for (auto &p : h->par) cudaFree(p);
+  for (int k = 0; k < 3; ++k) {
+    cudaFree(h->d_rx[k]);
+    cudaFree(h->d_rz[k]);
+    cudaFree(h->d_rec[k]);
+  }
+  cudaFree(h->d_sx);
+  cudaFree(h->d_sz);
+  cudaFree(h->d_src);
+  cudaFree(h->d_energy);
+  cudaFree(h->d_flag);
+  cudaFree(h->d_snap);
+  if (h->h_snap) cudaFreeHost(h->h_snap);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  for (auto e : h->pev)
+    if (e) cudaEventDestroy(e);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return TTI_OK;
+}
+
+int tti_grid(const tti_handle *h, int *Nz, int *Nx, int *E)
+{
+  if (!h) return TTI_ERR_ARG;
+  if (Nz) *Nz = h->g.Nz;
+  if (Nx) *Nx = h->g.Nx;
+  if (E) *E = h->g.E;
+  return TTI_OK;
+}
+
+int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const float *rho, const float *epsilon,
+                     const float *delta, const float *theta)
+{
+  if (!h || !vp || !vs || !rho || !epsilon || !delta || !theta) return set_err(h, TTI_ERR_ARG, "null model array");
+  CK(h, cudaSetDevice(h->device));
+  const tti_config &c = h->cfg;
+  const Grid &g = h->g;
+  const size_t np = (size_t)g.Nz * g.Nx;
+  // stability check on the unscaled padded vp (stable.c:217-246)
+  {
+    double vmax = FLT_MIN;
+    for (size_t i = 0; i < np; ++i) vmax = fmaxf(vp[i], (float)vmax);
+    const double csum = (double)rsg(0) + (double)rsg(2) + (double)rsg(4);
+    const double dtmax = 1.0f / (vmax * sqrt((1.0 / (c.dx * c.dx) + 1.0 / (c.dz * c.dz)) * csum));
+    if (c.dt > dtmax)
+      return set_err(h, TTI_ERR_UNSTABLE,
+                     "the finite differenct scheme is unstable! the time step size must smaller than %5.5f!", dtmax);
+  }
+  // raw model on the device (pitched), freed after the precompute
+  float *raw[6] = {};
+  const float *src[6] = {vp, vs, rho, epsilon, delta, theta};
+  float *d_w = nullptr;
+  int rc = TTI_OK;
+  for (int k = 0; k < 6 && rc == TTI_OK; ++k) {
+    cudaError_t e = cudaMalloc(&raw[k], g.n * sizeof(float));
+    if (e != cudaSuccess) rc = set_err(h, TTI_ERR_NOMEM, "device allocation failed: %s", cudaGetErrorString(e));
+    else
+      e = cudaMemcpy2DAsync(raw[k], (size_t)g.ldz * sizeof(float), src[k], (size_t)g.Nz * sizeof(float),
+                            (size_t)g.Nz * sizeof(float), g.Nx, cudaMemcpyHostToDevice, h->stream);
+    if (rc == TTI_OK && e != cudaSuccess) rc = set_err(h, TTI_ERR_CUDA, "model upload: %s", cudaGetErrorString(e));
+  }
+  if (rc == TTI_OK) {
+    // MEAL scalars evaluated with the host libm, as meal.c:23-29, 62-66 do
+    const int nl = g.E;
+    const float pd = 2;
+    const float Rcoef = powf(10.0f, -1.0f * ((log10f((float)nl) - 1.0f) / (log10f(2.0f))) - 3.0f - 0.5f * pd);
+    const float alpha = c.eal_alpha == -1.0f ? 2.5f : c.eal_alpha;
+    std::vector<float> w(nl + 1, 0.0f);
+    for (int l = 1; l <= nl; ++l) {
+      const float d = (0.1f * l) / (0.1f * nl);
+      w[l] = expf(logf(2.0f) * powf(d, alpha)) - 1.0f;
+    }
+    cudaError_t e = cudaMalloc(&d_w, sizeof(float) * (nl + 1));
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d_w, w.data(), sizeof(float) * (nl + 1), cudaMemcpyHostToDevice, h->stream);
+    if (e != cudaSuccess) rc = set_err(h, TTI_ERR_CUDA, "MEAL table upload: %s", cudaGetErrorString(e));
+    MealConst mc;
+    mc.w = d_w;
+    mc.logR = logf(Rcoef);
+    const float thx = nl * c.dx, thz = nl * c.dz;
+    mc.two_thx = 2.0f * thx;
+    mc.two_thz = 2.0f * thz;
+    mc.dx_fpeak = c.dx * c.fpeak;
+    mc.dz_fpeak = c.dz * c.fpeak;
+    mc.sqrt3 = sqrtf(3.0f);
+    mc.dt = c.dt;
+    float **P = h->par;
+    SetupIn in{raw[0], raw[1], raw[2], raw[3], raw[4], raw[5]};
+    SetupOut o{P[TTI_P_D],   P[TTI_P_BETA],  P[TTI_P_COEF1], P[TTI_P_COEF2], P[TTI_P_VP],    P[TTI_P_VS],
+               P[TTI_P_RHO], P[TTI_P_INVRHO], P[TTI_P_C11],  P[TTI_P_C13],   P[TTI_P_C15],   P[TTI_P_C33],
+               P[TTI_P_C35], P[TTI_P_C55],   P[TTI_P_SIN],   P[TTI_P_COS],   P[TTI_P_SIN_V], P[TTI_P_COS_V],
+               P[TTI_P_SIN2], P[TTI_P_COS2], P[TTI_P_SIN_2T]};
+    if (rc == TTI_OK) {
+      launch_setup(g, in, o, mc, c.variant, c.scalar, c.freesurface, h->stream);
+      e = cudaGetLastError();
+      if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+      if (e != cudaSuccess) rc = set_err(h, TTI_ERR_CUDA, "setup kernels: %s", cudaGetErrorString(e));
+    }
+  }
+  cudaStreamSynchronize(h->stream);
+  for (auto p : raw) cudaFree(p);
+  cudaFree(d_w);
+  if (rc == TTI_OK) h->have_model = true;
+  return rc;
+}
+
+int tti_fetch_param(tti_handle *h, int which, float *out)
+{
+  if (!h || !out) return TTI_ERR_ARG;
+  if (which < 0 || which >= TTI_P_COUNT || !h->par[which])
+    return set_err(h, TTI_ERR_ARG, "parameter %d is not used by this formulation", which);
+  if (!h->have_model) return set_err(h, TTI_ERR_STATE, "model not uploaded");
+  CK(h, cudaSetDevice(h->device));
+  return copy_out_pitched(h, h->par[which], out);
+}
+
+int tti_set_source(tti_handle *h, int ntrace, const int *posx, const int *posz, const float *src)
+{
+  if (!h || ntrace < 0 || (ntrace > 0 && (!posx || !posz || !src))) return set_err(h, TTI_ERR_ARG, "bad source");
+  const tti_config &c = h->cfg;
+  for (int i = 0; i < ntrace; ++i) {
+    if (posz[i] < 0 || posz[i] > c.nz)
+      return set_err(h, TTI_ERR_RANGE, "the position of source in 1st dimension (%d) must be between 0 and %d!",
+                     posz[i], c.nz);
+    if (posx[i] < 0 || posx[i] > c.nx)
+      return set_err(h, TTI_ERR_RANGE, "the position of source in 2nd dimension (%d) must be between 0 and %d!",
+                     posx[i], c.nx);
+  }
+  CK(h, cudaSetDevice(h->device));
+  cudaFree(h->d_sx);
+  cudaFree(h->d_sz);
+  cudaFree(h->d_src);
+  h->d_sx = h->d_sz = nullptr;
+  h->d_src = nullptr;
+  h->nsrc = 0;
+  if (ntrace == 0) return TTI_OK;
+  std::vector<int> x(ntrace), z(ntrace);
+  for (int i = 0; i < ntrace; ++i) {
+    x[i] = posx[i] + h->g.E;
+    z[i] = posz[i] + h->g.E;
+  }
+  CK(h, cudaMalloc(&h->d_sx, sizeof(int) * ntrace));
+  CK(h, cudaMalloc(&h->d_sz, sizeof(int) * ntrace));
+  CK(h, cudaMalloc(&h->d_src, sizeof(float) * (size_t)ntrace * c.nt));
+  CK(h, cudaMemcpy(h->d_sx, x.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice));
+  CK(h, cudaMemcpy(h->d_sz, z.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice));
+  CK(h, cudaMemcpy(h->d_src, src, sizeof(float) * (size_t)ntrace * c.nt, cudaMemcpyHostToDevice));
+  h->nsrc = ntrace;
+  return TTI_OK;
+}
+
+int tti_set_receivers(tti_handle *h, int kind, int ntrace, const int *posx, const int *posz)
+{
+  if (!h || kind < 0 || kind > 2 || ntrace < 0 || (ntrace > 0 && (!posx || !posz)))
+    return set_err(h, TTI_ERR_ARG, "bad receiver arguments");
+  const tti_config &c = h->cfg;
+  for (int i = 0; i < ntrace; ++i) {
+    if (posz[i] < 0 || posz[i] > c.nz)
+      return set_err(h, TTI_ERR_RANGE, "the position of receiver in 1st dimension (%d) must be between 0 and %d!",
+                     posz[i], c.nz);
+    if (posx[i] < 0 || posx[i] > c.nx)
+      return set_err(h, TTI_ERR_RANGE, "the position of receiver in 2nd dimension (%d) must be between 0 and %d!",
+                     posx[i], c.nx);
+  }
+  CK(h, cudaSetDevice(h->device));
+  cudaFree(h->d_rx[kind]);
+  cudaFree(h->d_rz[kind]);
+  cudaFree(h->d_rec[kind]);
+  h->d_rx[kind] = h->d_rz[kind] = nullptr;
+  h->d_rec[kind] = nullptr;
+  h->nrec[kind] = 0;
+  if (ntrace == 0) return TTI_OK;
+  std::vector<int> x(ntrace), z(ntrace);
+  for (int i = 0; i < ntrace; ++i) {
+    x[i] = posx[i] + h->g.E;
+    z[i] = posz[i] + h->g.E;
+  }
+  CK(h, cudaMalloc(&h->d_rx[kind], sizeof(int) * ntrace));
+  CK(h, cudaMalloc(&h->d_rz[kind], sizeof(int) * ntrace));
+  CK(h, cudaMalloc(&h->d_rec[kind], sizeof(float) * (size_t)ntrace * h->nts));
+  CK(h, cudaMemcpy(h->d_rx[kind], x.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice));
+  CK(h, cudaMemcpy(h->d_rz[kind], z.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice));
+  CK(h, cudaMemset(h->d_rec[kind], 0, sizeof(float) * (size_t)ntrace * h->nts));
+  h->nrec[kind] = ntrace;
+  return TTI_OK;
+}
+
+int tti_reset(tti_handle *h)
+{
+  if (!h) return TTI_ERR_ARG;
+  CK(h, cudaSetDevice(h->device));
+  for (auto p : h->fld)
+    if (p) CK(h, cudaMemsetAsync(p, 0, h->g.n * sizeof(float), h->stream));
+  for (int k = 0; k < 3; ++k)
+    if (h->d_rec[k]) CK(h, cudaMemsetAsync(h->d_rec[k], 0, sizeof(float) * (size_t)h->nrec[k] * h->nts, h->stream));
+  CK(h, cudaMemsetAsync(h->d_energy, 0, sizeof(double) * 2 * (size_t)h->cfg.nt, h->stream));
+  CK(h, cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+  h->step_index = 0;
+  return TTI_OK;
+}
+
+int tti_step(tti_handle *h, int nsteps)
+{
+  if (!h || nsteps < 0) return TTI_ERR_ARG;
+  if (!h->have_model) return set_err(h, TTI_ERR_STATE, "model not uploaded");
+  if (h->step_index + nsteps > h->cfg.nt) return set_err(h, TTI_ERR_STATE, "step past nt");
+  CK(h, cudaSetDevice(h->device));
+  SourceTables tab;
+  source_tables(h, &tab);
+  CK(h, cudaEventRecord(h->ev0, h->stream));
+  for (int n = 0; n < nsteps; ++n) {
+    int rc = launch_one_step(h, tab);
+    if (rc) return rc;
+  }
+  CK(h, cudaEventRecord(h->ev1, h->stream));
+  CK(h, cudaEventSynchronize(h->ev1));
+  CK(h, cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
+  return check_flag(h);
+}
+
+int tti_run(tti_handle *h, tti_snapshot_fn snap, void *user)
+{
+  if (!h) return TTI_ERR_ARG;
+  if (!h->have_model) return set_err(h, TTI_ERR_STATE, "model not uploaded");
+  int rc = tti_reset(h);
+  if (rc) return rc;
+  SourceTables tab;
+  source_tables(h, &tab);
+  const tti_config &c = h->cfg;
+  CK(h, cudaEventRecord(h->ev0, h->stream));
+  for (int n = 0; n < c.nt; ++n) {
+    const int it = current_it(h);
+    if ((rc = launch_one_step(h, tab))) return rc;
+    if (snap && c.wsave > 0 && it % c.snap_sample == 0)
+      if ((rc = do_snapshot(h, snap, user, it))) return rc;
+  }
+  CK(h, cudaEventRecord(h->ev1, h->stream));
+  CK(h, cudaEventSynchronize(h->ev1));
+  CK(h, cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
+  return check_flag(h);
+}
+
+int tti_profile_steps(tti_handle *h, int nsteps, float ms[3])
+{
+  if (!h || !ms || nsteps < 0) return TTI_ERR_ARG;
+  if (!h->have_model) return set_err(h, TTI_ERR_STATE, "model not uploaded");
+  if (h->step_index + nsteps > h->cfg.nt) return set_err(h, TTI_ERR_STATE, "step past nt");
+  CK(h, cudaSetDevice(h->device));
+  for (int k = 0; k < 5; ++k)
+    if (!h->pev[k]) CK(h, cudaEventCreate(&h->pev[k]));
+  SourceTables tab;
+  source_tables(h, &tab);
+  ms[0] = ms[1] = ms[2] = 0.0f;
+  for (int n = 0; n < nsteps; ++n) {
+    int rc = launch_one_step(h, tab, h->pev);
+    if (rc) return rc;
+    CK(h, cudaEventSynchronize(h->pev[4]));
+    float t01, t12, t23, t34;
+    CK(h, cudaEventElapsedTime(&t01, h->pev[0], h->pev[1]));
+    CK(h, cudaEventElapsedTime(&t12, h->pev[1], h->pev[2]));
+    CK(h, cudaEventElapsedTime(&t23, h->pev[2], h->pev[3]));
+    CK(h, cudaEventElapsedTime(&t34, h->pev[3], h->pev[4]));
+    ms[0] += t01;
+    ms[1] += t23;
+    ms[2] += t12 + t34;
+  }
+  return check_flag(h);
+}
+
+int tti_kernel_launches(const tti_handle *h, long long *n)
+{
+  if (!h || !n) return TTI_ERR_ARG;
+  *n = h->launches;
+  return TTI_OK;
+}
+
+int tti_elapsed_ms(const tti_handle *h, float *ms)
+{
+  if (!h || !ms) return TTI_ERR_ARG;
+  *ms = h->last_ms;
+  return TTI_OK;
+}
+
+int tti_fetch_traces(tti_handle *h, int kind, float *out)
+{
+  if (!h || !out || kind < 0 || kind > 2) return TTI_ERR_ARG;
+  if (!h->d_rec[kind]) return set_err(h, TTI_ERR_ARG, "no receivers of kind %d", kind);
+  CK(h, cudaSetDevice(h->device));
+  const int n = h->nrec[kind], nts = h->nts;
+  std::vector<float> tm((size_t)n * nts);
+  CK(h, cudaMemcpyAsync(tm.data(), h->d_rec[kind], sizeof(float) * tm.size(), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  for (int t = 0; t < nts; ++t)
+    for (int r = 0; r < n; ++r) out[(size_t)r * nts + t] = tm[(size_t)t * n + r];
+  return TTI_OK;
+}
+
+int tti_fetch_field(tti_handle *h, int which, float *out)
+{
+  if (!h || !out || which < 0 || which >= 8) return TTI_ERR_ARG;
+  if (!h->fld[which]) return set_err(h, TTI_ERR_ARG, "field %d is not used by this formulation", which);
+  CK(h, cudaSetDevice(h->device));
+  return copy_out_pitched(h, h->fld[which], out);
+}
+
+int tti_fetch_energy(tti_handle *h, float *ek, float *ep)
+{
+  if (!h || !ek || !ep) return TTI_ERR_ARG;
+  CK(h, cudaSetDevice(h->device));
+  const int nt = h->cfg.nt;
+  std::vector<double> e(2 * (size_t)nt);
+  CK(h, cudaMemcpyAsync(e.data(), h->d_energy, sizeof(double) * e.size(), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  for (int it = 0; it < nt; ++it) {
+    ek[it] = 0.5f * (float)e[2 * (size_t)it] * h->cfg.dx * h->cfg.dz;
+    ep[it] = 0.5f * (float)e[2 * (size_t)it + 1] * h->cfg.dx * h->cfg.dz;
+  }
+  return TTI_OK;
+}
+
+}  // extern "C"

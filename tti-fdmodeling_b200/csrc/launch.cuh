@@ -1,0 +1,64 @@
+// Kernel launch wrappers shared by the C-ABI layer (api.cu).
+#pragma once
+
+#include "ttifd_internal.cuh"
+
+namespace ttifd {
+
+// ---------------- setup ----------------
+struct SetupIn {
+  const float *vp, *vs, *rho, *eps, *delta, *theta;  // padded raw model
+};
+struct SetupOut {
+  float *D, *Beta, *coef1, *coef2, *vp, *vs, *rho, *invrho;
+  float *c11, *c13, *c15, *c33, *c35, *c55;
+  float *sn, *cs, *snv, *csv, *s2, *c2, *s2t;
+};
+// Scalars of the MEAL profile computed on the host with the host libm
+// (exactly as meal.c evaluates them): w[l] = absorbWeight(alpha, l, E).
+struct MealConst {
+  const float *w;  // device, [E + 1]
+  float logR;      // logf(Rcoef)
+  float two_thx, two_thz;   // 2 * E * dx, 2 * E * dz
+  float dx_fpeak, dz_fpeak; // dx * fpeak, dz * fpeak
+  float sqrt3;              // sqrtf(3)
+  float dt;
+};
+void launch_setup(const Grid &g, const SetupIn &in, const SetupOut &out, const MealConst &mc, int variant,
+                  float scalar, int freesurface, cudaStream_t st);
+
+// ---------------- per-step ----------------
+// Source weight tables over the 11 x 11 window (offset (a, b) at a*11+b,
+// a = ix - isx + 5, b = iz - isz + 5), precomputed on the host in the
+// reference's float expression order (coord:674-886).
+struct SourceTables {
+  float k1[121];  // 0.5 w          (stype 1, on sxx/szz)
+  float kx[121];  // 2 alpha rx w   (stype 2/3)
+  float kz[121];  // 2 alpha rz w
+  float k5[121];  // w              (stype 5/6)
+  float k7[121];  // 0.5 sqrt2 w    (stype 7)
+  float q8;       // 0.125 sqrt2    (stype 8)
+};
+
+struct StepArgs {
+  Grid g;
+  Fields f;
+  Params p;
+  float invdx, invdz;
+  int variant;
+  bool exact;
+};
+
+void launch_velocity(const StepArgs &a, cudaStream_t st);
+void launch_stress(const StepArgs &a, cudaStream_t st);
+void launch_free_surface(const StepArgs &a, cudaStream_t st);
+// stage 0: velocity sources (stype 2..8), stage 1: stress source (stype 1)
+void launch_sources(const StepArgs &a, const SourceSet &s, const SourceTables *tab, int stype, int stage, int it,
+                    cudaStream_t st);
+void launch_receivers(const StepArgs &a, const ReceiverSet &r, int seistype, int irec, int *flag, cudaStream_t st);
+void launch_energy(const StepArgs &a, int nz, int nx, double *out2, cudaStream_t st);
+// Pack a snapshot (kind 1..7) of the physical (savew = 0) or padded area
+// into a dense [nx_out][nz_out] buffer.
+void launch_snapshot(const StepArgs &a, int kind, int savew, float *dst, cudaStream_t st);
+
+}  // namespace ttifd

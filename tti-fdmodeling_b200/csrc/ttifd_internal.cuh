@@ -1,0 +1,108 @@
+// Internal declarations of the B200 TTI RSG library (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/ttifd.h"
+
+namespace ttifd {
+
+constexpr int NH = 5;  // half length of the 10th-order RSG operator
+
+// Least-squares RSG coefficients C1..C5 (coord:468-469).
+__host__ __device__ __forceinline__ constexpr float rsg(int k)
+{
+  return k == 0   ? 1.24362739770907f
+         : k == 1 ? -0.114021164233934f
+         : k == 2 ? 0.0272965993810630f
+         : k == 3 ? -0.00699199493927320f
+                  : 0.00132022981661381f;
+}
+
+// Device grid description. Arrays are column-major in x: element (ix, iz) at
+// ix * ldz + iz, ldz = Nz rounded up to 32 floats so every column starts on a
+// 128-byte boundary. Cells iz in [Nz, ldz) are padding and stay zero.
+struct Grid {
+  int Nz, Nx, ldz, E, izStart;
+  size_t n;  // ldz * Nx
+};
+
+// Arithmetic policy. Exact<true> rounds every product and sum separately in
+// the reference's expression order (no FMA contraction), which reproduces a
+// gcc -ffp-contract=off build of the reference bit for bit. Exact<false> lets
+// the compiler contract a*b+c into FMA (one rounding instead of two).
+template <bool X>
+struct Ar;
+template <>
+struct Ar<true> {
+  static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+  static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+  static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+};
+template <>
+struct Ar<false> {
+  static __device__ __forceinline__ float mul(float a, float b) { return a * b; }
+  static __device__ __forceinline__ float add(float a, float b) { return a + b; }
+  static __device__ __forceinline__ float sub(float a, float b) { return a - b; }
+};
+
+struct Fields {
+  float *vx, *vz, *sxx, *szz, *sxz, *txx, *tzz, *txz;
+};
+
+struct Params {
+  const float *coef1, *coef2, *invrho;
+  const float *c11, *c13, *c15, *c33, *c35, *c55;
+  const float *sn, *cs, *snv, *csv;   // coordinate: sin/cos theta (stress / velocity node)
+  const float *s2, *c2, *s2t;         // tensor: sin^2, cos^2, sin 2theta
+};
+
+struct SourceSet {
+  int n;
+  const int *x, *z;  // padded-grid cell of each source
+  const float *w;    // [n][nt]
+  int nt;
+};
+
+struct ReceiverSet {
+  int n[3];
+  const int *x[3], *z[3];  // padded-grid cells
+  float *rec[3];           // time-major on the device: [nts][n]
+};
+
+}  // namespace ttifd
+
+// Host-side handle (C ABI object).
+struct tti_handle {
+  tti_config cfg;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  ttifd::Grid g{};
+  float *fld[8] = {};
+  float *par[TTI_P_COUNT] = {};
+  float invdx = 0, invdz = 0, alpha_src = 0;
+  // geometry
+  int nsrc = 0;
+  int *d_sx = nullptr, *d_sz = nullptr;
+  float *d_src = nullptr;
+  int nrec[3] = {0, 0, 0};
+  int *d_rx[3] = {}, *d_rz[3] = {};
+  float *d_rec[3] = {};
+  int nts = 0;
+  double *d_energy = nullptr;  // [nt][2]
+  int *d_flag = nullptr;       // nonfinite watchdog
+  float *d_snap = nullptr;
+  float *h_snap = nullptr;     // pinned
+  size_t snap_cap = 0;
+  bool have_model = false;
+  int step_index = 0;
+  float last_ms = 0.0f;
+  long long launches = 0;
+  cudaEvent_t pev[8] = {};  // phase events for tti_profile_steps
+  bool exact = false;
+  std::string err;
+};

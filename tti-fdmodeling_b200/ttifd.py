@@ -1,0 +1,231 @@
+"""ctypes binding of the C ABI in include/ttifd.h (libttifd.so).
+
+The product path is C host code calling the CUDA library through the C ABI;
+this module exposes the same calls to Python for the tests and the benchmark.
+It never computes anything itself: when the shared library is missing the
+import of :func:`load` raises, there is no fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libttifd.so")
+
+# status codes
+OK, ERR_ARG, ERR_UNSTABLE, ERR_RANGE, ERR_CUDA, ERR_NOMEM, ERR_NONFINITE, ERR_STATE, ERR_CALLBACK = range(9)
+COORDINATE, TENSOR, BOND = 0, 1, 2
+VARIANTS = {"coordinate_rotation": COORDINATE, "tensor_rotation": TENSOR, "bond_transformation": BOND}
+REC_VX, REC_VZ, REC_P = 0, 1, 2
+F_VX, F_VZ, F_SXX, F_SZZ, F_SXZ, F_TXX, F_TZZ, F_TXZ = range(8)
+PARAMS = ["D", "Beta", "coef1", "coef2", "invrho", "c11", "c13", "c15", "c33", "c35", "c55", "sin", "cos",
+          "sin_v", "cos_v", "sin2", "cos2", "sin_2theta", "vp", "vs", "rho"]
+P = {name: i for i, name in enumerate(PARAMS)}
+
+
+class TTIError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class Config(C.Structure):
+    """tti_config: the getpar keys of the reference drivers."""
+
+    _fields_ = [("variant", C.c_int), ("nz", C.c_int), ("nx", C.c_int), ("nt", C.c_int), ("dx", C.c_float),
+                ("dz", C.c_float), ("dt", C.c_float), ("ealThick", C.c_int), ("eal_alpha", C.c_float),
+                ("freesurface", C.c_int), ("fpeak", C.c_float), ("scalar", C.c_float), ("stype", C.c_int),
+                ("seistype", C.c_int), ("mt", C.c_int), ("wsave", C.c_int), ("savew", C.c_int),
+                ("snap_sample", C.c_int), ("mode", C.c_int), ("energy", C.c_int)]
+
+    DEFAULTS = dict(variant=0, ealThick=30, eal_alpha=-1.0, freesurface=0, scalar=1.0, stype=1, seistype=0, mt=1,
+                    wsave=0, savew=0, snap_sample=1, mode=1, energy=0)
+
+    @classmethod
+    def make(cls, **kw) -> "Config":
+        d = dict(cls.DEFAULTS)
+        d.update(kw)
+        if isinstance(d["variant"], str):
+            d["variant"] = VARIANTS[d["variant"]]
+        return cls(**{k: d[k] for k, _ in cls._fields_})
+
+
+SNAP_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_float), C.c_int, C.c_int)
+
+_FP = C.POINTER(C.c_float)
+_IP = C.POINTER(C.c_int)
+_SIGNATURES = {
+    "create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(Config), C.c_int]),
+    "destroy": (C.c_int, [C.c_void_p]),
+    "last_error": (C.c_char_p, [C.c_void_p]),
+    "grid": (C.c_int, [C.c_void_p, _IP, _IP, _IP]),
+    "upload_model": (C.c_int, [C.c_void_p] + [_FP] * 6),
+    "fetch_param": (C.c_int, [C.c_void_p, C.c_int, _FP]),
+    "set_source": (C.c_int, [C.c_void_p, C.c_int, _IP, _IP, _FP]),
+    "set_receivers": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _IP, _IP]),
+    "run": (C.c_int, [C.c_void_p, SNAP_FN, C.c_void_p]),
+    "reset": (C.c_int, [C.c_void_p]),
+    "step": (C.c_int, [C.c_void_p, C.c_int]),
+    "elapsed_ms": (C.c_int, [C.c_void_p, _FP]),
+    "fetch_traces": (C.c_int, [C.c_void_p, C.c_int, _FP]),
+    "fetch_field": (C.c_int, [C.c_void_p, C.c_int, _FP]),
+    "fetch_energy": (C.c_int, [C.c_void_p, _FP, _FP]),
+    "profile_steps": (C.c_int, [C.c_void_p, C.c_int, _FP]),
+    "kernel_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+}
+
+EXPORTS = ["tti_" + k for k in _SIGNATURES]
+
+_lib = None
+
+
+def load(path: str | None = None) -> C.CDLL:
+    """Loads libttifd.so (raises OSError when it has not been built)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    lib = C.CDLL(path or LIB_PATH)
+    for name, (res, args) in _SIGNATURES.items():
+        fn = getattr(lib, "tti_" + name)
+        fn.restype, fn.argtypes = res, args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _f(a: np.ndarray):
+    return a.ctypes.data_as(_FP)
+
+
+def _i(a: np.ndarray):
+    return a.ctypes.data_as(_IP)
+
+
+class Modeling:
+    """One shot on one GPU: the object behind a tti_handle."""
+
+    prefix = "tti_"
+
+    def __init__(self, device: int = 0, lib: C.CDLL | None = None, **cfg):
+        self.lib = lib or load()
+        self.cfg = Config.make(**cfg)
+        self._h = C.c_void_p()
+        self._call("create", C.byref(self._h), C.byref(self.cfg), device, handle=False)
+        nz, nx, e = C.c_int(), C.c_int(), C.c_int()
+        self._call("grid", self._h, C.byref(nz), C.byref(nx), C.byref(e))
+        self.Nz, self.Nx, self.E = nz.value, nx.value, e.value
+        self.nts = (self.cfg.nt - 1) // self.cfg.mt + 1
+        self._nrec = {}
+
+    # -- plumbing
+    def _fn(self, name):
+        return getattr(self.lib, self.prefix + name)
+
+    def _call(self, name, *args, handle=True):
+        rc = self._fn(name)(*args)
+        if rc != OK:
+            msg = self._fn("last_error")(self._h if handle else None)
+            raise TTIError(rc, (msg or b"").decode(errors="replace"))
+        return rc
+
+    def close(self):
+        if self._h:
+            self._fn("destroy")(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- API
+    def upload_model(self, vp, vs, rho, epsilon, delta, theta):
+        arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (vp, vs, rho, epsilon, delta, theta)]
+        for a in arrs:
+            if a.shape != (self.Nx, self.Nz):
+                raise ValueError(f"model arrays must be padded (Nx, Nz) = {(self.Nx, self.Nz)}, got {a.shape}")
+        self._call("upload_model", self._h, *[_f(a) for a in arrs])
+
+    def fetch_param(self, name) -> np.ndarray:
+        out = np.empty((self.Nx, self.Nz), np.float32)
+        self._call("fetch_param", self._h, P[name] if isinstance(name, str) else name, _f(out))
+        return out
+
+    def set_source(self, posx, posz, wavelets):
+        w = np.ascontiguousarray(np.atleast_2d(wavelets), dtype=np.float32)
+        x = np.ascontiguousarray(np.atleast_1d(posx), dtype=np.int32)
+        z = np.ascontiguousarray(np.atleast_1d(posz), dtype=np.int32)
+        if w.shape != (x.size, self.cfg.nt):
+            raise ValueError("wavelets must be [ntrace][nt]")
+        self._call("set_source", self._h, x.size, _i(x), _i(z), _f(w))
+
+    def set_receivers(self, kind, posx, posz):
+        x = np.ascontiguousarray(posx, dtype=np.int32)
+        z = np.ascontiguousarray(np.broadcast_to(posz, x.shape), dtype=np.int32)
+        self._call("set_receivers", self._h, kind, x.size, _i(x), _i(z))
+        self._nrec[kind] = x.size
+
+    def run(self, snapshot=None):
+        """snapshot(it, kind, array[nx_out, nz_out]) -> None, or None."""
+        if snapshot is None:
+            cb = SNAP_FN()
+        else:
+            def _cb(user, it, kind, data, nzo, nxo):
+                try:
+                    arr = np.ctypeslib.as_array(data, shape=(nxo, nzo)).copy()
+                    snapshot(it, kind, arr)
+                    return 0
+                except Exception:  # abort the run
+                    return 1
+            cb = SNAP_FN(_cb)
+        self._call("run", self._h, cb, None)
+
+    def reset(self):
+        self._call("reset", self._h)
+
+    def step(self, n=1):
+        self._call("step", self._h, n)
+
+    @property
+    def elapsed_ms(self) -> float:
+        v = C.c_float()
+        self._call("elapsed_ms", self._h, C.byref(v))
+        return v.value
+
+    def profile_steps(self, n):
+        """Advances n steps; returns total device ms (velocity, stress, other)."""
+        ms = np.zeros(3, np.float32)
+        self._call("profile_steps", self._h, n, _f(ms))
+        return tuple(float(x) for x in ms)
+
+    @property
+    def kernel_launches(self) -> int:
+        v = C.c_longlong()
+        self._call("kernel_launches", self._h, C.byref(v))
+        return v.value
+
+    def fetch_traces(self, kind) -> np.ndarray:
+        out = np.empty((self._nrec.get(kind, 0), self.nts), np.float32)
+        self._call("fetch_traces", self._h, kind, _f(out))
+        return out
+
+    def fetch_field(self, which) -> np.ndarray:
+        out = np.empty((self.Nx, self.Nz), np.float32)
+        self._call("fetch_field", self._h, which, _f(out))
+        return out
+
+    def fetch_energy(self):
+        ek = np.empty(self.cfg.nt, np.float32)
+        ep = np.empty(self.cfg.nt, np.float32)
+        self._call("fetch_energy", self._h, _f(ek), _f(ep))
+        return ek, ep
