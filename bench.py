@@ -323,8 +323,11 @@ def main():
                     choices=["coordinate_rotation", "tensor_rotation", "bond_transformation"])
     ap.add_argument("--profile-steps", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nx", type=int, default=WORKLOAD["nx"],
+                    help="narrower model for profiler captures (default: the full 7872)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    WORKLOAD["nx"] = args.nx
     rank, world, local_rank = dist_init()
 
     if args.impl == "reference":

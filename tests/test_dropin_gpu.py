@@ -93,7 +93,7 @@ def test_dropin_error_exits(tmp_path, gpu_lib):
                               env=dict(os.environ, TTIFD_QUIET="1"))
 
     r = run([a for a in args if not a.startswith("fpeak=")])
-    assert r.returncode == 1 and "fpeak" in r.stderr
+    assert r.returncode == 1 and "peak frequency" in r.stderr
     r = run(args + ["dt=0.01"])
     assert r.returncode == 1 and "unstable" in r.stderr
     import synthetic
