@@ -193,12 +193,21 @@ def run_ours(args, rank, world, local_rank):
 
     # roofline of the dominant kernel (per-launch algorithmic bytes / event time)
     n = args.profile_steps
-    interior = (h.Nx - 10) * (h.Nz - 5 - h.E)  # freesurface: rows [E, Nz-5)
-    halves = ALG_BYTES_HALF[variant]
-    dom = "stress" if ps >= pv else "velocity"
-    t_launch = (ps if dom == "stress" else pv) / n / 1e3
-    bytes_launch = halves[dom] * interior
     peak, src = peaks()
+    if ps == 0.0:  # one fused kernel per step: a launch is one whole time step
+        dom = "fused"
+        kname = f"k_fused<{variant}>"
+        alg = ALG_BYTES_STEP[variant]
+        units = cells
+        t_launch = pv / n / 1e3
+    else:
+        interior = (h.Nx - 10) * (h.Nz - 5 - h.E)  # freesurface: rows [E, Nz-5)
+        dom = "stress" if ps >= pv else "velocity"
+        kname = f"k_{dom}<{variant}>"
+        alg = ALG_BYTES_HALF[variant][dom]
+        units = interior
+        t_launch = (ps if dom == "stress" else pv) / n / 1e3
+    bytes_launch = alg * units
     achieved = bytes_launch / t_launch / 1e9
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "ncu_traffic.json")
@@ -207,9 +216,9 @@ def run_ours(args, rank, world, local_rank):
             traffic = json.load(open(tfile)).get(variant, {}).get(dom)
         except Exception:
             traffic = None
-    roof = {"bound": "hbm", "kernel": f"k_{dom}<{variant}>", "achieved": achieved, "peak": peak, "unit": "GB/s",
+    roof = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": src, "traffic": traffic,
-            "alg_bytes_per_cell": halves[dom], "cells_per_launch": interior,
+            "alg_bytes_per_cell": alg, "cells_per_launch": units, "launch_ms": t_launch * 1e3,
             "step": {"alg_bytes_per_cell_update": ALG_BYTES_STEP[variant],
                      "achieved_GBps": ALG_BYTES_STEP[variant] * cells * K / (ms / 1e3) / 1e9,
                      "frac": ALG_BYTES_STEP[variant] * cells * K / (ms / 1e3) / 1e9 / peak},

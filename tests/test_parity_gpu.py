@@ -58,3 +58,33 @@ def test_gpu_exact_rounding_mode(name, gpu_lib, monkeypatch):
     case = helpers.load_golden(name)
     got = helpers.run_backend(ttifd.Modeling, case)
     _compare(name, got, helpers.golden_arrays(case), 1e-6, 1e-6)
+
+
+@pytest.mark.parametrize("name", ["coord_fs", "tensor_basic", "bond_thin_rim", "coord_stype4", "bond_stype7"])
+def test_gpu_one_thread_per_cell_path(name, gpu_lib, monkeypatch):
+    """The per-kernel path (used when the free-surface rows do not fit the
+    fused kernel's first band) against the same golden outputs."""
+    import ttifd
+
+    monkeypatch.setenv("TTIFD_KERNEL", "naive")
+    case = helpers.load_golden(name)
+    got = helpers.run_backend(ttifd.Modeling, case)
+    _compare(name, got, helpers.golden_arrays(case), TRACE_RTOL, TRACE_PEAK)
+
+
+@pytest.mark.parametrize("seg", ["16", "23", "40"])
+def test_gpu_fused_segment_lengths(seg, gpu_lib, monkeypatch):
+    """Column-segment boundaries of the fused step must not change results:
+    fused traces at several segment lengths equal the per-kernel path's to
+    the last bit in the exact rounding mode."""
+    import ttifd
+
+    monkeypatch.setenv("TTIFD_EXACT", "1")
+    case = helpers.load_golden("coord_multi_dxdz")
+    monkeypatch.setenv("TTIFD_KERNEL", "naive")
+    ref = helpers.run_backend(ttifd.Modeling, case)
+    monkeypatch.setenv("TTIFD_KERNEL", "fused")
+    monkeypatch.setenv("TTIFD_SEG", seg)
+    got = helpers.run_backend(ttifd.Modeling, case)
+    for k, v in ref.items():
+        assert np.array_equal(np.asarray(got[k]).view(np.uint32), np.asarray(v).view(np.uint32)), k

@@ -7,7 +7,10 @@
 #include <cstring>
 #include <vector>
 
-#include "launch.cuh"
+#include <algorithm>
+#include <numeric>
+
+#include "fused.cuh"
 
 using namespace ttifd;
 
@@ -125,6 +128,47 @@ int launch_one_step(tti_handle *h, const SourceTables &tab, cudaEvent_t *ev = nu
   StepArgs a = step_args(h);
   SourceSet s{h->nsrc, h->d_sx, h->d_sz, h->d_src, c.nt};
   const bool vsrc = s.n > 0 && c.stype >= 2, ssrc = s.n > 0 && c.stype == 1;
+  if (h->use_fused) {
+    fused::FusedArgs fa;
+    fa.g = h->g;
+    fa.old = a.f;
+    fa.nw = Fields{h->fld2[0], h->fld2[1], h->fld2[2], h->fld2[3], h->fld2[4], h->fld2[5], h->fld2[6], h->fld2[7]};
+    fa.p = a.p;
+    fa.invdx = h->invdx;
+    fa.invdz = h->invdz;
+    fa.dt = c.dt;
+    fa.seg = h->seg;
+    fa.stype = c.stype;
+    fa.src = s;
+    fa.tab = tab;
+    fa.it = it;
+    fa.irec = (c.seistype > 0 && it % c.mt == 0) ? it / c.mt : -1;
+    const bool want_v = c.seistype == 1 || c.seistype == 3, want_p = c.seistype == 2 || c.seistype == 3;
+    for (int k = 0; k < 3; ++k) {
+      const bool on = (k < 2 ? want_v : want_p) && h->nrec[k] > 0;
+      fa.rec[k] = fused::RecLookup{on ? h->d_rcol[k] : nullptr, h->d_rzs[k], h->d_rid[k], h->d_rec[k], h->nrec[k]};
+    }
+    fa.freesurface = c.freesurface;
+    fa.undamped_ok = h->undamped_ok;
+    fa.err = h->d_flag;
+    if (ev) CK(h, cudaEventRecord(ev[0], h->stream));
+    CK(h, fused::launch_fused(fa, c.variant, h->exact, h->stream));
+    if (ev) {
+      CK(h, cudaEventRecord(ev[1], h->stream));
+      CK(h, cudaEventRecord(ev[2], h->stream));
+      CK(h, cudaEventRecord(ev[3], h->stream));
+    }
+    h->launches++;
+    std::swap(h->fld, h->fld2);
+    if (c.energy == 1) {
+      launch_energy(step_args(h), c.nz, c.nx, h->d_energy + 2 * (size_t)it, h->stream);
+      h->launches++;
+    }
+    if (ev) CK(h, cudaEventRecord(ev[4], h->stream));
+    CK(h, cudaGetLastError());
+    h->step_index++;
+    return TTI_OK;
+  }
   if (ev) CK(h, cudaEventRecord(ev[0], h->stream));
   launch_velocity(a, h->stream);
   if (ev) CK(h, cudaEventRecord(ev[1], h->stream));
@@ -208,6 +252,7 @@ int check_flag(tti_handle *h)
   int flag = 0;
   CK(h, cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
+  if (flag & 2) return set_err(h, TTI_ERR_CUDA, "a shared-memory copy wait timed out in the fused step kernel");
   if (flag) return set_err(h, TTI_ERR_NONFINITE, "non-finite value recorded at a receiver (unstable run?)");
   return TTI_OK;
 }
@@ -276,8 +321,32 @@ int tti_create(tti_handle **out, const tti_config *cfg, int device)
     set_err(h, TTI_ERR_CUDA, "stream/event creation failed");
     return fail(TTI_ERR_CUDA);
   }
-  for (int f = 0; f < nfields(cfg->variant); ++f)
+  {
+    const char *kern = getenv("TTIFD_KERNEL");
+    const bool naive = kern && strcmp(kern, "naive") == 0;
+    // the fused step needs the free-surface rows E-5 .. E+5 inside the first band
+    h->use_fused = !naive && !(cfg->freesurface == 1 && g.E + NH >= fused::BZ);
+  }
+  for (int f = 0; f < nfields(cfg->variant); ++f) {
     if ((rc = alloc(&h->fld[f]))) return fail(rc);
+    if (h->use_fused && (rc = alloc(&h->fld2[f]))) return fail(rc);
+  }
+  if (h->use_fused) {
+    // columns per CTA: one wave of CTAs over the SMs at the kernel's occupancy
+    int sms = 148, dev = device;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    size_t smem_per_sm = 0;
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    smem_per_sm = (size_t)v;
+    const size_t per_cta = fused::smem_bytes(cfg->variant) + 1024;
+    int occ = (int)std::max<size_t>(1, std::min<size_t>(3, smem_per_sm / per_cta));
+    const int bands = (g.Nz + fused::BZ - 1) / fused::BZ;
+    int nseg = std::max(1, sms * occ / bands);
+    h->seg = std::max(16, (g.Nx + nseg - 1) / nseg);
+    const char *segenv = getenv("TTIFD_SEG");
+    if (segenv && atoi(segenv) > 0) h->seg = atoi(segenv);
+  }
   for (int p = 0; p < TTI_P_COUNT; ++p)
     if (param_used(cfg->variant, p) && (rc = alloc(&h->par[p]))) return fail(rc);
   if (cudaMalloc(&h->d_flag, sizeof(int)) != cudaSuccess ||
@@ -301,11 +370,15 @@ int tti_destroy(tti_handle *h)
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (auto &p : h->fld) cudaFree(p);
+  for (auto &p : h->fld2) cudaFree(p);
   for (auto &p : h->par) cudaFree(p);
   for (int k = 0; k < 3; ++k) {
     cudaFree(h->d_rx[k]);
     cudaFree(h->d_rz[k]);
     cudaFree(h->d_rec[k]);
+    cudaFree(h->d_rcol[k]);
+    cudaFree(h->d_rzs[k]);
+    cudaFree(h->d_rid[k]);
   }
   cudaFree(h->d_sx);
   cudaFree(h->d_sz);
@@ -404,6 +477,21 @@ int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const floa
   cudaStreamSynchronize(h->stream);
   for (auto p : raw) cudaFree(p);
   cudaFree(d_w);
+  if (rc == TTI_OK && h->use_fused) {
+    // the fused step skips coef1/coef2 loads where they are exactly 1 and dt;
+    // verify that on the device instead of assuming the MEAL rim geometry
+    int *cnt = nullptr;
+    int bad = -1;
+    if (cudaMalloc(&cnt, sizeof(int)) == cudaSuccess) {
+      cudaMemsetAsync(cnt, 0, sizeof(int), h->stream);
+      fused::launch_check_undamped(g, h->par[TTI_P_COEF1], h->par[TTI_P_COEF2], c.dt, c.freesurface ? 0 : g.E, cnt,
+                                   h->stream);
+      cudaMemcpyAsync(&bad, cnt, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+      cudaStreamSynchronize(h->stream);
+      cudaFree(cnt);
+    }
+    h->undamped_ok = bad == 0;
+  }
   if (rc == TTI_OK) h->have_model = true;
   return rc;
 }
@@ -485,6 +573,29 @@ int tti_set_receivers(tti_handle *h, int kind, int ntrace, const int *posx, cons
   CK(h, cudaMemcpy(h->d_rx[kind], x.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice));
   CK(h, cudaMemcpy(h->d_rz[kind], z.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice));
   CK(h, cudaMemset(h->d_rec[kind], 0, sizeof(float) * (size_t)ntrace * h->nts));
+  // receivers grouped by padded-grid column for the fused step
+  {
+    const int Nx = h->g.Nx;
+    std::vector<int> order(ntrace), colptr(Nx + 1, 0), zs(ntrace), ids(ntrace);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return x[a] < x[b]; });
+    for (int i = 0; i < ntrace; ++i) colptr[x[i] + 1]++;
+    for (int c = 0; c < Nx; ++c) colptr[c + 1] += colptr[c];
+    for (int i = 0; i < ntrace; ++i) {
+      zs[i] = z[order[i]];
+      ids[i] = order[i];
+    }
+    cudaFree(h->d_rcol[kind]);
+    cudaFree(h->d_rzs[kind]);
+    cudaFree(h->d_rid[kind]);
+    h->d_rcol[kind] = h->d_rzs[kind] = h->d_rid[kind] = nullptr;
+    CK(h, cudaMalloc(&h->d_rcol[kind], sizeof(int) * (Nx + 1)));
+    CK(h, cudaMalloc(&h->d_rzs[kind], sizeof(int) * ntrace));
+    CK(h, cudaMalloc(&h->d_rid[kind], sizeof(int) * ntrace));
+    CK(h, cudaMemcpy(h->d_rcol[kind], colptr.data(), sizeof(int) * (Nx + 1), cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(h->d_rzs[kind], zs.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(h->d_rid[kind], ids.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice));
+  }
   h->nrec[kind] = ntrace;
   return TTI_OK;
 }
@@ -494,6 +605,8 @@ int tti_reset(tti_handle *h)
   if (!h) return TTI_ERR_ARG;
   CK(h, cudaSetDevice(h->device));
   for (auto p : h->fld)
+    if (p) CK(h, cudaMemsetAsync(p, 0, h->g.n * sizeof(float), h->stream));
+  for (auto p : h->fld2)
     if (p) CK(h, cudaMemsetAsync(p, 0, h->g.n * sizeof(float), h->stream));
   for (int k = 0; k < 3; ++k)
     if (h->d_rec[k]) CK(h, cudaMemsetAsync(h->d_rec[k], 0, sizeof(float) * (size_t)h->nrec[k] * h->nts, h->stream));
