@@ -138,16 +138,11 @@ int launch_one_step(tti_handle *h, const SourceTables &tab, cudaEvent_t *ev = nu
     fa.invdz = h->invdz;
     fa.dt = c.dt;
     fa.seg = h->seg;
+    fa.bz = h->bz;
     fa.stype = c.stype;
     fa.src = s;
     fa.tab = tab;
     fa.it = it;
-    fa.irec = (c.seistype > 0 && it % c.mt == 0) ? it / c.mt : -1;
-    const bool want_v = c.seistype == 1 || c.seistype == 3, want_p = c.seistype == 2 || c.seistype == 3;
-    for (int k = 0; k < 3; ++k) {
-      const bool on = (k < 2 ? want_v : want_p) && h->nrec[k] > 0;
-      fa.rec[k] = fused::RecLookup{on ? h->d_rcol[k] : nullptr, h->d_rzs[k], h->d_rid[k], h->d_rec[k], h->nrec[k]};
-    }
     fa.freesurface = c.freesurface;
     fa.undamped_ok = h->undamped_ok;
     fa.err = h->d_flag;
@@ -160,6 +155,17 @@ int launch_one_step(tti_handle *h, const SourceTables &tab, cudaEvent_t *ev = nu
     }
     h->launches++;
     std::swap(h->fld, h->fld2);
+    if (c.seistype > 0 && it % c.mt == 0 && h->nrec[0] + h->nrec[1] + h->nrec[2] > 0) {
+      ReceiverSet r;
+      for (int k = 0; k < 3; ++k) {
+        r.n[k] = h->nrec[k];
+        r.x[k] = h->d_rx[k];
+        r.z[k] = h->d_rz[k];
+        r.rec[k] = h->d_rec[k];
+      }
+      launch_receivers(step_args(h), r, c.seistype, it / c.mt, h->d_flag, h->stream);
+      h->launches++;
+    }
     if (c.energy == 1) {
       launch_energy(step_args(h), c.nz, c.nx, h->d_energy + 2 * (size_t)it, h->stream);
       h->launches++;
@@ -324,8 +330,10 @@ int tti_create(tti_handle **out, const tti_config *cfg, int device)
   {
     const char *kern = getenv("TTIFD_KERNEL");
     const bool naive = kern && strcmp(kern, "naive") == 0;
+    const int bands = (g.Nz + fused::BZ - 1) / fused::BZ;
+    h->bz = (g.Nz + bands - 1) / bands;
     // the fused step needs the free-surface rows E-5 .. E+5 inside the first band
-    h->use_fused = !naive && !(cfg->freesurface == 1 && g.E + NH >= fused::BZ);
+    h->use_fused = !naive && !(cfg->freesurface == 1 && g.E + NH >= h->bz);
   }
   for (int f = 0; f < nfields(cfg->variant); ++f) {
     if ((rc = alloc(&h->fld[f]))) return fail(rc);
@@ -341,7 +349,7 @@ int tti_create(tti_handle **out, const tti_config *cfg, int device)
     smem_per_sm = (size_t)v;
     const size_t per_cta = fused::smem_bytes(cfg->variant) + 1024;
     int occ = (int)std::max<size_t>(1, std::min<size_t>(3, smem_per_sm / per_cta));
-    const int bands = (g.Nz + fused::BZ - 1) / fused::BZ;
+    const int bands = (g.Nz + h->bz - 1) / h->bz;
     int nseg = std::max(1, sms * occ / bands);
     h->seg = std::max(16, (g.Nx + nseg - 1) / nseg);
     const char *segenv = getenv("TTIFD_SEG");
@@ -677,9 +685,14 @@ int tti_profile_steps(tti_handle *h, int nsteps, float ms[3])
     CK(h, cudaEventElapsedTime(&t12, h->pev[1], h->pev[2]));
     CK(h, cudaEventElapsedTime(&t23, h->pev[2], h->pev[3]));
     CK(h, cudaEventElapsedTime(&t34, h->pev[3], h->pev[4]));
-    ms[0] += t01;
-    ms[1] += t23;
-    ms[2] += t12 + t34;
+    if (h->use_fused) {  // one step kernel: ev[1..3] are recorded back to back
+      ms[0] += t01;
+      ms[2] += t12 + t23 + t34;
+    } else {
+      ms[0] += t01;
+      ms[1] += t23;
+      ms[2] += t12 + t34;
+    }
   }
   return check_flag(h);
 }

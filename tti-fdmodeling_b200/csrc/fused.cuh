@@ -6,20 +6,12 @@
 namespace ttifd {
 namespace fused {
 
-constexpr int BZ = 128;    // rows owned by a CTA (= threads per CTA)
-constexpr int SR = BZ + 24;  // stress rows staged: [z0-12, z0+BZ+12)
-constexpr int VR = BZ + 16;  // velocity rows staged/computed: [z0-8, z0+BZ+8)
-constexpr int NV = 10;       // velocity ring columns (stencil width)
-constexpr int P = 4;         // copy stages in flight
-constexpr int R = P + 9;     // stress ring columns (stencil width + prefetch)
-
-// Receivers of one component grouped by padded-grid column:
-// entries colptr[x] .. colptr[x+1]-1 hold row z[] and trace index id[].
-struct RecLookup {
-  const int *colptr, *z, *id;
-  float *out;  // time-major [irec][n]
-  int n;
-};
+constexpr int NT = 224;      // threads per CTA: one velocity row each
+constexpr int BZ = NT - 10;  // rows owned by a CTA (velocity rows add a 5-row halo each side)
+constexpr int SR = 240;      // stress rows staged: [floor4(z0-9), ceil4(z0+BZ+10)) <= BZ + 25
+constexpr int NV = 11;       // velocity ring columns (stencil width + 1: no end-of-column barrier)
+constexpr int P = 4;         // stress columns in flight ahead of use
+constexpr int R = P + 10;    // stress ring columns (stencil width + prefetch + 1)
 
 struct FusedArgs {
   Grid g;
@@ -27,12 +19,11 @@ struct FusedArgs {
   Params p;
   float invdx, invdz, dt;
   int seg;  // columns per CTA
+  int bz;   // rows per band (<= BZ; bands balanced over Nz)
   int stype;
   SourceSet src;  // padded-grid positions
   SourceTables tab;
   int it;
-  int irec;  // receiver sample index of this step, -1 when not recording
-  RecLookup rec[3];
   int freesurface;
   int undamped_ok;  // coef1 == 1 and coef2 == dt verified outside the rims
   int *err;         // bit 2: a copy wait timed out

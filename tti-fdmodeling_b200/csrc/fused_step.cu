@@ -1,21 +1,25 @@
 // One kernel per time step: velocity half-step, velocity sources, stress
 // half-step, free surface, stress source and receiver sampling fused.
 //
-// Work decomposition: a CTA owns a band of BZ rows (z, the contiguous axis)
-// and a segment of columns [x0, x1) and marches along x. At iteration j it
+// Work decomposition: a CTA of NT = 224 threads owns a band of at most BZ = 214 rows
+// (z, the contiguous axis) and a segment of columns [x0, x1), and marches
+// along x. At iteration j it
 //   1. computes v_new for column xv = x0 - 5 + j over rows [z0-5, z0+BZ+5)
-//      (its band plus the 5-row halo the stress stencil needs) from the
-//      stress columns xv-4 .. xv+5 held in a shared-memory ring,
-//   2. computes sigma_new for column xs = xv - 4 over its own rows from the
-//      v_new columns xs-5 .. xs+4 held in a second ring.
-// Stress columns, v_old and the per-cell parameters of the columns in use
-// arrive through cp.async.bulk copies (one elected thread, completion on an
-// mbarrier per stage) issued P iterations ahead. State is double buffered
-// (old -> new) so halo rows and columns read by one CTA are never written by
-// another during the step.
+//      (one row per thread: its band plus the 5-row halo the stress stencil
+//      needs) from the stress columns xv-4 .. xv+5 held in a shared ring,
+//   2. computes sigma_new for column xs = xv - 4 over its own BZ rows from the
+//      v_new columns xs-5 .. xs+4 held in a second shared ring.
+// Stress columns arrive by cp.async.bulk (one elected thread; completion on a
+// per-column mbarrier that every thread tests before use) P columns ahead;
+// the per-cell parameters and v_old, read once each, are loaded into
+// registers one iteration ahead. One CTA barrier per column: the velocity
+// ring has NV = 11 slots and the stress ring R = P + 10, so a slot is only
+// refilled after the barrier that follows its last read.
+// State is double buffered (old -> new): the halo rows and columns a CTA
+// reads are never written during the step.
 //
 // Per-cell arithmetic is the reference's (coord:614-886, tensor:617-895,
-// bond:654-913) with the same policy as the one-thread-per-cell kernels.
+// bond:654-913) under the same rounding policy as the per-kernel path.
 #include "fused.cuh"
 
 namespace ttifd {
@@ -66,19 +70,14 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned by
 
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-template <int V>
-struct Lay {
-  static constexpr int NVP = V == TTI_COORDINATE ? 5 : 3;  // coef1 coef2 invrho [sinv cosv]
-  static constexpr int NSP = V == TTI_TENSOR ? 9 : 8;      // coef1 coef2 + moduli / angles
-  static constexpr int NTAU = V == TTI_TENSOR ? 3 : 0;
-  static constexpr int STAGE = 2 * VR + NVP * VR + NSP * BZ + NTAU * BZ;  // floats
-  static constexpr int SRING = R * 3 * SR;
-  static constexpr int VRING = NV * 2 * VR;
-  static constexpr int FLOATS = SRING + VRING + P * STAGE + 32;
-  static constexpr size_t BYTES = FLOATS * sizeof(float) + (P + 1) * sizeof(unsigned long long);
-};
+constexpr int COLS = 3 * SR;  // floats per stress column (sxx, szz, sxz)
+constexpr int COLV = 2 * NT;  // floats per velocity column (vx, vz)
+constexpr int SMEM_FLOATS = R * COLS + NV * COLV + 32;
+constexpr size_t SMEM_BYTES = SMEM_FLOATS * sizeof(float) + R * sizeof(unsigned long long);
+static_assert(SMEM_FLOATS % 2 == 0, "mbarriers need 8-byte alignment");
+static_assert(BZ + 25 <= SR, "stress ring rows");
 
-// source table and receiver lookup (kernel parameters)
+// velocity sources (stype 2..8) on one cell, in the reference's order
 __device__ __forceinline__ void vsource_cell(const FusedArgs &a, int x, int z, float &vx, float &vz)
 {
   const int st = a.stype;
@@ -88,8 +87,7 @@ __device__ __forceinline__ void vsource_cell(const FusedArgs &a, int x, int z, f
     for (int n = 0; n < a.src.n; ++n) {
       const int dx = x - a.src.x[n], dz = z - a.src.z[n];
       if (dx < -1 || dx > 0 || dz < -1 || dz > 0) continue;
-      const float s = __ldg(a.src.w + (size_t)n * a.src.nt + a.it);
-      const float qs = __fmul_rn(q, s);
+      const float qs = __fmul_rn(q, __ldg(a.src.w + (size_t)n * a.src.nt + a.it));
       if (dx == 0 && dz == 0) {
         vx = __fsub_rn(vx, qs);
         vz = __fadd_rn(vz, qs);
@@ -106,7 +104,7 @@ __device__ __forceinline__ void vsource_cell(const FusedArgs &a, int x, int z, f
     }
     return;
   }
-  // passes in the reference's block order: divergence, then curl, then forces
+  // divergence pass over all sources, then the curl pass (stype 4), or the force
   for (int pass = 0; pass < 2; ++pass) {
     int kind;
     if (pass == 0) kind = (st == 2 || st == 4) ? 2 : (st == 3 ? 3 : (st >= 5 ? st : 0));
@@ -141,272 +139,252 @@ __device__ __forceinline__ void vsource_cell(const FusedArgs &a, int x, int z, f
   }
 }
 
-__device__ __forceinline__ void record(const FusedArgs &a, int kind, int x, int z, float v)
+// per-cell inputs read once, prefetched one iteration ahead
+struct VIn {
+  float vx, vz, c1, c2, ir, sv, cv;
+};
+struct SIn {
+  float c1, c2, m[7], tau[3];
+};
+
+template <int V>
+__device__ __forceinline__ void load_v(const FusedArgs &a, bool ok, bool und, size_t i, VIn &o)
 {
-  const RecLookup &L = a.rec[kind];
-  if (L.colptr == nullptr) return;
-  const int b = __ldg(L.colptr + x), e = __ldg(L.colptr + x + 1);
-  for (int j = b; j < e; ++j)
-    if (__ldg(L.z + j) == z) L.out[(size_t)a.irec * L.n + __ldg(L.id + j)] = v;
+  if (!ok) return;
+  o.vx = __ldg(a.old.vx + i);
+  o.vz = __ldg(a.old.vz + i);
+  o.c1 = und ? 1.0f : __ldg(a.p.coef1 + i);
+  o.c2 = und ? a.dt : __ldg(a.p.coef2 + i);
+  o.ir = __ldg(a.p.invrho + i);
+  if (V == TTI_COORDINATE) {
+    o.sv = __ldg(a.p.snv + i);
+    o.cv = __ldg(a.p.csv + i);
+  }
+}
+
+// m[] holds, coordinate: c11 c13 c33 c55 sin cos; tensor: c11 c13 c33 c55 s2 c2 s2t;
+// bond: c11 c13 c15 c33 c35 c55
+template <int V>
+__device__ __forceinline__ void load_s(const FusedArgs &a, bool ok, bool und, size_t i, SIn &o)
+{
+  if (!ok) return;
+  o.c1 = und ? 1.0f : __ldg(a.p.coef1 + i);
+  o.c2 = und ? a.dt : __ldg(a.p.coef2 + i);
+  o.m[0] = __ldg(a.p.c11 + i);
+  o.m[1] = __ldg(a.p.c13 + i);
+  if (V == TTI_BOND) {
+    o.m[2] = __ldg(a.p.c15 + i);
+    o.m[3] = __ldg(a.p.c33 + i);
+    o.m[4] = __ldg(a.p.c35 + i);
+    o.m[5] = __ldg(a.p.c55 + i);
+  } else {
+    o.m[2] = __ldg(a.p.c33 + i);
+    o.m[3] = __ldg(a.p.c55 + i);
+    if (V == TTI_COORDINATE) {
+      o.m[4] = __ldg(a.p.sn + i);
+      o.m[5] = __ldg(a.p.cs + i);
+    } else {
+      o.m[4] = __ldg(a.p.s2 + i);
+      o.m[5] = __ldg(a.p.c2 + i);
+      o.m[6] = __ldg(a.p.s2t + i);
+      o.tau[0] = __ldg(a.old.txx + i);
+      o.tau[1] = __ldg(a.old.tzz + i);
+      o.tau[2] = __ldg(a.old.txz + i);
+    }
+  }
 }
 
 template <int V, bool X>
-__global__ void __launch_bounds__(BZ, 3) k_fused(const __grid_constant__ FusedArgs a)
+__global__ void __launch_bounds__(NT, 3) k_fused(const __grid_constant__ FusedArgs a)
 {
   using A = Ar<X>;
-  using Ly = Lay<V>;
-  // shared memory: stress ring [R][3][SR] (row z at z - (z0 - 12)), velocity
-  // ring [NV][2][VR] (row z at z - (z0 - 8)), P copy stages, the free-surface
-  // exchange rows, then P + 1 mbarriers (stages, prologue)
+  // shared memory: stress ring [R][3][SR] (row s at s - sbase), velocity ring
+  // [NV][2][NT] (row r at r - (z0 - 5)), free-surface exchange, R mbarriers
   extern __shared__ __align__(128) float smem[];
-  float *sring = smem;
-  float *vring = sring + Ly::SRING;
-  float *stage = vring + Ly::VRING;
-  float *fsbuf = stage + P * Ly::STAGE;
-  unsigned long long *bar = reinterpret_cast<unsigned long long *>(smem + Ly::FLOATS);
+  float *fsbuf = smem + R * COLS + NV * COLV;
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(smem + SMEM_FLOATS);
+  constexpr int VOFF = R * COLS;  // start of the velocity ring
 
   const Grid &g = a.g;
   const int t = threadIdx.x;
-  const int z0 = blockIdx.y * BZ;
+  const int bz = a.bz;  // rows owned by this CTA's band (<= BZ)
+  const int z0 = blockIdx.y * bz;
   const int x0 = blockIdx.x * a.seg, x1 = min(x0 + a.seg, g.Nx);
   const int L = g.ldz;
   const int niter = (x1 - x0) + 9;  // xv = x0-5 .. x1+3
-  const int xbeg = x0 - 5;
-  // Undamped CTA: every cell it touches has D = 0, so coef1 = 1 and
-  // coef2 = dt exactly (meal.c:486-487 with D = 0); those loads are skipped.
-  const bool und = a.undamped_ok && (xbeg - 4 >= g.E) && (x1 + 3 + 5 < g.Nx - g.E) &&
-                   (z0 - 9 >= (a.freesurface ? 0 : g.E)) && (z0 + BZ + 9 < g.Nz - g.E);
+  const int ncol = niter + 9;       // stress columns x0-9 .. x1+8
+  const int sbase = (z0 - 9) & ~3;  // first staged stress row (16-byte aligned)
+  const int s_lo = max(sbase, 0), s_hi = min((z0 + bz + 10 + 3) & ~3, L);
+  // Undamped CTA: every coefficient it reads is outside the MEAL rims, where
+  // D = 0 makes coef1 = 1 and coef2 = dt exactly (meal.c:486-487).
+  const bool und = a.undamped_ok && (x0 - 5 >= g.E) && (x1 + 3 < g.Nx - g.E) &&
+                   (z0 - 5 >= (a.freesurface ? 0 : g.E)) && (z0 + bz + 5 < g.Nz - g.E);
   const bool fs_band = a.freesurface && z0 == 0;
 
-  // row ranges (clamped, 16-byte aligned) of the three kinds of column loads
-  const int s_lo = max(z0 - 12, 0), s_hi = min(z0 + BZ + 12, L);
-  const int v_lo = max(z0 - 8, 0), v_hi = min(z0 + BZ + 8, L);
-  const int p_lo = z0, p_hi = min(z0 + BZ, L);
-
-  auto ring_slot = [](int c, int n) { return (c + n * 4096) % n; };
-
-  // one elected thread issues the copies of iteration j into stage j % P
-  auto issue = [&](int j) {
-    unsigned long long *b = bar + (j % P);
-    float *st = stage + (j % P) * Ly::STAGE;
-    const int xv = xbeg + j, cs = xv + 5, xs = xv - 4;
-    unsigned bytes = 0;
-    // pass 1: byte count (expect_tx must precede the copies)
-    const bool has_s = cs >= 0 && cs < g.Nx;
-    const bool has_v = xv >= 0 && xv < g.Nx;
-    const bool has_p = xs >= x0 && xs < x1;
-    const unsigned sb = (s_hi - s_lo) * 4u, vb = (v_hi - v_lo) * 4u, pb = (p_hi - p_lo) * 4u;
-    if (has_s) bytes += 3 * sb;
-    if (has_v) bytes += (2 + Ly::NVP - (und ? 2 : 0)) * vb;
-    if (has_p) bytes += (Ly::NSP - (und ? 2 : 0) + Ly::NTAU) * pb;
-    mbar_arrive_expect_tx(b, bytes);
-    if (has_s) {
-      float *dst = sring + ring_slot(cs, R) * 3 * SR + (s_lo - (z0 - 12));
-      const size_t off = (size_t)cs * L + s_lo;
-      bulk_g2s(dst, a.old.sxx + off, sb, b);
-      bulk_g2s(dst + SR, a.old.szz + off, sb, b);
-      bulk_g2s(dst + 2 * SR, a.old.sxz + off, sb, b);
+  // stress column q (x = x0 - 9 + q) into ring slot q % R, mbarrier q % R
+  auto issue_col = [&](int q) {
+    unsigned long long *b = bar + (q % R);
+    const int c = x0 - 9 + q;
+    if (c < 0 || c >= g.Nx || s_hi <= s_lo) {
+      mbar_arrive_expect_tx(b, 0);
+      return;
     }
-    if (has_v) {
-      const size_t off = (size_t)xv * L + v_lo;
-      float *dst = st + (v_lo - (z0 - 8));
-      bulk_g2s(dst, a.old.vx + off, vb, b);
-      bulk_g2s(dst + VR, a.old.vz + off, vb, b);
-      float *pv = dst + 2 * VR;
-      if (!und) {
-        bulk_g2s(pv, a.p.coef1 + off, vb, b);
-        bulk_g2s(pv + VR, a.p.coef2 + off, vb, b);
-      }
-      bulk_g2s(pv + 2 * VR, a.p.invrho + off, vb, b);
-      if (V == TTI_COORDINATE) {
-        bulk_g2s(pv + 3 * VR, a.p.snv + off, vb, b);
-        bulk_g2s(pv + 4 * VR, a.p.csv + off, vb, b);
-      }
-    }
-    if (has_p) {
-      const size_t off = (size_t)xs * L + p_lo;
-      float *dst = st + (2 + Ly::NVP) * VR + (p_lo - z0);
-      const float *src[12];
-      int n = 0;
-      src[n++] = a.p.coef1;
-      src[n++] = a.p.coef2;
-      src[n++] = a.p.c11;
-      src[n++] = a.p.c13;
-      if (V == TTI_BOND) src[n++] = a.p.c15;
-      src[n++] = a.p.c33;
-      if (V == TTI_BOND) src[n++] = a.p.c35;
-      src[n++] = a.p.c55;
-      if (V == TTI_COORDINATE) {
-        src[n++] = a.p.sn;
-        src[n++] = a.p.cs;
-      }
-      if (V == TTI_TENSOR) {
-        src[n++] = a.p.s2;
-        src[n++] = a.p.c2;
-        src[n++] = a.p.s2t;
-        src[n++] = a.old.txx;
-        src[n++] = a.old.tzz;
-        src[n++] = a.old.txz;
-      }
-      for (int k = und ? 2 : 0; k < n; ++k) bulk_g2s(dst + k * BZ, src[k] + off, pb, b);
+    const unsigned sb = (s_hi - s_lo) * 4u;
+    mbar_arrive_expect_tx(b, 3 * sb);
+    float *dst = smem + (q % R) * COLS + (s_lo - sbase);
+    const size_t off = (size_t)c * L + s_lo;
+    bulk_g2s(dst, a.old.sxx + off, sb, b);
+    bulk_g2s(dst + SR, a.old.szz + off, sb, b);
+    bulk_g2s(dst + 2 * SR, a.old.sxz + off, sb, b);
+  };
+  // each thread tests the column's mbarrier itself (a single poll once the
+  // copy has landed); a timeout is voted at the next CTA barrier
+  auto wait_col = [&](int q) -> bool { return mbar_wait(bar + (q % R), (q / R) & 1); };
+  // on a timed-out wait: flag it, give copies in flight a bounded time, leave
+  auto bail = [&](int first) {
+    if (t == 0) {
+      atomicOr(a.err, 2);
+      for (int q = first; q < first + R && q < ncol; ++q) mbar_wait(bar + (q % R), (q / R) & 1, 1u << 14);
     }
   };
 
   if (t == 0) {
-    for (int k = 0; k <= P; ++k) mbar_init(bar + k, 1);
+    for (int k = 0; k < R; ++k) mbar_init(bar + k, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  if (t == 0) {
-    // prologue: stress columns x0-9 .. x0-1 (read by the first stencils)
-    unsigned long long *b = bar + P;
-    const unsigned sb = (s_hi - s_lo) * 4u;
-    unsigned bytes = 0;
-    for (int c = x0 - 9; c < x0; ++c)
-      if (c >= 0 && c < g.Nx) bytes += 3 * sb;
-    mbar_arrive_expect_tx(b, bytes);
-    for (int c = x0 - 9; c < x0; ++c) {
-      if (c < 0 || c >= g.Nx) continue;
-      float *dst = sring + ring_slot(c, R) * 3 * SR + (s_lo - (z0 - 12));
-      const size_t off = (size_t)c * L + s_lo;
-      bulk_g2s(dst, a.old.sxx + off, sb, b);
-      bulk_g2s(dst + SR, a.old.szz + off, sb, b);
-      bulk_g2s(dst + 2 * SR, a.old.sxz + off, sb, b);
-    }
-    for (int j = 0; j < P && j < niter; ++j) issue(j);
-  }
-  // On a timed-out wait: flag it, give the copies still in flight a bounded
-  // time to land, and leave.
-  auto bail = [&](int first_pending) {
-    if (t == 0) {
-      atomicOr(a.err, 2);
-      for (int j = first_pending; j < first_pending + P && j < niter; ++j)
-        mbar_wait(bar + (j % P), (j / P) & 1, 1u << 16);
-    }
-  };
-  bool ok = mbar_wait(bar + P, 0);
-  if (__syncthreads_or(!ok)) {
-    bail(0);
-    return;
+  if (t == 0)
+    for (int q = 0; q < P + 9 && q < ncol; ++q) issue_col(q);
+
+  // thread roles
+  const int r = z0 - 5 + t;  // velocity row
+  const bool r_ok = t < bz + 10 && r >= 0 && r < g.Nz;
+  const bool r_in = r >= g.izStart && r < g.Nz - NH;
+  const bool r_own = t >= 5 && t < bz + 5 && r < g.Nz;
+  const int z = z0 + t;  // stress row (t < bz)
+  const bool z_ok = t < bz && z < g.Nz;
+  const bool z_in = z_ok && z >= g.izStart && z < g.Nz - NH;
+  const int srow = r - sbase;  // this thread's velocity row in the stress ring
+  const int zrow = z - sbase;  // this thread's stress row in the stress ring
+
+  VIn va{}, vb{};
+  SIn sa{}, sb{};
+  {
+    const int xv = x0 - 5, xs = xv - 4;
+    load_v<V>(a, r_ok && xv >= 0 && xv < g.Nx, und, (size_t)xv * L + r, va);
+    load_s<V>(a, z_ok && xs >= x0 && xs < x1, und, (size_t)xs * L + z, sa);
   }
 
-  const float dt = a.dt;
-  for (int j = 0; j < niter; ++j) {
-    ok = mbar_wait(bar + (j % P), (j / P) & 1);
+  {
+    bool ok = true;
+    for (int q = 0; q < 9 && q < ncol; ++q) ok = wait_col(q) && ok;
     if (__syncthreads_or(!ok)) {
-      bail(j);
+      bail(0);
       return;
     }
-    const float *st = stage + (j % P) * Ly::STAGE;
-    const int xv = xbeg + j, xs = xv - 4;
+  }
 
-    // ---------------- velocity half-step at column xv
-    if (xv >= 0 && xv < g.Nx) {
-      const bool xin = xv >= NH && xv < g.Nx - NH;
-      const bool own_x = xv >= x0 && xv < x1;
-      float *vr = vring + ring_slot(xv, NV) * 2 * VR;
-      const float *sbase[10];
+  // one march iteration; `vin/sin_` hold this iteration's inputs, `vnx/snx`
+  // receive the next one's (two register sets alternate: no copies)
+  auto body = [&](int j, const VIn &vin, const SIn &sin_, VIn &vnx, SIn &snx) -> bool {
+    const int xv = x0 - 5 + j, xs = xv - 4;
+    const int s13 = j % R, v10 = j % NV;
+    load_v<V>(a, r_ok && xv + 1 < g.Nx && xv + 1 >= 0 && j + 1 < niter, und, (size_t)(xv + 1) * L + r, vnx);
+    load_s<V>(a, z_ok && xs + 1 >= x0 && xs + 1 < x1, und, (size_t)(xs + 1) * L + z, snx);
+    const bool ok = wait_col(j + 9);
+
+    // ---------------- velocity half-step at column xv, row r
+    if (xv >= 0 && xv < g.Nx && r_ok) {
+      float vx = vin.vx, vz = vin.vz;
+      if (r_in && xv >= NH && xv < g.Nx - NH) {
+        // stress column xv+m (m = -4..5) sits in ring slot (s13 + m + 4) % R
+        int cb[10];
 #pragma unroll
-      for (int k = 0; k < 10; ++k) sbase[k] = sring + ring_slot(xv - 4 + k, R) * 3 * SR;
-      for (int pass = 0; pass < 2; ++pass) {
-        int r;
-        if (pass == 0) r = z0 + t;
-        else if (t < 5) r = z0 - 5 + t;
-        else if (t < 10) r = z0 + BZ + (t - 5);
-        else break;
-        if (r < 0 || r >= g.Nz) continue;
-        const int iv = r - (z0 - 8);  // index in v rows
-        float vx = st[iv], vz = st[VR + iv];
-        if (xin && r >= g.izStart && r < g.Nz - NH) {
-          const int is = r - (z0 - 12);  // index in sigma rows
-          // d1 = sum C_k (s[x+k][z+k] - s[x-k+1][z-k+1]), d2 = sum C_k (s[x+k][z-k+1] - s[x-k+1][z+k]);
-          // column xv+m lives in sbase[m+4]
-          float d[3][2];
+        for (int k = 0; k < 10; ++k) cb[k] = (s13 + k >= R ? s13 + k - R : s13 + k) * COLS + srow;
+        float d[3][2];
 #pragma unroll
-          for (int f = 0; f < 3; ++f) {
-            float s1 = A::mul(rsg(0), A::sub(sbase[5][f * SR + is + 1], sbase[4][f * SR + is]));
-            float s2 = A::mul(rsg(0), A::sub(sbase[5][f * SR + is], sbase[4][f * SR + is + 1]));
+        for (int f = 0; f < 3; ++f) {
+          const int o = f * SR;
+          // d1 = sum C_k (s[x+k][z+k] - s[x-k+1][z-k+1]); d2 = sum C_k (s[x+k][z-k+1] - s[x-k+1][z+k])
+          float s1 = A::mul(rsg(0), A::sub(smem[cb[5] + o + 1], smem[cb[4] + o]));
+          float s2 = A::mul(rsg(0), A::sub(smem[cb[5] + o], smem[cb[4] + o + 1]));
 #pragma unroll
-            for (int k = 2; k <= NH; ++k) {
-              s1 = A::add(s1, A::mul(rsg(k - 1), A::sub(sbase[4 + k][f * SR + is + k],
-                                                         sbase[5 - k][f * SR + is - k + 1])));
-              s2 = A::add(s2, A::mul(rsg(k - 1), A::sub(sbase[4 + k][f * SR + is - k + 1],
-                                                         sbase[5 - k][f * SR + is + k])));
-            }
-            d[f][0] = s1;
-            d[f][1] = s2;
+          for (int k = 2; k <= NH; ++k) {
+            s1 = A::add(s1, A::mul(rsg(k - 1), A::sub(smem[cb[4 + k] + o + k], smem[cb[5 - k] + o - k + 1])));
+            s2 = A::add(s2, A::mul(rsg(k - 1), A::sub(smem[cb[4 + k] + o - k + 1], smem[cb[5 - k] + o + k])));
           }
-          const float *pv = st + 2 * VR;
-          const float c1 = und ? 1.0f : pv[iv], c2 = und ? dt : pv[VR + iv], ir = pv[2 * VR + iv];
-          const float invdx = a.invdx, invdz = a.invdz;
-          const float sxx_x = A::mul(A::mul(0.5f, A::add(d[0][0], d[0][1])), invdx);
-          const float szz_z = A::mul(A::mul(0.5f, A::sub(d[1][0], d[1][1])), invdz);
-          const float sxz_x = A::mul(A::mul(0.5f, A::add(d[2][0], d[2][1])), invdx);
-          const float sxz_z = A::mul(A::mul(0.5f, A::sub(d[2][0], d[2][1])), invdz);
-          const float br = A::mul(c2, ir);
-          float fx, fz;
-          if (V == TTI_COORDINATE) {
-            const float sxx_z = A::mul(A::mul(0.5f, A::sub(d[0][0], d[0][1])), invdx);  // coord:633
-            const float szz_x = A::mul(A::mul(0.5f, A::add(d[1][0], d[1][1])), invdx);
-            const float sv = pv[3 * VR + iv], cv = pv[4 * VR + iv];
-            fx = A::add(A::add(A::sub(A::mul(cv, sxx_x), A::mul(sv, sxx_z)), A::mul(sv, sxz_x)), A::mul(cv, sxz_z));
-            fz = A::add(A::add(A::sub(A::mul(cv, sxz_x), A::mul(sv, sxz_z)), A::mul(sv, szz_x)), A::mul(cv, szz_z));
-          } else {
-            fx = A::add(sxx_x, sxz_z);
-            fz = A::add(sxz_x, szz_z);
-          }
-          vx = A::add(A::mul(c1, vx), A::mul(br, fx));
-          vz = A::add(A::mul(c1, vz), A::mul(br, fz));
+          d[f][0] = s1;
+          d[f][1] = s2;
         }
-        vsource_cell(a, xv, r, vx, vz);
-        vr[iv] = vx;
-        vr[VR + iv] = vz;
-        if (own_x && pass == 0) {
-          const size_t gi = (size_t)xv * L + r;
-          a.nw.vx[gi] = vx;
-          a.nw.vz[gi] = vz;
-          if (a.irec >= 0) {
-            record(a, TTI_REC_VX, xv, r, vx);
-            record(a, TTI_REC_VZ, xv, r, vz);
-          }
+        const float invdx = a.invdx, invdz = a.invdz;
+        const float sxx_x = A::mul(A::mul(0.5f, A::add(d[0][0], d[0][1])), invdx);
+        const float szz_z = A::mul(A::mul(0.5f, A::sub(d[1][0], d[1][1])), invdz);
+        const float sxz_x = A::mul(A::mul(0.5f, A::add(d[2][0], d[2][1])), invdx);
+        const float sxz_z = A::mul(A::mul(0.5f, A::sub(d[2][0], d[2][1])), invdz);
+        const float br = A::mul(vin.c2, vin.ir);
+        float fx, fz;
+        if (V == TTI_COORDINATE) {
+          const float sxx_z = A::mul(A::mul(0.5f, A::sub(d[0][0], d[0][1])), invdx);  // invdx as coord:633
+          const float szz_x = A::mul(A::mul(0.5f, A::add(d[1][0], d[1][1])), invdx);
+          const float sv = vin.sv, cv = vin.cv;
+          fx = A::add(A::add(A::sub(A::mul(cv, sxx_x), A::mul(sv, sxx_z)), A::mul(sv, sxz_x)), A::mul(cv, sxz_z));
+          fz = A::add(A::add(A::sub(A::mul(cv, sxz_x), A::mul(sv, sxz_z)), A::mul(sv, szz_x)), A::mul(cv, szz_z));
+        } else {
+          fx = A::add(sxx_x, sxz_z);
+          fz = A::add(sxz_x, szz_z);
         }
+        vx = A::add(A::mul(vin.c1, vx), A::mul(br, fx));
+        vz = A::add(A::mul(vin.c1, vz), A::mul(br, fz));
+      }
+      vsource_cell(a, xv, r, vx, vz);
+      smem[VOFF + v10 * COLV + t] = vx;
+      smem[VOFF + v10 * COLV + NT + t] = vz;
+      if (r_own && xv >= x0 && xv < x1) {
+        const size_t gi = (size_t)xv * L + r;
+        a.nw.vx[gi] = vx;
+        a.nw.vz[gi] = vz;
       }
     }
-    __syncthreads();
+    // the one CTA barrier per column: v_new of column xv visible; every read
+    // of stress column xs - 1 (previous column) is done, so its slot refills
+    if (__syncthreads_or(!ok)) {
+      bail(j + 9);
+      return false;
+    }
+    if (t == 0 && j + 9 + P < ncol) {
+      fence_proxy_async();
+      issue_col(j + 9 + P);  // slot of column q = j - 1
+    }
 
-    // ---------------- stress half-step at column xs
+    // ---------------- stress half-step at column xs, row z
     const bool do_s = xs >= x0 && xs < x1;
-    const int z = z0 + t;
     float sxx = 0.f, szz = 0.f, sxz = 0.f, txx = 0.f, tzz = 0.f, txz = 0.f;
-    const bool row_ok = z < g.Nz;
-    const bool sin_ = do_s && row_ok && xs >= NH && xs < g.Nx - NH && z >= g.izStart && z < g.Nz - NH;
-    if (do_s && row_ok) {
-      const float *so = sring + ring_slot(xs, R) * 3 * SR + (z - (z0 - 12));
-      sxx = so[0];
-      szz = so[SR];
-      sxz = so[2 * SR];
-      const float *sp = st + (2 + Ly::NVP) * VR + t;
+    if (do_s && z_ok) {
+      const int so = s13 * COLS + zrow;  // stress column xs = xv - 4
+      sxx = smem[so];
+      szz = smem[so + SR];
+      sxz = smem[so + 2 * SR];
       if (V == TTI_TENSOR) {
-        txx = sp[(Ly::NSP + 0) * BZ];
-        tzz = sp[(Ly::NSP + 1) * BZ];
-        txz = sp[(Ly::NSP + 2) * BZ];
+        txx = sin_.tau[0];
+        tzz = sin_.tau[1];
+        txz = sin_.tau[2];
       }
-      if (sin_) {
-        const float *vb[10];
+      if (z_in && xs >= NH && xs < g.Nx - NH) {
+        // velocity column xs+m (m = -5..4) sits in ring slot (v10 + 2 + m + 5) % NV; row z at t + 5
+        int cb[10];
 #pragma unroll
-        for (int k = 0; k < 10; ++k) vb[k] = vring + ring_slot(xs - 5 + k, NV) * 2 * VR;
-        // column xs+m lives in vb[m+5]; row z at index iv
-        const int iv = z - (z0 - 8);
+        for (int k = 0; k < 10; ++k) cb[k] = VOFF + (v10 + 2 + k >= NV ? v10 + 2 + k - NV : v10 + 2 + k) * COLV + t + 5;
         float d[2][2];
 #pragma unroll
         for (int f = 0; f < 2; ++f) {
-          // d1 = sum C_k (v[x+k-1][z+k-1] - v[x-k][z-k]), d2 = sum C_k (v[x+k-1][z-k] - v[x-k][z+k-1])
-          float s1 = A::mul(rsg(0), A::sub(vb[5][f * VR + iv], vb[4][f * VR + iv - 1]));
-          float s2 = A::mul(rsg(0), A::sub(vb[5][f * VR + iv - 1], vb[4][f * VR + iv]));
+          const int o = f * NT;
+          // d1 = sum C_k (v[x+k-1][z+k-1] - v[x-k][z-k]); d2 = sum C_k (v[x+k-1][z-k] - v[x-k][z+k-1])
+          float s1 = A::mul(rsg(0), A::sub(smem[cb[5] + o], smem[cb[4] + o - 1]));
+          float s2 = A::mul(rsg(0), A::sub(smem[cb[5] + o - 1], smem[cb[4] + o]));
 #pragma unroll
           for (int k = 2; k <= NH; ++k) {
-            s1 = A::add(s1, A::mul(rsg(k - 1), A::sub(vb[4 + k][f * VR + iv + k - 1], vb[5 - k][f * VR + iv - k])));
-            s2 = A::add(s2, A::mul(rsg(k - 1), A::sub(vb[4 + k][f * VR + iv - k], vb[5 - k][f * VR + iv + k - 1])));
+            s1 = A::add(s1, A::mul(rsg(k - 1), A::sub(smem[cb[4 + k] + o + k - 1], smem[cb[5 - k] + o - k])));
+            s2 = A::add(s2, A::mul(rsg(k - 1), A::sub(smem[cb[4 + k] + o - k], smem[cb[5 - k] + o + k - 1])));
           }
           d[f][0] = s1;
           d[f][1] = s2;
@@ -416,21 +394,21 @@ __global__ void __launch_bounds__(BZ, 3) k_fused(const __grid_constant__ FusedAr
         float vxz = A::mul(A::mul(0.5f, A::sub(d[0][0], d[0][1])), invdz);
         float vzx = A::mul(A::mul(0.5f, A::add(d[1][0], d[1][1])), invdx);
         float vzz = A::mul(A::mul(0.5f, A::sub(d[1][0], d[1][1])), invdz);
-        const float c1 = und ? 1.0f : sp[0], c2 = und ? dt : sp[BZ];
-        const float c11 = sp[2 * BZ], c13 = sp[3 * BZ];
+        const float c1 = sin_.c1, c2 = sin_.c2;
+        const float *m = sin_.m;
         if (V == TTI_COORDINATE) {
-          const float c33 = sp[4 * BZ], c55 = sp[5 * BZ], s = sp[6 * BZ], c = sp[7 * BZ];
-          float r = A::add(A::mul(s, vxx), A::mul(c, vxz));
+          const float c11 = m[0], c13 = m[1], c33 = m[2], c55 = m[3], s = m[4], c = m[5];
+          float q = A::add(A::mul(s, vxx), A::mul(c, vxz));
           vxx = A::sub(A::mul(c, vxx), A::mul(s, vxz));
-          vxz = r;
-          r = A::add(A::mul(s, vzx), A::mul(c, vzz));
+          vxz = q;
+          q = A::add(A::mul(s, vzx), A::mul(c, vzz));
           vzx = A::sub(A::mul(c, vzx), A::mul(s, vzz));
-          vzz = r;
+          vzz = q;
           sxx = A::add(A::mul(c1, sxx), A::mul(c2, A::add(A::mul(c11, vxx), A::mul(c13, vzz))));
           szz = A::add(A::mul(c1, szz), A::mul(c2, A::add(A::mul(c13, vxx), A::mul(c33, vzz))));
           sxz = A::add(A::mul(c1, sxz), A::mul(A::mul(c2, c55), A::add(vzx, vxz)));
         } else if (V == TTI_TENSOR) {
-          const float c33 = sp[4 * BZ], c55 = sp[5 * BZ], s2 = sp[6 * BZ], cc2 = sp[7 * BZ], s2t = sp[8 * BZ];
+          const float c11 = m[0], c13 = m[1], c33 = m[2], c55 = m[3], s2 = m[4], cc2 = m[5], s2t = m[6];
           const float sh = A::add(vxz, vzx);
           const float exx = A::sub(A::add(A::mul(cc2, vxx), A::mul(s2, vzz)), A::mul(A::mul(0.5f, s2t), sh));
           const float ezz = A::add(A::add(A::mul(s2, vxx), A::mul(cc2, vzz)), A::mul(A::mul(0.5f, s2t), sh));
@@ -442,7 +420,7 @@ __global__ void __launch_bounds__(BZ, 3) k_fused(const __grid_constant__ FusedAr
           szz = A::sub(A::add(A::mul(s2, txx), A::mul(cc2, tzz)), A::mul(s2t, txz));
           sxz = A::add(A::mul(A::mul(-0.5f, s2t), A::sub(txx, tzz)), A::mul(A::sub(cc2, s2), txz));
         } else {
-          const float c15 = sp[4 * BZ], c33 = sp[5 * BZ], c35 = sp[6 * BZ], c55 = sp[7 * BZ];
+          const float c11 = m[0], c13 = m[1], c15 = m[2], c33 = m[3], c35 = m[4], c55 = m[5];
           const float sh = A::add(vzx, vxz);
           sxx = A::add(A::mul(c1, sxx), A::mul(c2, A::add(A::add(A::mul(c11, vxx), A::mul(c13, vzz)), A::mul(c15, sh))));
           szz = A::add(A::mul(c1, szz), A::mul(c2, A::add(A::add(A::mul(c13, vxx), A::mul(c33, vzz)), A::mul(c35, sh))));
@@ -450,17 +428,17 @@ __global__ void __launch_bounds__(BZ, 3) k_fused(const __grid_constant__ FusedAr
         }
       }
     }
-    // free surface: stress image about row E (coord:847-863) for interior columns
+    // free surface: stress image about row E for interior columns (coord:847-863)
     if (fs_band) {
       const int E = g.izStart;
       const bool col_fs = do_s && xs >= NH && xs < g.Nx - NH;
-      if (col_fs && z >= E && z <= E + NH) {
+      if (col_fs && z_ok && z >= E && z <= E + NH) {
         fsbuf[z - E] = sxx;
         fsbuf[8 + z - E] = szz;
         fsbuf[16 + z - E] = sxz;
       }
       __syncthreads();
-      if (col_fs) {
+      if (col_fs && z_ok) {
         if (z == E) {
           szz = 0.0f;
           sxz = 0.0f;
@@ -472,15 +450,13 @@ __global__ void __launch_bounds__(BZ, 3) k_fused(const __grid_constant__ FusedAr
         }
       }
     }
-    if (do_s && row_ok) {
-      // stress source (stype 1), after the free surface (coord:865-886)
-      if (a.stype == 1) {
+    if (do_s && z_ok) {
+      if (a.stype == 1) {  // stress source after the free surface (coord:865-886)
         for (int n = 0; n < a.src.n; ++n) {
           const int dx = xs - a.src.x[n], dz = z - a.src.z[n];
           if (dx < -NH || dx > NH || dz < -NH || dz > NH) continue;
-          const float w = a.tab.k1[(dx + NH) * 11 + (dz + NH)];
-          const float s = __ldg(a.src.w + (size_t)n * a.src.nt + a.it);
-          const float ws = __fmul_rn(w, s);
+          const float ws = __fmul_rn(a.tab.k1[(dx + NH) * 11 + (dz + NH)],
+                                     __ldg(a.src.w + (size_t)n * a.src.nt + a.it));
           sxx = __fadd_rn(sxx, ws);
           szz = __fadd_rn(szz, ws);
           if (V == TTI_TENSOR) {
@@ -494,23 +470,19 @@ __global__ void __launch_bounds__(BZ, 3) k_fused(const __grid_constant__ FusedAr
       a.nw.szz[gi] = szz;
       a.nw.sxz[gi] = sxz;
       if (V == TTI_TENSOR) {
-        // tau is only updated in the interior; elsewhere it keeps its value
-        // plus the stype-1 source (tensor:871-895)
         a.nw.txx[gi] = txx;
         a.nw.tzz[gi] = tzz;
         a.nw.txz[gi] = txz;
       }
-      if (a.irec >= 0) record(a, TTI_REC_P, xs, z, __fmul_rn(0.5f, __fadd_rn(sxx, szz)));
     }
-    __syncthreads();
-    if (t == 0 && j + P < niter) {
-      fence_proxy_async();
-      issue(j + P);
-    }
+    return true;
+  };
+
+  for (int j = 0; j < niter; j += 2) {
+    if (!body(j, va, sa, vb, sb)) return;
+    if (j + 1 < niter && !body(j + 1, vb, sb, va, sa)) return;
   }
 }
-
-}  // namespace
 
 __global__ void k_check_undamped(Grid g, const float *__restrict__ c1, const float *__restrict__ c2, float dt,
                                  int zD, int *count)
@@ -525,6 +497,8 @@ __global__ void k_check_undamped(Grid g, const float *__restrict__ c1, const flo
   if (threadIdx.x == 0 && bad) atomicAdd(count, bad);
 }
 
+}  // namespace
+
 void launch_check_undamped(const Grid &g, const float *coef1, const float *coef2, float dt, int zD, int *count,
                            cudaStream_t st)
 {
@@ -533,27 +507,19 @@ void launch_check_undamped(const Grid &g, const float *coef1, const float *coef2
   k_check_undamped<<<dim3(1, nx), 256, 0, st>>>(g, coef1, coef2, dt, zD, count);
 }
 
-size_t smem_bytes(int variant)
-{
-  switch (variant) {
-  case TTI_COORDINATE: return Lay<TTI_COORDINATE>::BYTES;
-  case TTI_TENSOR: return Lay<TTI_TENSOR>::BYTES;
-  default: return Lay<TTI_BOND>::BYTES;
-  }
-}
+size_t smem_bytes(int) { return SMEM_BYTES; }
 
 template <int V, bool X>
 static cudaError_t launch_t(const FusedArgs &a, cudaStream_t st)
 {
-  const size_t bytes = Lay<V>::BYTES;
-  static bool configured = false;  // per template instance, per process
+  static bool configured = false;  // per template instance
   if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k_fused<V, X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaError_t e = cudaFuncSetAttribute(k_fused<V, X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  const dim3 grid((a.g.Nx + a.seg - 1) / a.seg, (a.g.Nz + BZ - 1) / BZ);
-  k_fused<V, X><<<grid, BZ, bytes, st>>>(a);
+  const dim3 grid((a.g.Nx + a.seg - 1) / a.seg, (a.g.Nz + a.bz - 1) / a.bz);
+  k_fused<V, X><<<grid, NT, SMEM_BYTES, st>>>(a);
   return cudaGetLastError();
 }
 

@@ -86,6 +86,7 @@ struct tti_handle {
   float *fld2[8] = {};  // second set: the fused step reads fld and writes fld2, then swaps
   bool use_fused = false;
   int seg = 0;          // columns per CTA of the fused step
+  int bz = 0;           // rows per band of the fused step
   int undamped_ok = 0;  // coef1 == 1, coef2 == dt outside the absorbing rims (checked at upload)
   int *d_rcol[3] = {}, *d_rzs[3] = {}, *d_rid[3] = {};  // receivers grouped by column
   float *par[TTI_P_COUNT] = {};
