@@ -128,12 +128,13 @@ int launch_one_step(tti_handle *h, const SourceTables &tab, cudaEvent_t *ev = nu
   StepArgs a = step_args(h);
   SourceSet s{h->nsrc, h->d_sx, h->d_sz, h->d_src, c.nt};
   const bool vsrc = s.n > 0 && c.stype >= 2, ssrc = s.n > 0 && c.stype == 1;
-  if (h->use_fused) {
+  if (h->use_fused && h->nsrc <= fused::MAXSRC) {
     fused::FusedArgs fa;
     fa.g = h->g;
     fa.old = a.f;
     fa.nw = Fields{h->fld2[0], h->fld2[1], h->fld2[2], h->fld2[3], h->fld2[4], h->fld2[5], h->fld2[6], h->fld2[7]};
     fa.p = a.p;
+    fa.pk = fused::Packed{h->pk_cf, h->pk_vsc, h->pk_sc, h->pk_c4};
     fa.invdx = h->invdx;
     fa.invdz = h->invdz;
     fa.dt = c.dt;
@@ -340,6 +341,14 @@ int tti_create(tti_handle **out, const tti_config *cfg, int device)
     if (h->use_fused && (rc = alloc(&h->fld2[f]))) return fail(rc);
   }
   if (h->use_fused) {
+    bool okp = cudaMalloc(&h->pk_cf, g.n * sizeof(float2)) == cudaSuccess &&
+               cudaMalloc(&h->pk_sc, g.n * sizeof(float2)) == cudaSuccess &&
+               cudaMalloc(&h->pk_c4, g.n * sizeof(float4)) == cudaSuccess &&
+               (cfg->variant != TTI_COORDINATE || cudaMalloc(&h->pk_vsc, g.n * sizeof(float2)) == cudaSuccess);
+    if (!okp) {
+      set_err(h, TTI_ERR_NOMEM, "device allocation of the packed parameters failed");
+      return fail(TTI_ERR_NOMEM);
+    }
     // columns per CTA: one wave of CTAs over the SMs at the kernel's occupancy
     int sms = 148, dev = device;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -349,6 +358,8 @@ int tti_create(tti_handle **out, const tti_config *cfg, int device)
     smem_per_sm = (size_t)v;
     const size_t per_cta = fused::smem_bytes(cfg->variant) + 1024;
     int occ = (int)std::max<size_t>(1, std::min<size_t>(3, smem_per_sm / per_cta));
+    const char *occenv = getenv("TTIFD_CTAS_PER_SM");
+    if (occenv && atoi(occenv) > 0) occ = atoi(occenv);
     const int bands = (g.Nz + h->bz - 1) / h->bz;
     int nseg = std::max(1, sms * occ / bands);
     h->seg = std::max(16, (g.Nx + nseg - 1) / nseg);
@@ -391,6 +402,10 @@ int tti_destroy(tti_handle *h)
   cudaFree(h->d_sx);
   cudaFree(h->d_sz);
   cudaFree(h->d_src);
+  cudaFree(h->pk_cf);
+  cudaFree(h->pk_vsc);
+  cudaFree(h->pk_sc);
+  cudaFree(h->pk_c4);
   cudaFree(h->d_energy);
   cudaFree(h->d_flag);
   cudaFree(h->d_snap);
@@ -485,6 +500,12 @@ int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const floa
   cudaStreamSynchronize(h->stream);
   for (auto p : raw) cudaFree(p);
   cudaFree(d_w);
+  if (rc == TTI_OK && h->use_fused) {
+    fused::launch_pack(g, step_args(h).p, fused::Packed{h->pk_cf, h->pk_vsc, h->pk_sc, h->pk_c4}, c.variant,
+                       h->stream);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) rc = set_err(h, TTI_ERR_CUDA, "packing parameters: %s", cudaGetErrorString(e));
+  }
   if (rc == TTI_OK && h->use_fused) {
     // the fused step skips coef1/coef2 loads where they are exactly 1 and dt;
     // verify that on the device instead of assuming the MEAL rim geometry

@@ -89,6 +89,8 @@ struct tti_handle {
   int bz = 0;           // rows per band of the fused step
   int undamped_ok = 0;  // coef1 == 1, coef2 == dt outside the absorbing rims (checked at upload)
   int *d_rcol[3] = {}, *d_rzs[3] = {}, *d_rid[3] = {};  // receivers grouped by column
+  float2 *pk_cf = nullptr, *pk_vsc = nullptr, *pk_sc = nullptr;  // packed parameters (fused step)
+  float4 *pk_c4 = nullptr;
   float *par[TTI_P_COUNT] = {};
   float invdx = 0, invdz = 0, alpha_src = 0;
   // geometry
