@@ -164,6 +164,18 @@ int tti_profile_steps(tti_handle *h, int nsteps, float ms[3]);
 /* Number of kernels this handle has launched since tti_create. */
 int tti_kernel_launches(const tti_handle *h, long long *n);
 
+/* Snapshot of the current wavefield without allocating device memory (no
+ * counterpart in the reference). For callers that cannot allocate at the point
+ * of the call, e.g. while a stream is being captured or under a fixed GPU
+ * memory budget. `kind` as for tti_snapshot_fn; `out` receives nx_out records
+ * of nz_out floats. The field is packed in a static device array of 16 Mi
+ * floats (64 MiB per GPU, held from the library's first use on a device until
+ * process exit); larger snapshots fail with TTI_ERR_ARG. Calls share that
+ * array: calls whose GPU work overlaps race. The first call on each device
+ * resolves the array's device address and should come before any stream
+ * capture. */
+int tti_snapshot_static(tti_handle *h, int kind, float *out);
+
 /* Recorded traces of one component, [ntrace][(nt-1)/mt+1] (Receiver2D.recv). */
 int tti_fetch_traces(tti_handle *h, int kind, float *out);
 /* Current wavefield ([Nx][Nz]). */

@@ -275,6 +275,11 @@ int copy_out_pitched(tti_handle *h, const float *src, float *out)
 
 }  // namespace
 
+namespace ttifd {
+StepArgs handle_step_args(const tti_handle *h) { return step_args(h); }
+int handle_error(tti_handle *h, int code, const char *msg) { return set_err(h, code, "%s", msg); }
+}  // namespace ttifd
+
 extern "C" {
 
 const char *tti_last_error(const tti_handle *h) { return h ? h->err.c_str() : g_create_error.c_str(); }

@@ -61,4 +61,8 @@ void launch_energy(const StepArgs &a, int nz, int nx, double *out2, cudaStream_t
 // into a dense [nx_out][nz_out] buffer.
 void launch_snapshot(const StepArgs &a, int kind, int savew, float *dst, cudaStream_t st);
 
+// C-ABI helpers shared by the entry points in other translation units
+StepArgs handle_step_args(const tti_handle *h);
+int handle_error(tti_handle *h, int code, const char *msg);
+
 }  // namespace ttifd

@@ -75,6 +75,7 @@ _SIGNATURES = {
     "fetch_energy": (C.c_int, [C.c_void_p, _FP, _FP]),
     "profile_steps": (C.c_int, [C.c_void_p, C.c_int, _FP]),
     "kernel_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    "snapshot_static": (C.c_int, [C.c_void_p, C.c_int, _FP]),
 }
 
 EXPORTS = ["tti_" + k for k in _SIGNATURES]
@@ -213,6 +214,16 @@ class Modeling:
         v = C.c_longlong()
         self._call("kernel_launches", self._h, C.byref(v))
         return v.value
+
+    def snapshot_static(self, kind) -> np.ndarray:
+        """Snapshot through tti_snapshot_static (no device allocation)."""
+        if self.cfg.savew == 0:
+            shape = (self.Nx - 2 * self.E, self.Nz - 2 * self.E)
+        else:
+            shape = (self.Nx, self.Nz)
+        out = np.empty(shape, np.float32)
+        self._call("snapshot_static", self._h, kind, _f(out))
+        return out
 
     def fetch_traces(self, kind) -> np.ndarray:
         out = np.empty((self._nrec.get(kind, 0), self.nts), np.float32)
