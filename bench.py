@@ -286,40 +286,23 @@ def run_reference_cpu(variant: str, budget_s: float = 20.0, max_steps: int = 400
 
 
 # ---------------------------------------------------------------- distributed
-_PG = None
+_G = None  # shots.Group
 
 
 def dist_init():
-    global _PG
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    if world > 1:
-        import datetime
+    global _G
+    import shots
 
-        import torch
-        import torch.distributed as dist
-
-        backend = "nccl" if torch.cuda.is_available() else "gloo"
-        if backend == "nccl":
-            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
-        _PG = dist
-    return int(os.environ.get("RANK", "0")), world, int(os.environ.get("LOCAL_RANK", "0"))
+    _G = shots.Group(timeout_s=300)
+    return _G.rank, _G.world, _G.local_rank
 
 
 def dist_barrier():
-    if _PG is not None:
-        _PG.barrier()
+    _G.barrier()
 
 
 def dist_max(x: float) -> float:
-    if _PG is None:
-        return x
-    import torch
-
-    dev = "cuda" if torch.cuda.is_available() else "cpu"
-    t = torch.tensor([x], dtype=torch.float64, device=dev)
-    _PG.all_reduce(t, op=_PG.ReduceOp.MAX)
-    return float(t.item())
+    return _G.max(x)
 
 
 def main():
@@ -354,8 +337,7 @@ def main():
                         "e2e": {"value": cb["value"], "unit": "Gcell/s", "h2d_bytes_per_step": 0,
                                 "d2h_bytes_per_step": 0}}
                 print(json.dumps(line), flush=True)
-        if _PG is not None:
-            _PG.destroy_process_group()
+        _G.close()
         return
 
     line = run_ours(args, rank, world, local_rank)
@@ -366,8 +348,7 @@ def main():
             except Exception as e:  # reported, not fatal
                 line["cpu_baseline"] = {"error": str(e)[:300]}
         print(json.dumps(line), flush=True)
-    if _PG is not None:
-        _PG.destroy_process_group()
+    _G.close()
 
 
 if __name__ == "__main__":

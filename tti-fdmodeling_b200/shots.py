@@ -1,0 +1,73 @@
+"""Shot sharding across ranks (one process per GPU).
+
+Shots are independent in forward modelling (no exchange during propagation),
+so a multi-GPU run gives each rank its own shots and needs no collective on
+the data path. The collectives here are host-side plumbing over
+torch.distributed: a barrier, the max over ranks of a timing, the sum of a
+per-rank quantity, and gathering per-shot results on rank 0.
+"""
+from __future__ import annotations
+
+import datetime
+import os
+
+
+def assign(n_shots: int, rank: int, world: int) -> list[int]:
+    """Contiguous block of shot indices for `rank` (sizes differ by at most one)."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("bad rank/world")
+    base, extra = divmod(n_shots, world)
+    start = rank * base + min(rank, extra)
+    return list(range(start, start + base + (1 if rank < extra else 0)))
+
+
+class Group:
+    """torch.distributed process group (or a single process when WORLD_SIZE is 1)."""
+
+    def __init__(self, backend: str | None = None, timeout_s: int = 300):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.dist = None
+        self.device = "cpu"
+        if self.world > 1:
+            import torch
+            import torch.distributed as dist
+
+            if backend is None:
+                backend = "nccl" if torch.cuda.is_available() else "gloo"
+            if backend == "nccl":
+                torch.cuda.set_device(self.local_rank)
+                self.device = f"cuda:{self.local_rank}"
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+            self.dist = dist
+
+    def barrier(self) -> None:
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def _reduce(self, x: float, op) -> float:
+        import torch
+
+        t = torch.tensor([float(x)], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    def max(self, x: float) -> float:
+        return x if self.dist is None else self._reduce(x, self.dist.ReduceOp.MAX)
+
+    def sum(self, x: float) -> float:
+        return x if self.dist is None else self._reduce(x, self.dist.ReduceOp.SUM)
+
+    def gather(self, obj):
+        """List of every rank's `obj` on rank 0 (None elsewhere)."""
+        if self.dist is None:
+            return [obj]
+        out = [None] * self.world if self.rank == 0 else None
+        self.dist.gather_object(obj, out, dst=0)
+        return out
+
+    def close(self) -> None:
+        if self.dist is not None:
+            self.dist.destroy_process_group()
+            self.dist = None
