@@ -1,5 +1,6 @@
-"""Fused single-kernel step vs the one-thread-per-cell kernels on grids with
-several 128-row bands and many column segments. In the exact rounding mode
+"""Fused single-kernel step and tiled half-step kernels vs the
+one-thread-per-cell kernels on grids with several bands / tiles and many
+column segments. In the exact rounding mode
 both paths perform the same operations in the same order, so the wavefields,
 traces and snapshots must be bit-identical."""
 import numpy as np
@@ -40,11 +41,12 @@ def _run(kernel, monkeypatch, variant, fs, stype, nz=300, nx=260, nt=160, seg=No
     return out
 
 
+@pytest.mark.parametrize("path", ["fused", "tiled"])
 @pytest.mark.parametrize("variant", ["coordinate_rotation", "tensor_rotation", "bond_transformation"])
 @pytest.mark.parametrize("fs,stype", [(0, 1), (1, 1), (1, 4), (0, 8)])
-def test_fused_equals_per_kernel_path(variant, fs, stype, monkeypatch, gpu_lib):
+def test_fused_and_tiled_equal_per_kernel_path(path, variant, fs, stype, monkeypatch, gpu_lib):
     ref = _run("naive", monkeypatch, variant, fs, stype)
-    got = _run("fused", monkeypatch, variant, fs, stype, seg=37)
+    got = _run(path, monkeypatch, variant, fs, stype, seg=37)
     assert ref.keys() == got.keys()
     for k in ref:
         a, b = np.asarray(got[k]), np.asarray(ref[k])

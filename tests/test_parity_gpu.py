@@ -72,6 +72,17 @@ def test_gpu_one_thread_per_cell_path(name, gpu_lib, monkeypatch):
     _compare(name, got, helpers.golden_arrays(case), TRACE_RTOL, TRACE_PEAK)
 
 
+@pytest.mark.parametrize("name", ["coord_fs", "tensor_stype6", "bond_fs", "coord_multi_dxdz"])
+def test_gpu_fused_path(name, gpu_lib, monkeypatch):
+    """The single-kernel step against the golden outputs."""
+    import ttifd
+
+    monkeypatch.setenv("TTIFD_KERNEL", "fused")
+    case = helpers.load_golden(name)
+    got = helpers.run_backend(ttifd.Modeling, case)
+    _compare(name, got, helpers.golden_arrays(case), TRACE_RTOL, TRACE_PEAK)
+
+
 @pytest.mark.parametrize("seg", ["16", "23", "40"])
 def test_gpu_fused_segment_lengths(seg, gpu_lib, monkeypatch):
     """Column-segment boundaries of the fused step must not change results:

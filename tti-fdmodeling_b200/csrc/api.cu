@@ -10,7 +10,7 @@
 #include <algorithm>
 #include <numeric>
 
-#include "fused.cuh"
+#include "tiled.cuh"
 
 using namespace ttifd;
 
@@ -176,31 +176,63 @@ int launch_one_step(tti_handle *h, const SourceTables &tab, cudaEvent_t *ev = nu
     h->step_index++;
     return TTI_OK;
   }
+  tiled::HalfArgs ha;
+  if (h->use_tiled) {
+    const CUtensorMap *tm = static_cast<const CUtensorMap *>(h->tmaps);
+    ha.g = h->g;
+    ha.f = a.f;
+    ha.p = a.p;
+    ha.pk = fused::Packed{h->pk_cf, h->pk_vsc, h->pk_sc, h->pk_c4};
+    ha.invdx = h->invdx;
+    ha.invdz = h->invdz;
+    ha.dt = c.dt;
+    ha.x_base = NH;
+    ha.undamped_ok = h->undamped_ok;
+    ha.freesurface = c.freesurface;
+    ha.err = h->d_flag;
+    ha.map[0] = tm[2];  // sxx szz sxz for the velocity update
+    ha.map[1] = tm[3];
+    ha.map[2] = tm[4];
+  }
   if (ev) CK(h, cudaEventRecord(ev[0], h->stream));
-  launch_velocity(a, h->stream);
+  if (h->use_tiled) CK(h, tiled::launch_velocity(ha, c.variant, h->exact, h->stream));
+  else launch_velocity(a, h->stream);
   if (ev) CK(h, cudaEventRecord(ev[1], h->stream));
   if (vsrc) launch_sources(a, s, &tab, c.stype, 0, it, h->stream);
   if (ev) CK(h, cudaEventRecord(ev[2], h->stream));
-  launch_stress(a, h->stream);
-  if (ev) CK(h, cudaEventRecord(ev[3], h->stream));
-  h->launches += 2 + vsrc + ssrc;
-  if (c.freesurface == 1) {
-    launch_free_surface(a, h->stream);
-    h->launches++;
+  if (h->use_tiled) {
+    const CUtensorMap *tm = static_cast<const CUtensorMap *>(h->tmaps);
+    ha.map[0] = tm[0];  // vx vz for the stress update
+    ha.map[1] = tm[1];
+    CK(h, tiled::launch_stress(ha, c.variant, h->exact, h->stream));
+  } else {
+    launch_stress(a, h->stream);
   }
-  if (ssrc) launch_sources(a, s, &tab, c.stype, 1, it, h->stream);
-  if (c.seistype > 0 && it % c.mt == 0) {
-    ReceiverSet r;
+  if (ev) CK(h, cudaEventRecord(ev[3], h->stream));
+  h->launches += 2 + vsrc;
+  // free surface, stress source and receivers: one column-parallel launch
+  const bool rec_now = c.seistype > 0 && it % c.mt == 0 && h->nrec[0] + h->nrec[1] + h->nrec[2] > 0;
+  if (c.freesurface == 1 || ssrc || rec_now) {
+    PostArgs pa;
+    pa.freesurface = c.freesurface;
+    pa.stype = ssrc ? 1 : 0;
+    pa.tensor = c.variant == TTI_TENSOR;
+    pa.it = it;
+    pa.irec = rec_now ? it / c.mt : -1;
+    pa.src = s;
+    memcpy(pa.k1, tab.k1, sizeof pa.k1);
+    const bool want_v = c.seistype == 1 || c.seistype == 3, want_p = c.seistype == 2 || c.seistype == 3;
     for (int k = 0; k < 3; ++k) {
-      r.n[k] = h->nrec[k];
-      r.x[k] = h->d_rx[k];
-      r.z[k] = h->d_rz[k];
-      r.rec[k] = h->d_rec[k];
+      const bool on = (k < 2 ? want_v : want_p) && h->nrec[k] > 0;
+      pa.colptr[k] = on ? h->d_rcol[k] : nullptr;
+      pa.rz[k] = h->d_rzs[k];
+      pa.rid[k] = h->d_rid[k];
+      pa.rec[k] = h->d_rec[k];
+      pa.nrec[k] = h->nrec[k];
     }
-    if (r.n[0] + r.n[1] + r.n[2] > 0) {
-      launch_receivers(a, r, c.seistype, it / c.mt, h->d_flag, h->stream);
-      h->launches++;
-    }
+    pa.flag = h->d_flag;
+    launch_post(a, pa, h->stream);
+    h->launches++;
   }
   if (c.energy == 1) {
     launch_energy(a, c.nz, c.nx, h->d_energy + 2 * (size_t)it, h->stream);
@@ -336,16 +368,33 @@ int tti_create(tti_handle **out, const tti_config *cfg, int device)
   {
     const char *kern = getenv("TTIFD_KERNEL");
     const bool naive = kern && strcmp(kern, "naive") == 0;
+    const bool fused_req = kern && strcmp(kern, "fused") == 0;
     const int bands = (g.Nz + fused::BZ - 1) / fused::BZ;
     h->bz = (g.Nz + bands - 1) / bands;
     // the fused step needs the free-surface rows E-5 .. E+5 inside the first band
-    h->use_fused = !naive && !(cfg->freesurface == 1 && g.E + NH >= h->bz);
+    // default: the tiled half-step kernels; `fused` selects the single-kernel step
+    h->use_fused = fused_req && !(cfg->freesurface == 1 && g.E + NH >= h->bz);
+    h->use_tiled = !naive && !h->use_fused;
   }
   for (int f = 0; f < nfields(cfg->variant); ++f) {
     if ((rc = alloc(&h->fld[f]))) return fail(rc);
     if (h->use_fused && (rc = alloc(&h->fld2[f]))) return fail(rc);
   }
-  if (h->use_fused) {
+  if (h->use_tiled) {
+    void *mem = nullptr;
+    if (posix_memalign(&mem, 64, 5 * sizeof(CUtensorMap)) != 0) {
+      set_err(h, TTI_ERR_NOMEM, "host allocation failed");
+      return fail(TTI_ERR_NOMEM);
+    }
+    h->tmaps = mem;
+    CUtensorMap *tm = static_cast<CUtensorMap *>(mem);
+    for (int k = 0; k < 5; ++k)
+      if (!tiled::encode_map(tm + k, g, h->fld[k])) {
+        set_err(h, TTI_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+        return fail(TTI_ERR_CUDA);
+      }
+  }
+  if (h->use_fused || h->use_tiled) {
     bool okp = cudaMalloc(&h->pk_cf, g.n * sizeof(float2)) == cudaSuccess &&
                cudaMalloc(&h->pk_sc, g.n * sizeof(float2)) == cudaSuccess &&
                cudaMalloc(&h->pk_c4, g.n * sizeof(float4)) == cudaSuccess &&
@@ -417,6 +466,7 @@ int tti_destroy(tti_handle *h)
   if (h->h_snap) cudaFreeHost(h->h_snap);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
+  free(h->tmaps);
   for (auto e : h->pev)
     if (e) cudaEventDestroy(e);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -505,13 +555,13 @@ int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const floa
   cudaStreamSynchronize(h->stream);
   for (auto p : raw) cudaFree(p);
   cudaFree(d_w);
-  if (rc == TTI_OK && h->use_fused) {
+  if (rc == TTI_OK && (h->use_fused || h->use_tiled)) {
     fused::launch_pack(g, step_args(h).p, fused::Packed{h->pk_cf, h->pk_vsc, h->pk_sc, h->pk_c4}, c.variant,
                        h->stream);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) rc = set_err(h, TTI_ERR_CUDA, "packing parameters: %s", cudaGetErrorString(e));
   }
-  if (rc == TTI_OK && h->use_fused) {
+  if (rc == TTI_OK && (h->use_fused || h->use_tiled)) {
     // the fused step skips coef1/coef2 loads where they are exactly 1 and dt;
     // verify that on the device instead of assuming the MEAL rim geometry
     int *cnt = nullptr;

@@ -57,6 +57,17 @@ void launch_sources(const StepArgs &a, const SourceSet &s, const SourceTables *t
                     cudaStream_t st);
 void launch_receivers(const StepArgs &a, const ReceiverSet &r, int seistype, int irec, int *flag, cudaStream_t st);
 void launch_energy(const StepArgs &a, int nz, int nx, double *out2, cudaStream_t st);
+// free surface + stress source (stype 1) + receiver samples, one thread per column
+struct PostArgs {
+  int freesurface, stype, tensor, it, irec;
+  SourceSet src;
+  float k1[121];
+  const int *colptr[3], *rz[3], *rid[3];  // receivers grouped by column (null: component off)
+  float *rec[3];
+  int nrec[3];
+  int *flag;
+};
+void launch_post(const StepArgs &a, const PostArgs &p, cudaStream_t st);
 // Pack a snapshot (kind 1..7) of the physical (savew = 0) or padded area
 // into a dense [nx_out][nz_out] buffer.
 void launch_snapshot(const StepArgs &a, int kind, int savew, float *dst, cudaStream_t st);

@@ -276,6 +276,74 @@ __global__ void k_energy(Grid g, Fields f, Params p, int nz, int nx, double *out
   }
 }
 
+// After the stress update, one thread per padded-grid column applies, in the
+// reference's order for every cell of that column: the free-surface image
+// (coord:847-863), the stress source stype 1 of each source in turn
+// (coord:865-886; tensor:871-895 also adds to tau) and the receiver samples
+// (isoelastic.c:103-144, after the step). Columns do not interact, so one
+// launch replaces three.
+__global__ void k_post(Grid g, Fields f, PostArgs p)
+{
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ix >= g.Nx) return;
+  const size_t col = (size_t)ix * g.ldz;
+  if (p.freesurface && ix >= NH && ix < g.Nx - NH) {
+    const size_t c = col + g.izStart;
+    const float sxx0 = f.sxx[c];
+    float xx[NH], zz[NH], xz[NH];
+#pragma unroll
+    for (int k = 1; k <= NH; ++k) {
+      xx[k - 1] = f.sxx[c + k];
+      zz[k - 1] = f.szz[c + k];
+      xz[k - 1] = f.sxz[c + k];
+    }
+    f.sxz[c] = 0.0f;
+    f.szz[c] = 0.0f;
+#pragma unroll
+    for (int k = 1; k <= NH; ++k) {
+      f.sxx[c - k] = __fsub_rn(__fmul_rn(2.0f, sxx0), xx[k - 1]);
+      f.szz[c - k] = -zz[k - 1];
+      f.sxz[c - k] = -xz[k - 1];
+    }
+  }
+  if (p.stype == 1) {
+    for (int n = 0; n < p.src.n; ++n) {
+      const int dx = ix - p.src.x[n];
+      if (dx < -NH || dx > NH) continue;
+      const int z0 = p.src.z[n];
+      const float a = p.src.w[(size_t)n * p.src.nt + p.it];
+      for (int dz = -NH; dz <= NH; ++dz) {
+        const int iz = z0 + dz;
+        if (iz < 0 || iz >= g.Nz) continue;
+        const float k1 = p.k1[(dx + NH) * 11 + (dz + NH)];
+        const size_t c = col + iz;
+        const float ws = __fmul_rn(k1, a);
+        f.sxx[c] = __fadd_rn(f.sxx[c], ws);
+        f.szz[c] = __fadd_rn(f.szz[c], ws);
+        if (p.tensor) {
+          f.txx[c] = __fadd_rn(f.txx[c], ws);
+          f.tzz[c] = __fadd_rn(f.tzz[c], ws);
+        }
+      }
+    }
+  }
+  if (p.irec >= 0) {
+    for (int k = 0; k < 3; ++k) {
+      if (!p.colptr[k]) continue;
+      const int b = p.colptr[k][ix], e = p.colptr[k][ix + 1];
+      for (int j = b; j < e; ++j) {
+        const size_t c = col + p.rz[k][j];
+        float v;
+        if (k == TTI_REC_VX) v = f.vx[c];
+        else if (k == TTI_REC_VZ) v = f.vz[c];
+        else v = __fmul_rn(0.5f, __fadd_rn(f.sxx[c], f.szz[c]));
+        p.rec[k][(size_t)p.irec * p.nrec[k] + p.rid[k][j]] = v;
+        if (!isfinite(v)) atomicOr(p.flag, 1);
+      }
+    }
+  }
+}
+
 __global__ void k_snapshot(Grid g, Fields f, int kind, int x0, int z0, int nzo, int nxo, float *dst)
 {
   const int iz = blockIdx.x * blockDim.x + threadIdx.x;
@@ -343,6 +411,11 @@ void launch_receivers(const StepArgs &a, const ReceiverSet &r, int seistype, int
 void launch_energy(const StepArgs &a, int nz, int nx, double *out2, cudaStream_t st)
 {
   k_energy<<<296, 256, 0, st>>>(a.g, a.f, a.p, nz, nx, out2);
+}
+
+void launch_post(const StepArgs &a, const PostArgs &p, cudaStream_t st)
+{
+  k_post<<<(a.g.Nx + 127) / 128, 128, 0, st>>>(a.g, a.f, p);
 }
 
 void launch_snapshot(const StepArgs &a, int kind, int savew, float *dst, cudaStream_t st)

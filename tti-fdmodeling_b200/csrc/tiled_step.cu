@@ -1,0 +1,400 @@
+// Tiled half-step kernels: the velocity update (coord:614-672, tensor:617-666,
+// bond:654-703) and the stress update (coord:804-845, tensor:799-851 with the
+// sigma = R tau pass fused, bond:836-873), each in place.
+//
+// A CTA owns a tile of TZ = 128 rows and TX = 16 columns. One elected thread
+// loads the tile plus the stencil halo of every input field with a 2D TMA copy
+// (cp.async.bulk.tensor, completion on an mbarrier, bounded wait); the box
+// starts at row z0 - 8 so its innermost coordinate stays 16-byte aligned, and
+// coordinates outside the array read zeros. Every stencil tap is then a
+// shared-memory load at a compile-time offset from the thread's own cell.
+// Each thread updates one row of TX / 4 columns (a warp's shared loads touch 32
+// consecutive words); per-cell parameters are plain coalesced loads whose
+// latency is hidden by 64 resident warps per SM (32 registers per thread).
+// The velocity kernel reads only stress and the stress kernel only velocity
+// from the tiles, so in-place updates are race-free.
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "tiled.cuh"
+
+namespace ttifd {
+namespace tiled {
+
+namespace {
+
+__device__ __forceinline__ unsigned smem_u32(const void *p)
+{
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count)
+{
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, unsigned bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+// bounded wait (about a second) so a copy that never lands cannot hang the GPU
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, unsigned limit = 1u << 20)
+{
+  const unsigned a = smem_u32(bar);
+  for (unsigned n = 0; n < limit; ++n) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(float *dst, const CUtensorMap *map, int c_inner, int c_outer,
+                                            unsigned long long *bar)
+{
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(c_inner), "r"(c_outer), "r"(smem_u32(bar))
+      : "memory");
+}
+
+static_assert((BZ * 4) % 16 == 0, "TMA inner box extent must be a multiple of 16 bytes");
+
+// tile cells handled by a thread: row zr, columns xc .. xc + TX/4 - 1
+struct Cells {
+  int x0, z0, xc, zr;
+};
+__device__ __forceinline__ Cells cells_of(const HalfArgs &a)
+{
+  const int t = threadIdx.x;
+  Cells c;
+  c.z0 = a.z_base + blockIdx.x * TZ;
+  c.x0 = a.x_base + blockIdx.y * TX;
+  c.xc = c.x0 + (TX / 4) * (t >> 7);
+  c.zr = c.z0 + (t & 127);
+  return c;
+}
+
+// Issues the TMA copies of the halo boxes of `n` fields (origin row z0 - 8,
+// column x0 - xoff); waited for by wait_tiles.
+__device__ __forceinline__ void issue_tiles(const HalfArgs &a, float *sm, unsigned long long *bar, int n, int z0,
+                                            int x0, int xoff)
+{
+  constexpr unsigned BOX_BYTES = BX * BZ * 4;
+  const int t = threadIdx.x;
+  if (t == 0) {
+    mbar_init(bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (t == 0) {
+    mbar_arrive_expect_tx(bar, n * BOX_BYTES);
+    for (int f = 0; f < n; ++f) tma_load_2d(sm + f * FIELD, &a.map[f], z0 - 8, x0 - xoff, bar);
+  }
+}
+
+// returns false (all threads) after a timed-out wait
+__device__ __forceinline__ bool wait_tiles(const HalfArgs &a, unsigned long long *bar)
+{
+  const bool ok = mbar_wait(bar, 0);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) {
+      atomicOr(a.err, 4);
+      mbar_wait(bar, 0, 1u << 16);  // give the copies in flight a bounded time
+    }
+    return false;
+  }
+  return true;
+}
+
+// true when every cell of the tile lies where coef1 = 1 and coef2 = dt
+__device__ __forceinline__ bool tile_undamped(const HalfArgs &a, const Cells &c)
+{
+  const Grid &g = a.g;
+  return a.undamped_ok && c.x0 >= g.E && c.x0 + TX <= g.Nx - g.E && c.z0 >= (a.freesurface ? 0 : g.E) &&
+         c.z0 + TZ <= g.Nz - g.E;
+}
+
+template <int V, bool X>
+__global__ void __launch_bounds__(NT, 4) k_velocity_tiled(const __grid_constant__ HalfArgs a)
+{
+  using A = Ar<X>;
+  extern __shared__ __align__(128) float sm[];
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm + 3 * FIELD);
+  const Grid &g = a.g;
+  const Cells c = cells_of(a);
+  issue_tiles(a, sm, bar, 3, c.z0, c.x0, 4);
+  const int L = g.ldz;
+  const bool und = tile_undamped(a, c);
+  const int z = c.zr;
+  const bool zin = z >= g.izStart && z < g.Nz - NH;
+  if (!wait_tiles(a, bar)) return;
+  if (!zin) return;
+  const float invdx = a.invdx, invdz = a.invdz;
+#pragma unroll
+  for (int i = 0; i < TX / 4; ++i) {
+    const int x = c.xc + i;
+    if (x >= g.Nx - NH) break;
+    const size_t gi = (size_t)x * L + z;
+    const float vx0 = a.f.vx[gi], vz0 = a.f.vz[gi];
+    float c1 = 1.0f, c2 = a.dt;
+    if (!und) {
+      const float2 cf = __ldg(a.pk.cf + gi);
+      c1 = cf.x;
+      c2 = cf.y;
+    }
+    const float ir = __ldg(a.p.invrho + gi);
+    // stress value at column x+m, row z+n: s[f * FIELD + m * BZ + n]
+    const float *s = sm + (x - c.x0 + 4) * BZ + (z - c.z0 + 8);
+    float d[3][2];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      const float *q = s + f * FIELD;
+      // d1 = sum C_k (s[x+k][z+k] - s[x-k+1][z-k+1]); d2 = sum C_k (s[x+k][z-k+1] - s[x-k+1][z+k])
+      float s1 = A::mul(rsg(0), A::sub(q[BZ + 1], q[0]));
+      float s2 = A::mul(rsg(0), A::sub(q[BZ], q[1]));
+#pragma unroll
+      for (int k = 2; k <= NH; ++k) {
+        s1 = A::add(s1, A::mul(rsg(k - 1), A::sub(q[k * BZ + k], q[(1 - k) * BZ + 1 - k])));
+        s2 = A::add(s2, A::mul(rsg(k - 1), A::sub(q[k * BZ + 1 - k], q[(1 - k) * BZ + k])));
+      }
+      d[f][0] = s1;
+      d[f][1] = s2;
+    }
+    const float sxx_x = A::mul(A::mul(0.5f, A::add(d[0][0], d[0][1])), invdx);
+    const float szz_z = A::mul(A::mul(0.5f, A::sub(d[1][0], d[1][1])), invdz);
+    const float sxz_x = A::mul(A::mul(0.5f, A::add(d[2][0], d[2][1])), invdx);
+    const float sxz_z = A::mul(A::mul(0.5f, A::sub(d[2][0], d[2][1])), invdz);
+    const float br = A::mul(c2, ir);
+    float fx, fz;
+    if (V == TTI_COORDINATE) {
+      const float2 sc = __ldg(a.pk.vsc + gi);
+      const float sv = sc.x, cv = sc.y;
+      const float sxx_z = A::mul(A::mul(0.5f, A::sub(d[0][0], d[0][1])), invdx);  // invdx as coord:633
+      const float szz_x = A::mul(A::mul(0.5f, A::add(d[1][0], d[1][1])), invdx);
+      fx = A::add(A::add(A::sub(A::mul(cv, sxx_x), A::mul(sv, sxx_z)), A::mul(sv, sxz_x)), A::mul(cv, sxz_z));
+      fz = A::add(A::add(A::sub(A::mul(cv, sxz_x), A::mul(sv, sxz_z)), A::mul(sv, szz_x)), A::mul(cv, szz_z));
+    } else {
+      fx = A::add(sxx_x, sxz_z);
+      fz = A::add(sxz_x, szz_z);
+    }
+    a.f.vx[gi] = A::add(A::mul(c1, vx0), A::mul(br, fx));
+    a.f.vz[gi] = A::add(A::mul(c1, vz0), A::mul(br, fz));
+  }
+}
+
+// per-cell inputs of the stress update
+struct SCell {
+  float c1, c2, s2t, o0, o1, o2;  // o*: sigma (coordinate, Bond) or tau (tensor)
+  float4 c4;
+  float2 sc;
+};
+
+template <int V>
+__device__ __forceinline__ void load_scell(const HalfArgs &a, bool und, size_t gi, SCell &o)
+{
+  if (und) {
+    o.c1 = 1.0f;
+    o.c2 = a.dt;
+  } else {
+    const float2 cf = __ldg(a.pk.cf + gi);
+    o.c1 = cf.x;
+    o.c2 = cf.y;
+  }
+  o.c4 = __ldg(a.pk.c4 + gi);
+  o.sc = __ldg(a.pk.sc + gi);
+  if (V == TTI_TENSOR) {
+    o.s2t = __ldg(a.p.s2t + gi);
+    o.o0 = a.f.txx[gi];
+    o.o1 = a.f.tzz[gi];
+    o.o2 = a.f.txz[gi];
+  } else {
+    o.o0 = a.f.sxx[gi];
+    o.o1 = a.f.szz[gi];
+    o.o2 = a.f.sxz[gi];
+  }
+}
+
+template <int V, bool X>
+__device__ __forceinline__ void stress_store(const HalfArgs &a, size_t gi, float vxx, float vxz, float vzx, float vzz,
+                                             const SCell &p)
+{
+  using A = Ar<X>;
+  const float c1 = p.c1, c2 = p.c2;
+  const float c11 = p.c4.x, c13 = p.c4.y, c33 = p.c4.z, c55 = p.c4.w;
+  if (V == TTI_COORDINATE) {
+    const float sn = p.sc.x, cs = p.sc.y;
+    float q = A::add(A::mul(sn, vxx), A::mul(cs, vxz));
+    vxx = A::sub(A::mul(cs, vxx), A::mul(sn, vxz));
+    vxz = q;
+    q = A::add(A::mul(sn, vzx), A::mul(cs, vzz));
+    vzx = A::sub(A::mul(cs, vzx), A::mul(sn, vzz));
+    vzz = q;
+    a.f.sxx[gi] = A::add(A::mul(c1, p.o0), A::mul(c2, A::add(A::mul(c11, vxx), A::mul(c13, vzz))));
+    a.f.szz[gi] = A::add(A::mul(c1, p.o1), A::mul(c2, A::add(A::mul(c13, vxx), A::mul(c33, vzz))));
+    a.f.sxz[gi] = A::add(A::mul(c1, p.o2), A::mul(A::mul(c2, c55), A::add(vzx, vxz)));
+  } else if (V == TTI_TENSOR) {
+    const float s2 = p.sc.x, cc2 = p.sc.y, s2t = p.s2t;
+    const float sh = A::add(vxz, vzx);
+    const float exx = A::sub(A::add(A::mul(cc2, vxx), A::mul(s2, vzz)), A::mul(A::mul(0.5f, s2t), sh));
+    const float ezz = A::add(A::add(A::mul(s2, vxx), A::mul(cc2, vzz)), A::mul(A::mul(0.5f, s2t), sh));
+    const float exz = A::add(A::mul(s2t, A::sub(vxx, vzz)), A::mul(A::sub(cc2, s2), sh));
+    const float ntx = A::add(A::mul(c1, p.o0), A::mul(c2, A::add(A::mul(c11, exx), A::mul(c13, ezz))));
+    const float ntz = A::add(A::mul(c1, p.o1), A::mul(c2, A::add(A::mul(c13, exx), A::mul(c33, ezz))));
+    const float ntq = A::add(A::mul(c1, p.o2), A::mul(A::mul(c2, c55), exz));
+    a.f.txx[gi] = ntx;
+    a.f.tzz[gi] = ntz;
+    a.f.txz[gi] = ntq;
+    a.f.sxx[gi] = A::add(A::add(A::mul(cc2, ntx), A::mul(s2, ntz)), A::mul(s2t, ntq));
+    a.f.szz[gi] = A::sub(A::add(A::mul(s2, ntx), A::mul(cc2, ntz)), A::mul(s2t, ntq));
+    a.f.sxz[gi] = A::add(A::mul(A::mul(-0.5f, s2t), A::sub(ntx, ntz)), A::mul(A::sub(cc2, s2), ntq));
+  } else {
+    const float c15 = p.sc.x, c35 = p.sc.y;
+    const float sh = A::add(vzx, vxz);
+    a.f.sxx[gi] =
+        A::add(A::mul(c1, p.o0), A::mul(c2, A::add(A::add(A::mul(c11, vxx), A::mul(c13, vzz)), A::mul(c15, sh))));
+    a.f.szz[gi] =
+        A::add(A::mul(c1, p.o1), A::mul(c2, A::add(A::add(A::mul(c13, vxx), A::mul(c33, vzz)), A::mul(c35, sh))));
+    a.f.sxz[gi] =
+        A::add(A::mul(c1, p.o2), A::mul(c2, A::add(A::add(A::mul(c15, vxx), A::mul(c35, vzz)), A::mul(c55, sh))));
+  }
+}
+
+template <int V, bool X>
+__global__ void __launch_bounds__(NT, 4) k_stress_tiled(const __grid_constant__ HalfArgs a)
+{
+  using A = Ar<X>;
+  extern __shared__ __align__(128) float sm[];
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm + 2 * FIELD);
+  const Grid &g = a.g;
+  const Cells c = cells_of(a);
+  issue_tiles(a, sm, bar, 2, c.z0, c.x0, 5);
+  const bool und = tile_undamped(a, c);
+  const int z = c.zr;
+  const bool zin = z >= g.izStart && z < g.Nz - NH;
+  if (!wait_tiles(a, bar)) return;
+  if (!zin) return;
+  const float invdx = a.invdx, invdz = a.invdz;
+#pragma unroll
+  for (int i = 0; i < TX / 4; ++i) {
+    const int x = c.xc + i;
+    if (x >= g.Nx - NH) break;
+    const size_t gi = (size_t)x * g.ldz + z;
+    SCell p;
+    load_scell<V>(a, und, gi, p);
+    // velocity value at column x+m, row z+n: s[f * FIELD + m * BZ + n]
+    const float *s = sm + (x - c.x0 + 5) * BZ + (z - c.z0 + 8);
+    float d[2][2];
+#pragma unroll
+    for (int f = 0; f < 2; ++f) {
+      const float *q = s + f * FIELD;
+      // d1 = sum C_k (v[x+k-1][z+k-1] - v[x-k][z-k]); d2 = sum C_k (v[x+k-1][z-k] - v[x-k][z+k-1])
+      float s1 = A::mul(rsg(0), A::sub(q[0], q[-BZ - 1]));
+      float s2 = A::mul(rsg(0), A::sub(q[-1], q[-BZ]));
+#pragma unroll
+      for (int k = 2; k <= NH; ++k) {
+        s1 = A::add(s1, A::mul(rsg(k - 1), A::sub(q[(k - 1) * BZ + k - 1], q[-k * BZ - k])));
+        s2 = A::add(s2, A::mul(rsg(k - 1), A::sub(q[(k - 1) * BZ - k], q[-k * BZ + k - 1])));
+      }
+      d[f][0] = s1;
+      d[f][1] = s2;
+    }
+    const float vxx = A::mul(A::mul(0.5f, A::add(d[0][0], d[0][1])), invdx);
+    const float vxz = A::mul(A::mul(0.5f, A::sub(d[0][0], d[0][1])), invdz);
+    const float vzx = A::mul(A::mul(0.5f, A::add(d[1][0], d[1][1])), invdx);
+    const float vzz = A::mul(A::mul(0.5f, A::sub(d[1][0], d[1][1])), invdz);
+    stress_store<V, X>(a, gi, vxx, vxz, vzx, vzz, p);
+  }
+}
+
+template <typename K>
+cudaError_t launch_k(K kernel, const HalfArgs &a, int nfields, cudaStream_t st)
+{
+  const size_t bytes = (size_t)nfields * FIELD * sizeof(float) + 16;
+  static std::mutex mu;
+  static const void *done[32];
+  static int ndone = 0;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    bool seen = false;
+    for (int i = 0; i < ndone; ++i) seen = seen || done[i] == (const void *)kernel;
+    if (!seen) {
+      cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+      if (e != cudaSuccess) return e;
+      if (ndone < 32) done[ndone++] = (const void *)kernel;
+    }
+  }
+  HalfArgs b = a;
+  const dim3 gr = grid(a.g, &b.z_base);
+  if (gr.x == 0 || gr.y == 0) return cudaSuccess;
+  kernel<<<gr, NT, bytes, st>>>(b);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+dim3 grid(const Grid &g, int *z_base)
+{
+  *z_base = g.izStart & ~3;
+  const int nz = g.Nz - NH - *z_base, nx = g.Nx - 2 * NH;
+  if (nz <= 0 || nx <= 0) return dim3(0, 0);
+  return dim3((nz + TZ - 1) / TZ, (nx + TX - 1) / TX);
+}
+
+bool encode_map(CUtensorMap *map, const Grid &g, float *field)
+{
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    cudaDriverEntryPointQueryResult q;
+    void *fn = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+      return false;
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  const cuuint64_t dims[2] = {(cuuint64_t)g.ldz, (cuuint64_t)g.Nx};
+  const cuuint64_t strides[1] = {(cuuint64_t)g.ldz * sizeof(float)};
+  const cuuint32_t box[2] = {(cuuint32_t)BZ, (cuuint32_t)BX};
+  const cuuint32_t estr[2] = {1, 1};
+  return encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, field, dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+cudaError_t launch_velocity(const HalfArgs &a, int variant, bool exact, cudaStream_t st)
+{
+  if (exact) {
+    if (variant == TTI_COORDINATE) return launch_k(k_velocity_tiled<TTI_COORDINATE, true>, a, 3, st);
+    if (variant == TTI_TENSOR) return launch_k(k_velocity_tiled<TTI_TENSOR, true>, a, 3, st);
+    return launch_k(k_velocity_tiled<TTI_BOND, true>, a, 3, st);
+  }
+  if (variant == TTI_COORDINATE) return launch_k(k_velocity_tiled<TTI_COORDINATE, false>, a, 3, st);
+  if (variant == TTI_TENSOR) return launch_k(k_velocity_tiled<TTI_TENSOR, false>, a, 3, st);
+  return launch_k(k_velocity_tiled<TTI_BOND, false>, a, 3, st);
+}
+
+cudaError_t launch_stress(const HalfArgs &a, int variant, bool exact, cudaStream_t st)
+{
+  if (exact) {
+    if (variant == TTI_COORDINATE) return launch_k(k_stress_tiled<TTI_COORDINATE, true>, a, 2, st);
+    if (variant == TTI_TENSOR) return launch_k(k_stress_tiled<TTI_TENSOR, true>, a, 2, st);
+    return launch_k(k_stress_tiled<TTI_BOND, true>, a, 2, st);
+  }
+  if (variant == TTI_COORDINATE) return launch_k(k_stress_tiled<TTI_COORDINATE, false>, a, 2, st);
+  if (variant == TTI_TENSOR) return launch_k(k_stress_tiled<TTI_TENSOR, false>, a, 2, st);
+  return launch_k(k_stress_tiled<TTI_BOND, false>, a, 2, st);
+}
+
+}  // namespace tiled
+}  // namespace ttifd

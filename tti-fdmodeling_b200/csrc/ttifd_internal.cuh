@@ -85,6 +85,8 @@ struct tti_handle {
   float *fld[8] = {};   // current wavefields
   float *fld2[8] = {};  // second set: the fused step reads fld and writes fld2, then swaps
   bool use_fused = false;
+  bool use_tiled = false;  // tiled half-step kernels with TMA halo tiles (in place)
+  void *tmaps = nullptr;   // host copy of the 5 tensor maps (vx vz sxx szz sxz), 64-byte aligned
   int seg = 0;          // columns per CTA of the fused step
   int bz = 0;           // rows per band of the fused step
   int undamped_ok = 0;  // coef1 == 1, coef2 == dt outside the absorbing rims (checked at upload)
