@@ -235,6 +235,73 @@ def run_ours(args, rank, world, local_rank):
     return line
 
 
+# ---------------------------------------------------------------- batched arm
+BATCH_WORKLOAD = dict(nz=1126, nx=3000, x0=2436, dx=10.0, dz=10.0, dt=0.0008, fpeak=10.0, ealThick=50,
+                      freesurface=1, stype=1, seistype=1, mt=1, wsave=0, savew=0, mode=1, scalar=1.0, energy=0)
+
+
+def run_batched(args, local_rank):
+    """Many shots of one model through tti_batch_* (one launch per half-step for
+    all shots, the loop in CUDA-graph replays) against one shot of the same
+    model through the plain path. Shots 120 m apart along the surface of the
+    nx=3000 crop (columns 2436..5435) of the salt-like model, 3000 receivers
+    per shot at z=2, 10 Hz, ealThick=50, free surface."""
+    import ttifd
+
+    variant, S, K, W = args.variant, args.batch_shots, args.batch_steps, args.warmup
+    bw = dict(BATCH_WORKLOAD)
+    x0 = bw.pop("x0")
+    m = synthetic.crop(model(), x0, bw["nx"]) if WORKLOAD["nx"] >= x0 + bw["nx"] else \
+        synthetic.salt_model(bw["nz"], bw["nx"], seed=1)
+    pads = synthetic.padded(m, bw["ealThick"])
+    cfg = dict(bw, variant=variant, nt=W + K)
+    wav = synthetic.ricker(cfg["nt"], cfg["dt"], cfg["fpeak"])[None, :]
+    gx = np.arange(bw["nx"], dtype=np.int32)
+    gz = np.full(bw["nx"], 2, np.int32)
+    shots = [1122 + 12 * i for i in range(S)]
+    # plain: one shot of the same model
+    with ttifd.Modeling(device=local_rank, **cfg) as h:
+        h.upload_model(*pads)
+        h.set_source([shots[0]], [2], wav)
+        for k in (0, 1):
+            h.set_receivers(k, gx, gz)
+        h.reset()
+        h.step(W)
+        h.step(K)
+        plain_ms = h.elapsed_ms
+        cells = h.Nz * h.Nx
+    plain = cells * K / (plain_ms / 1e3) / 1e9
+    with ttifd.Batch([cfg], [0] * S, device=local_rank) as b:
+        b.upload_model(0, *pads)
+        for i, sx in enumerate(shots):
+            inst = b.instances[i]
+            inst.set_source([sx], [2], wav)
+            for k in (0, 1):
+                inst.set_receivers(k, gx, gz)
+        tuned = b.autotune(min(20, K))
+        b.reset()
+        b.step(W)
+        l0 = b.kernel_launches
+        with ClockSampler(local_rank) as clk:
+            b.step(K)
+            ms = b.elapsed_ms
+        launches = b.kernel_launches - l0
+    value = S * cells * K / (ms / 1e3) / 1e9
+    peak, src = peaks()
+    state = 64 if variant == "tensor_rotation" else 40
+    param = ALG_BYTES_STEP[variant] - state
+    alg = (S * state + param) * cells * K / (ms / 1e3) / 1e9
+    return {"workload": f"batched forward, {variant}, {S} shots 120 m apart on the 1126x3000 crop of the "
+                        "salt-like model, 3000 receivers per shot, 10 Hz, ealThick=50, freesurface",
+            "shots": S, "steps": K, "value": value, "unit": "Gcell/s", "ms_per_step": ms / K,
+            "plain_same_model": plain, "speedup_vs_plain": value / plain,
+            "schedule": tuned, "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": alg, "peak": peak, "unit": "GB/s", "frac": alg / peak,
+                         "peak_source": src,
+                         "alg_bytes_per_step": f"shots x cells x {state} B state + cells x {param} B parameters"},
+            "clocks": clk.summary()}
+
+
 # ---------------------------------------------------------------- reference arm
 def ref_program(variant: str):
     for sub in ("bin", "strict"):
@@ -317,6 +384,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nx", type=int, default=WORKLOAD["nx"],
                     help="narrower model for profiler captures (default: the full 7872)")
+    ap.add_argument("--batch-shots", type=int, default=64)
+    ap.add_argument("--batch-steps", type=int, default=200)
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     WORKLOAD["nx"] = args.nx
@@ -341,6 +411,8 @@ def main():
         return
 
     line = run_ours(args, rank, world, local_rank)
+    if not args.no_batch and world == 1:
+        line["batched"] = run_batched(args, local_rank)
     if rank == 0:
         if not args.no_cpu_baseline:
             try:

@@ -183,6 +183,46 @@ int tti_fetch_field(tti_handle *h, int which, float *out);
 /* Energy per step (energy = 1): Ek[nt], Ep[nt] (coord:898-924, 942-968). */
 int tti_fetch_energy(tti_handle *h, float *ek, float *ep);
 
+/* ---- Batched execution ------------------------------------------------------
+ * Many shots (and many models, of different sizes and nt) advanced together:
+ * each half-step is one launch over every instance's tiles, and the time loop
+ * runs as replays of a CUDA graph of several steps. The reference runs one shot
+ * per program invocation (the time loop of coord:611-926); these entry points
+ * replace N such invocations. Instances record traces only (wsave = 0,
+ * energy = 0); all models use the same formulation.
+ *
+ * cfg[m] describes model m; model_of[i] (NULL: all 0) names the model of
+ * instance i. Instance handles (tti_batch_instance) are ordinary handles owned
+ * by the batch: tti_set_source, tti_set_receivers and tti_fetch_traces work on
+ * them as on a single shot. The instances of a model share its parameter
+ * arrays, uploaded once with tti_batch_upload_model. */
+typedef struct tti_batch tti_batch;
+int tti_batch_create(tti_batch **b, int nmodels, const tti_config *cfg, int ninst, const int *model_of,
+                     int device);
+int tti_batch_destroy(tti_batch *b);
+const char *tti_batch_last_error(const tti_batch *b);
+tti_handle *tti_batch_instance(tti_batch *b, int i);
+int tti_batch_upload_model(tti_batch *b, int m, const float *vp, const float *vs, const float *rho,
+                           const float *epsilon, const float *delta, const float *theta);
+/* Schedule: the shots of a model run tile by tile in groups of `group`
+ * (0: all of them, so each parameter tile is read from HBM once per step;
+ * 1: shot after shot), and the loop replays a CUDA graph of `graph_steps`
+ * steps (0: no graph). */
+int tti_batch_set_order(tti_batch *b, int group, int graph_steps);
+/* Times every group size in {all, 1, 2, 4, 8, 16} (those below the shot
+ * count) with and without a graph on nsteps steps, keeps the fastest and
+ * resets the batch. Outputs (may be NULL): the choice and its ms per step. */
+int tti_batch_autotune(tti_batch *b, int nsteps, int *group, int *graph_steps, float *ms_per_step);
+/* Zeroes every instance and rebuilds the launch tables from the current
+ * sources and receivers. */
+int tti_batch_reset(tti_batch *b);
+/* Advances every instance nsteps (an instance past its own nt stays idle). */
+int tti_batch_step(tti_batch *b, int nsteps);
+/* reset + step(max nt): every instance from it = 0 to its own nt. */
+int tti_batch_run(tti_batch *b);
+int tti_batch_elapsed_ms(const tti_batch *b, float *ms);
+int tti_batch_kernel_launches(const tti_batch *b, long long *n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -50,3 +50,21 @@ def test_create_without_gpu_fails_cleanly(gpu_lib):
     with pytest.raises(ttifd.TTIError) as e:
         ttifd.Modeling(nz=10, nx=10, nt=10, dx=10, dz=10, dt=0.001, fpeak=10)
     assert e.value.code == ttifd.ERR_CUDA
+
+
+@pytest.mark.parametrize("models,model_of,what", [
+    ([dict(wsave=2)], [0], "traces only"),
+    ([dict(energy=1)], [0], "traces only"),
+    ([dict(), dict(variant=1)], [0, 1], "same formulation"),
+    ([dict()], [0, 1], "out of range"),
+    ([dict(), dict()], [0, 0], "has no instance"),
+])
+def test_batch_argument_checks(models, model_of, what, gpu_lib):
+    """tti_batch_create validates its arguments on the host, before any device work."""
+    import ttifd
+
+    base = dict(nz=20, nx=30, nt=10, dx=10, dz=10, dt=0.001, fpeak=10)
+    with pytest.raises(ttifd.TTIError) as e:
+        ttifd.Batch([dict(base, **m) for m in models], model_of)
+    assert e.value.code == ttifd.ERR_ARG
+    assert what in str(e.value)

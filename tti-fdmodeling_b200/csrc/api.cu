@@ -292,6 +292,7 @@ int check_flag(tti_handle *h)
   CK(h, cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
   if (flag & 2) return set_err(h, TTI_ERR_CUDA, "a shared-memory copy wait timed out in the fused step kernel");
+  if (flag & 4) return set_err(h, TTI_ERR_CUDA, "a TMA tile wait timed out in a tiled half-step kernel");
   if (flag) return set_err(h, TTI_ERR_NONFINITE, "non-finite value recorded at a receiver (unstable run?)");
   return TTI_OK;
 }
@@ -309,6 +310,8 @@ int copy_out_pitched(tti_handle *h, const float *src, float *out)
 
 namespace ttifd {
 StepArgs handle_step_args(const tti_handle *h) { return step_args(h); }
+void handle_source_tables(const tti_handle *h, SourceTables *t) { source_tables(h, t); }
+int handle_check_flag(tti_handle *h) { return check_flag(h); }
 int handle_error(tti_handle *h, int code, const char *msg) { return set_err(h, code, "%s", msg); }
 }  // namespace ttifd
 
@@ -317,6 +320,18 @@ extern "C" {
 const char *tti_last_error(const tti_handle *h) { return h ? h->err.c_str() : g_create_error.c_str(); }
 
 int tti_create(tti_handle **out, const tti_config *cfg, int device)
+{
+  return ttifd::create_handle(out, cfg, device, nullptr, false);
+}
+
+}  // extern "C"
+
+namespace ttifd {
+
+// tti_create with two options for batched execution: `share` (its parameter
+// arrays are used, not allocated; cfg must describe the same grid) and
+// `force_tiled` (the tiled kernels whatever TTIFD_KERNEL says).
+int create_handle(tti_handle **out, const tti_config *cfg, int device, const tti_handle *share, bool force_tiled)
 {
   if (!out || !cfg) return set_err(nullptr, TTI_ERR_ARG, "null argument");
   *out = nullptr;
@@ -373,8 +388,8 @@ int tti_create(tti_handle **out, const tti_config *cfg, int device)
     h->bz = (g.Nz + bands - 1) / bands;
     // the fused step needs the free-surface rows E-5 .. E+5 inside the first band
     // default: the tiled half-step kernels; `fused` selects the single-kernel step
-    h->use_fused = fused_req && !(cfg->freesurface == 1 && g.E + NH >= h->bz);
-    h->use_tiled = !naive && !h->use_fused;
+    h->use_fused = !force_tiled && fused_req && !(cfg->freesurface == 1 && g.E + NH >= h->bz);
+    h->use_tiled = force_tiled || (!naive && !h->use_fused);
   }
   for (int f = 0; f < nfields(cfg->variant); ++f) {
     if ((rc = alloc(&h->fld[f]))) return fail(rc);
@@ -394,7 +409,14 @@ int tti_create(tti_handle **out, const tti_config *cfg, int device)
         return fail(TTI_ERR_CUDA);
       }
   }
-  if (h->use_fused || h->use_tiled) {
+  if (share) {
+    h->owner = share;
+    for (int p = 0; p < TTI_P_COUNT; ++p) h->par[p] = share->par[p];
+    h->pk_cf = share->pk_cf;
+    h->pk_vsc = share->pk_vsc;
+    h->pk_sc = share->pk_sc;
+    h->pk_c4 = share->pk_c4;
+  } else if (h->use_fused || h->use_tiled) {
     bool okp = cudaMalloc(&h->pk_cf, g.n * sizeof(float2)) == cudaSuccess &&
                cudaMalloc(&h->pk_sc, g.n * sizeof(float2)) == cudaSuccess &&
                cudaMalloc(&h->pk_c4, g.n * sizeof(float4)) == cudaSuccess &&
@@ -420,7 +442,7 @@ int tti_create(tti_handle **out, const tti_config *cfg, int device)
     const char *segenv = getenv("TTIFD_SEG");
     if (segenv && atoi(segenv) > 0) h->seg = atoi(segenv);
   }
-  for (int p = 0; p < TTI_P_COUNT; ++p)
+  for (int p = 0; p < TTI_P_COUNT && !share; ++p)
     if (param_used(cfg->variant, p) && (rc = alloc(&h->par[p]))) return fail(rc);
   if (cudaMalloc(&h->d_flag, sizeof(int)) != cudaSuccess ||
       cudaMalloc(&h->d_energy, sizeof(double) * 2 * (size_t)cfg->nt) != cudaSuccess) {
@@ -437,6 +459,10 @@ int tti_create(tti_handle **out, const tti_config *cfg, int device)
   return TTI_OK;
 }
 
+}  // namespace ttifd
+
+extern "C" {
+
 int tti_destroy(tti_handle *h)
 {
   if (!h) return TTI_OK;
@@ -444,7 +470,13 @@ int tti_destroy(tti_handle *h)
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (auto &p : h->fld) cudaFree(p);
   for (auto &p : h->fld2) cudaFree(p);
-  for (auto &p : h->par) cudaFree(p);
+  if (!h->owner) {
+    for (auto &p : h->par) cudaFree(p);
+    cudaFree(h->pk_cf);
+    cudaFree(h->pk_vsc);
+    cudaFree(h->pk_sc);
+    cudaFree(h->pk_c4);
+  }
   for (int k = 0; k < 3; ++k) {
     cudaFree(h->d_rx[k]);
     cudaFree(h->d_rz[k]);
@@ -456,10 +488,6 @@ int tti_destroy(tti_handle *h)
   cudaFree(h->d_sx);
   cudaFree(h->d_sz);
   cudaFree(h->d_src);
-  cudaFree(h->pk_cf);
-  cudaFree(h->pk_vsc);
-  cudaFree(h->pk_sc);
-  cudaFree(h->pk_c4);
   cudaFree(h->d_energy);
   cudaFree(h->d_flag);
   cudaFree(h->d_snap);
@@ -487,6 +515,7 @@ int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const floa
                      const float *delta, const float *theta)
 {
   if (!h || !vp || !vs || !rho || !epsilon || !delta || !theta) return set_err(h, TTI_ERR_ARG, "null model array");
+  if (h->owner) return set_err(h, TTI_ERR_STATE, "this handle shares the parameters of another; upload through it");
   CK(h, cudaSetDevice(h->device));
   const tti_config &c = h->cfg;
   const Grid &g = h->g;

@@ -68,12 +68,36 @@ struct PostArgs {
   int *flag;
 };
 void launch_post(const StepArgs &a, const PostArgs &p, cudaStream_t st);
+
+// ---------------- batched (many instances per launch) ----------------
+// Per-instance arguments in device memory; the time index comes from the
+// shared step counter `step` (it = step, or nt - 1 - step for mode 2), and an
+// instance whose nt has been reached does nothing.
+struct BatchPost {
+  Grid g;
+  Fields f;
+  PostArgs p;  // it / irec unused
+  int nt, mode2, mt, rec_on;
+};
+struct BatchSrc {
+  Grid g;
+  Fields f;
+  SourceSet s;
+  const SourceTables *tab;  // device
+  int variant, stype, nt, mode2;
+};
+void launch_post_batch(const BatchPost *d, int n, int maxNx, const int *step, cudaStream_t st);
+void launch_sources_batch(const BatchSrc *d, int n, const int *step, cudaStream_t st);
+void launch_advance(int *step, cudaStream_t st);
 // Pack a snapshot (kind 1..7) of the physical (savew = 0) or padded area
 // into a dense [nx_out][nz_out] buffer.
 void launch_snapshot(const StepArgs &a, int kind, int savew, float *dst, cudaStream_t st);
 
 // C-ABI helpers shared by the entry points in other translation units
 StepArgs handle_step_args(const tti_handle *h);
+void handle_source_tables(const tti_handle *h, SourceTables *t);
+int handle_check_flag(tti_handle *h);
+int create_handle(tti_handle **out, const tti_config *cfg, int device, const tti_handle *share, bool force_tiled);
 int handle_error(tti_handle *h, int code, const char *msg);
 
 }  // namespace ttifd

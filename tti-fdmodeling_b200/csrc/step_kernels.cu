@@ -160,7 +160,8 @@ __device__ __forceinline__ void dec(float *p, float k, float a) { *p = __fsub_rn
 // Sources over their 11 x 11 windows, one thread per window cell. Sources are
 // applied one after another (a barrier between them) so overlapping windows
 // accumulate in the reference's order; stype 8 runs on one thread.
-__global__ void k_sources(Grid g, Fields f, SourceSet s, SourceTables t, int variant, int stype, int stage, int it)
+__device__ void sources_block(const Grid &g, const Fields &f, const SourceSet &s, const SourceTables &t, int variant,
+                              int stype, int stage, int it)
 {
   const int tid = threadIdx.x;
   if (stage == 0 && stype == 8) {
@@ -232,6 +233,22 @@ __global__ void k_sources(Grid g, Fields f, SourceSet s, SourceTables t, int var
   }
 }
 
+__global__ void k_sources(Grid g, Fields f, SourceSet s, SourceTables t, int variant, int stype, int stage, int it)
+{
+  sources_block(g, f, s, t, variant, stype, stage, it);
+}
+
+// Batched velocity sources: one block per instance, time index from the step counter.
+__global__ void k_sources_batch(const BatchSrc *bs, const int *step)
+{
+  const BatchSrc &b = bs[blockIdx.x];
+  const int n = *step;
+  if (n >= b.nt || b.s.n == 0) return;
+  sources_block(b.g, b.f, b.s, *b.tab, b.variant, b.stype, 0, b.mode2 ? b.nt - 1 - n : n);
+}
+
+__global__ void k_advance(int *step) { ++*step; }
+
 // isoelastic.c:103-144; recorded time-major on the device ([irec][trace]).
 __global__ void k_receivers(Grid g, Fields f, ReceiverSet r, int want_v, int want_p, int irec, int *flag)
 {
@@ -282,10 +299,8 @@ __global__ void k_energy(Grid g, Fields f, Params p, int nz, int nx, double *out
 // (coord:865-886; tensor:871-895 also adds to tau) and the receiver samples
 // (isoelastic.c:103-144, after the step). Columns do not interact, so one
 // launch replaces three.
-__global__ void k_post(Grid g, Fields f, PostArgs p)
+__device__ void post_column(const Grid &g, const Fields &f, const PostArgs &p, int ix, int it, int irec)
 {
-  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
-  if (ix >= g.Nx) return;
   const size_t col = (size_t)ix * g.ldz;
   if (p.freesurface && ix >= NH && ix < g.Nx - NH) {
     const size_t c = col + g.izStart;
@@ -311,7 +326,7 @@ __global__ void k_post(Grid g, Fields f, PostArgs p)
       const int dx = ix - p.src.x[n];
       if (dx < -NH || dx > NH) continue;
       const int z0 = p.src.z[n];
-      const float a = p.src.w[(size_t)n * p.src.nt + p.it];
+      const float a = p.src.w[(size_t)n * p.src.nt + it];
       for (int dz = -NH; dz <= NH; ++dz) {
         const int iz = z0 + dz;
         if (iz < 0 || iz >= g.Nz) continue;
@@ -327,7 +342,7 @@ __global__ void k_post(Grid g, Fields f, PostArgs p)
       }
     }
   }
-  if (p.irec >= 0) {
+  if (irec >= 0) {
     for (int k = 0; k < 3; ++k) {
       if (!p.colptr[k]) continue;
       const int b = p.colptr[k][ix], e = p.colptr[k][ix + 1];
@@ -337,11 +352,32 @@ __global__ void k_post(Grid g, Fields f, PostArgs p)
         if (k == TTI_REC_VX) v = f.vx[c];
         else if (k == TTI_REC_VZ) v = f.vz[c];
         else v = __fmul_rn(0.5f, __fadd_rn(f.sxx[c], f.szz[c]));
-        p.rec[k][(size_t)p.irec * p.nrec[k] + p.rid[k][j]] = v;
+        p.rec[k][(size_t)irec * p.nrec[k] + p.rid[k][j]] = v;
         if (!isfinite(v)) atomicOr(p.flag, 1);
       }
     }
   }
+}
+
+__global__ void k_post(Grid g, Fields f, PostArgs p)
+{
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ix >= g.Nx) return;
+  post_column(g, f, p, ix, p.it, p.irec);
+}
+
+// Batched: blockIdx.y = instance; time index and receiver slot from the step counter.
+__global__ void k_post_batch(const BatchPost *bp, const int *step)
+{
+  const BatchPost &b = bp[blockIdx.y];
+  const int n = *step;
+  if (n >= b.nt) return;
+  const int it = b.mode2 ? b.nt - 1 - n : n;
+  const int irec = b.rec_on && it % b.mt == 0 ? it / b.mt : -1;
+  if (!b.p.freesurface && b.p.stype != 1 && irec < 0) return;
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ix >= b.g.Nx) return;
+  post_column(b.g, b.f, b.p, ix, it, irec);
 }
 
 __global__ void k_snapshot(Grid g, Fields f, int kind, int x0, int z0, int nzo, int nxo, float *dst)
@@ -417,6 +453,18 @@ void launch_post(const StepArgs &a, const PostArgs &p, cudaStream_t st)
 {
   k_post<<<(a.g.Nx + 127) / 128, 128, 0, st>>>(a.g, a.f, p);
 }
+
+void launch_post_batch(const BatchPost *d, int n, int maxNx, const int *step, cudaStream_t st)
+{
+  if (n > 0) k_post_batch<<<dim3((maxNx + 127) / 128, n), 128, 0, st>>>(d, step);
+}
+
+void launch_sources_batch(const BatchSrc *d, int n, const int *step, cudaStream_t st)
+{
+  if (n > 0) k_sources_batch<<<n, 128, 0, st>>>(d, step);
+}
+
+void launch_advance(int *step, cudaStream_t st) { k_advance<<<1, 1, 0, st>>>(step); }
 
 void launch_snapshot(const StepArgs &a, int kind, int savew, float *dst, cudaStream_t st)
 {

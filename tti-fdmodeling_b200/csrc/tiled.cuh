@@ -29,6 +29,13 @@ struct alignas(64) HalfArgs {
   int undamped_ok;
   int freesurface;
   int *err;    // bit 4: a TMA wait timed out
+  int nt;      // batched launches: time steps of this instance (its CTAs idle once the step counter reaches it)
+  int tiles_z; // batched launches: tile rows of this instance's grid
+};
+
+// One CTA of a batched launch: instance `inst`, tile `tile` (row tile % tiles_z, column tile / tiles_z).
+struct Work {
+  int inst, tile;
 };
 
 // Encodes the 2D tensor map of one [Nx][ldz] field for the halo box.
@@ -37,6 +44,15 @@ bool encode_map(CUtensorMap *map, const Grid &g, float *field);
 dim3 grid(const Grid &g, int *z_base);
 cudaError_t launch_velocity(const HalfArgs &a, int variant, bool exact, cudaStream_t st);
 cudaError_t launch_stress(const HalfArgs &a, int variant, bool exact, cudaStream_t st);
+// Batched: one launch over all instances' tiles. `inst` (device) holds each
+// instance's arguments (z_base set), `work` (device) the CTA -> (instance, tile)
+// table; `step` (device) is the shared step counter.
+cudaError_t launch_velocity_batch(const HalfArgs *inst, const Work *work, int nwork, const int *step, int variant,
+                                  bool exact, cudaStream_t st);
+cudaError_t launch_stress_batch(const HalfArgs *inst, const Work *work, int nwork, const int *step, int variant,
+                                bool exact, cudaStream_t st);
+// Sets the kernels' shared-memory attributes (call before a stream capture).
+cudaError_t prepare_batch(int variant, bool exact);
 
 }  // namespace tiled
 }  // namespace ttifd

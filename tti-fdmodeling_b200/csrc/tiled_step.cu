@@ -72,12 +72,12 @@ static_assert((BZ * 4) % 16 == 0, "TMA inner box extent must be a multiple of 16
 struct Cells {
   int x0, z0, xc, zr;
 };
-__device__ __forceinline__ Cells cells_of(const HalfArgs &a)
+__device__ __forceinline__ Cells cells_of(const HalfArgs &a, int tz, int tx)
 {
   const int t = threadIdx.x;
   Cells c;
-  c.z0 = a.z_base + blockIdx.x * TZ;
-  c.x0 = a.x_base + blockIdx.y * TX;
+  c.z0 = a.z_base + tz * TZ;
+  c.x0 = a.x_base + tx * TX;
   c.xc = c.x0 + (TX / 4) * (t >> 7);
   c.zr = c.z0 + (t & 127);
   return c;
@@ -85,7 +85,7 @@ __device__ __forceinline__ Cells cells_of(const HalfArgs &a)
 
 // Issues the TMA copies of the halo boxes of `n` fields (origin row z0 - 8,
 // column x0 - xoff); waited for by wait_tiles.
-__device__ __forceinline__ void issue_tiles(const HalfArgs &a, float *sm, unsigned long long *bar, int n, int z0,
+__device__ __forceinline__ void issue_tiles(const CUtensorMap *map, float *sm, unsigned long long *bar, int n, int z0,
                                             int x0, int xoff)
 {
   constexpr unsigned BOX_BYTES = BX * BZ * 4;
@@ -97,7 +97,7 @@ __device__ __forceinline__ void issue_tiles(const HalfArgs &a, float *sm, unsign
   __syncthreads();
   if (t == 0) {
     mbar_arrive_expect_tx(bar, n * BOX_BYTES);
-    for (int f = 0; f < n; ++f) tma_load_2d(sm + f * FIELD, &a.map[f], z0 - 8, x0 - xoff, bar);
+    for (int f = 0; f < n; ++f) tma_load_2d(sm + f * FIELD, map + f, z0 - 8, x0 - xoff, bar);
   }
 }
 
@@ -123,15 +123,15 @@ __device__ __forceinline__ bool tile_undamped(const HalfArgs &a, const Cells &c)
          c.z0 + TZ <= g.Nz - g.E;
 }
 
+// Velocity update of tile (tz, tx); `map` holds the tensor maps of sxx, szz, sxz.
 template <int V, bool X>
-__global__ void __launch_bounds__(NT, 4) k_velocity_tiled(const __grid_constant__ HalfArgs a)
+__device__ __forceinline__ void velocity_tile(const HalfArgs &a, const CUtensorMap *map, float *sm, int tz, int tx)
 {
   using A = Ar<X>;
-  extern __shared__ __align__(128) float sm[];
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm + 3 * FIELD);
   const Grid &g = a.g;
-  const Cells c = cells_of(a);
-  issue_tiles(a, sm, bar, 3, c.z0, c.x0, 4);
+  const Cells c = cells_of(a, tz, tx);
+  issue_tiles(map, sm, bar, 3, c.z0, c.x0, 4);
   const int L = g.ldz;
   const bool und = tile_undamped(a, c);
   const int z = c.zr;
@@ -268,15 +268,15 @@ __device__ __forceinline__ void stress_store(const HalfArgs &a, size_t gi, float
   }
 }
 
+// Stress update of tile (tz, tx); `map` holds the tensor maps of vx, vz.
 template <int V, bool X>
-__global__ void __launch_bounds__(NT, 4) k_stress_tiled(const __grid_constant__ HalfArgs a)
+__device__ __forceinline__ void stress_tile(const HalfArgs &a, const CUtensorMap *map, float *sm, int tz, int tx)
 {
   using A = Ar<X>;
-  extern __shared__ __align__(128) float sm[];
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm + 2 * FIELD);
   const Grid &g = a.g;
-  const Cells c = cells_of(a);
-  issue_tiles(a, sm, bar, 2, c.z0, c.x0, 5);
+  const Cells c = cells_of(a, tz, tx);
+  issue_tiles(map, sm, bar, 2, c.z0, c.x0, 5);
   const bool und = tile_undamped(a, c);
   const int z = c.zr;
   const bool zin = z >= g.izStart && z < g.Nz - NH;
@@ -315,10 +315,65 @@ __global__ void __launch_bounds__(NT, 4) k_stress_tiled(const __grid_constant__ 
   }
 }
 
-template <typename K>
-cudaError_t launch_k(K kernel, const HalfArgs &a, int nfields, cudaStream_t st)
+// Batched launches copy the instance's arguments (less the tensor maps, which
+// TMA reads from global memory) into shared memory once per CTA: the fields are
+// then uniform shared loads that the in-place global stores cannot alias.
+constexpr int ARGS_OFF = 3 * FIELD + 16;  // floats: after the largest field set and its barrier
+constexpr size_t ARGS_BYTES = sizeof(HalfArgs);
+static_assert(ARGS_OFF % 16 == 0, "argument copy must be 16-byte aligned");
+static_assert(ARGS_BYTES % 16 == 0, "HalfArgs must be a whole number of 16-byte words");
+
+__device__ __forceinline__ const HalfArgs *stage_args(const HalfArgs *src, float *sm)
 {
-  const size_t bytes = (size_t)nfields * FIELD * sizeof(float) + 16;
+  HalfArgs *dst = reinterpret_cast<HalfArgs *>(sm + ARGS_OFF);
+  const int4 *s4 = reinterpret_cast<const int4 *>(src);
+  int4 *d4 = reinterpret_cast<int4 *>(dst);
+  for (int i = threadIdx.x; i < (int)(ARGS_BYTES / 16); i += blockDim.x) d4[i] = s4[i];
+  __syncthreads();
+  return dst;
+}
+
+template <int V, bool X>
+__global__ void __launch_bounds__(NT, 4) k_velocity_tiled(const __grid_constant__ HalfArgs a)
+{
+  extern __shared__ __align__(128) float sm[];
+  velocity_tile<V, X>(a, a.map, sm, blockIdx.x, blockIdx.y);
+}
+
+template <int V, bool X>
+__global__ void __launch_bounds__(NT, 4) k_stress_tiled(const __grid_constant__ HalfArgs a)
+{
+  extern __shared__ __align__(128) float sm[];
+  stress_tile<V, X>(a, a.map, sm, blockIdx.x, blockIdx.y);
+}
+
+template <int V, bool X>
+__global__ void __launch_bounds__(NT, 4) k_velocity_batch(const HalfArgs *__restrict__ inst,
+                                                          const Work *__restrict__ work, const int *step)
+{
+  extern __shared__ __align__(128) float sm[];
+  const Work w = work[blockIdx.x];
+  const HalfArgs *src = inst + w.inst;
+  if (*step >= src->nt) return;
+  const HalfArgs *a = stage_args(src, sm);
+  velocity_tile<V, X>(*a, src->map, sm, w.tile % a->tiles_z, w.tile / a->tiles_z);
+}
+
+template <int V, bool X>
+__global__ void __launch_bounds__(NT, 4) k_stress_batch(const HalfArgs *__restrict__ inst,
+                                                        const Work *__restrict__ work, const int *step)
+{
+  extern __shared__ __align__(128) float sm[];
+  const Work w = work[blockIdx.x];
+  const HalfArgs *src = inst + w.inst;
+  if (*step >= src->nt) return;
+  const HalfArgs *a = stage_args(src, sm);
+  stress_tile<V, X>(*a, src->map, sm, w.tile % a->tiles_z, w.tile / a->tiles_z);
+}
+
+template <typename K>
+cudaError_t set_attr(K kernel, size_t bytes)
+{
   static std::mutex mu;
   static const void *done[32];
   static int ndone = 0;
@@ -335,6 +390,15 @@ cudaError_t launch_k(K kernel, const HalfArgs &a, int nfields, cudaStream_t st)
       if (ndone < 32) done[ndone++] = (const void *)kernel;
     }
   }
+  return cudaSuccess;
+}
+
+template <typename K>
+cudaError_t launch_k(K kernel, const HalfArgs &a, int nfields, cudaStream_t st)
+{
+  const size_t bytes = (size_t)nfields * FIELD * sizeof(float) + 16;
+  cudaError_t e = set_attr(kernel, bytes);
+  if (e != cudaSuccess) return e;
   HalfArgs b = a;
   const dim3 gr = grid(a.g, &b.z_base);
   if (gr.x == 0 || gr.y == 0) return cudaSuccess;
@@ -394,6 +458,58 @@ cudaError_t launch_stress(const HalfArgs &a, int variant, bool exact, cudaStream
   if (variant == TTI_COORDINATE) return launch_k(k_stress_tiled<TTI_COORDINATE, false>, a, 2, st);
   if (variant == TTI_TENSOR) return launch_k(k_stress_tiled<TTI_TENSOR, false>, a, 2, st);
   return launch_k(k_stress_tiled<TTI_BOND, false>, a, 2, st);
+}
+
+constexpr size_t BATCH_SMEM = (size_t)ARGS_OFF * sizeof(float) + ARGS_BYTES;
+
+template <typename K>
+cudaError_t launch_batch_k(K kernel, const HalfArgs *inst, const Work *work, int nwork, const int *step,
+                           cudaStream_t st)
+{
+  cudaError_t e = set_attr(kernel, BATCH_SMEM);
+  if (e != cudaSuccess || nwork == 0) return e;
+  kernel<<<nwork, NT, BATCH_SMEM, st>>>(inst, work, step);
+  return cudaGetLastError();
+}
+
+template <bool X>
+cudaError_t velocity_batch_x(const HalfArgs *inst, const Work *work, int nwork, const int *step, int variant,
+                             cudaStream_t st)
+{
+  if (variant == TTI_COORDINATE) return launch_batch_k(k_velocity_batch<TTI_COORDINATE, X>, inst, work, nwork, step, st);
+  if (variant == TTI_TENSOR) return launch_batch_k(k_velocity_batch<TTI_TENSOR, X>, inst, work, nwork, step, st);
+  return launch_batch_k(k_velocity_batch<TTI_BOND, X>, inst, work, nwork, step, st);
+}
+
+template <bool X>
+cudaError_t stress_batch_x(const HalfArgs *inst, const Work *work, int nwork, const int *step, int variant,
+                           cudaStream_t st)
+{
+  if (variant == TTI_COORDINATE) return launch_batch_k(k_stress_batch<TTI_COORDINATE, X>, inst, work, nwork, step, st);
+  if (variant == TTI_TENSOR) return launch_batch_k(k_stress_batch<TTI_TENSOR, X>, inst, work, nwork, step, st);
+  return launch_batch_k(k_stress_batch<TTI_BOND, X>, inst, work, nwork, step, st);
+}
+
+cudaError_t launch_velocity_batch(const HalfArgs *inst, const Work *work, int nwork, const int *step, int variant,
+                                  bool exact, cudaStream_t st)
+{
+  return exact ? velocity_batch_x<true>(inst, work, nwork, step, variant, st)
+               : velocity_batch_x<false>(inst, work, nwork, step, variant, st);
+}
+
+cudaError_t launch_stress_batch(const HalfArgs *inst, const Work *work, int nwork, const int *step, int variant,
+                                bool exact, cudaStream_t st)
+{
+  return exact ? stress_batch_x<true>(inst, work, nwork, step, variant, st)
+               : stress_batch_x<false>(inst, work, nwork, step, variant, st);
+}
+
+cudaError_t prepare_batch(int variant, bool exact)
+{
+  // a launch over zero CTAs only sets the attributes
+  cudaError_t e = launch_velocity_batch(nullptr, nullptr, 0, nullptr, variant, exact, nullptr);
+  if (e == cudaSuccess) e = launch_stress_batch(nullptr, nullptr, 0, nullptr, variant, exact, nullptr);
+  return e;
 }
 
 }  // namespace tiled

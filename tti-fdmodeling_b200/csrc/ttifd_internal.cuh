@@ -86,6 +86,7 @@ struct tti_handle {
   float *fld2[8] = {};  // second set: the fused step reads fld and writes fld2, then swaps
   bool use_fused = false;
   bool use_tiled = false;  // tiled half-step kernels with TMA halo tiles (in place)
+  const tti_handle *owner = nullptr;  // set when the parameter arrays belong to another handle (batched shots)
   void *tmaps = nullptr;   // host copy of the 5 tensor maps (vx vz sxx szz sxz), 64-byte aligned
   int seg = 0;          // columns per CTA of the fused step
   int bz = 0;           // rows per band of the fused step

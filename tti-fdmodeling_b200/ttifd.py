@@ -78,6 +78,21 @@ _SIGNATURES = {
     "snapshot_static": (C.c_int, [C.c_void_p, C.c_int, _FP]),
 }
 
+_BATCH_SIGNATURES = {
+    "batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(Config), C.c_int, _IP, C.c_int]),
+    "batch_destroy": (C.c_int, [C.c_void_p]),
+    "batch_last_error": (C.c_char_p, [C.c_void_p]),
+    "batch_instance": (C.c_void_p, [C.c_void_p, C.c_int]),
+    "batch_upload_model": (C.c_int, [C.c_void_p, C.c_int] + [_FP] * 6),
+    "batch_set_order": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "batch_autotune": (C.c_int, [C.c_void_p, C.c_int, _IP, _IP, _FP]),
+    "batch_reset": (C.c_int, [C.c_void_p]),
+    "batch_step": (C.c_int, [C.c_void_p, C.c_int]),
+    "batch_run": (C.c_int, [C.c_void_p]),
+    "batch_elapsed_ms": (C.c_int, [C.c_void_p, _FP]),
+    "batch_kernel_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+}
+_SIGNATURES.update(_BATCH_SIGNATURES)
 EXPORTS = ["tti_" + k for k in _SIGNATURES]
 
 _lib = None
@@ -240,3 +255,105 @@ class Modeling:
         ep = np.empty(self.cfg.nt, np.float32)
         self._call("fetch_energy", self._h, _f(ek), _f(ep))
         return ek, ep
+
+
+class Instance(Modeling):
+    """A shot of a batch: the batch's own handle, wrapped without ownership
+    (set_source, set_receivers and fetch_traces act on it as on a single shot)."""
+
+    def __init__(self, batch: "Batch", index: int, cfg: Config):
+        self.lib = batch.lib
+        self.cfg = cfg
+        self._batch = batch  # keeps the batch (and the handle) alive
+        self._h = C.c_void_p(self.lib.tti_batch_instance(batch._b, index))
+        if not self._h:
+            raise TTIError(ERR_ARG, f"no instance {index}")
+        nz, nx, e = C.c_int(), C.c_int(), C.c_int()
+        self._call("grid", self._h, C.byref(nz), C.byref(nx), C.byref(e))
+        self.Nz, self.Nx, self.E = nz.value, nx.value, e.value
+        self.nts = (self.cfg.nt - 1) // self.cfg.mt + 1
+        self._nrec = {}
+
+    def close(self):
+        self._h = C.c_void_p()
+
+
+class Batch:
+    """Many instances (shots of one or more models) advanced together
+    (tti_batch_*). `models` is a list of config dicts; `model_of[i]` is the
+    model of instance i."""
+
+    def __init__(self, models, model_of, device: int = 0, lib: C.CDLL | None = None):
+        self.lib = lib or load()
+        self.cfgs = [Config.make(**m) for m in models]
+        arr = (Config * len(self.cfgs))(*self.cfgs)
+        mo = np.ascontiguousarray(model_of, dtype=np.int32)
+        self._b = C.c_void_p()
+        self._call("batch_create", C.byref(self._b), len(self.cfgs), arr, mo.size, _i(mo), device, handle=False)
+        self.model_of = [int(m) for m in mo]
+        self.instances = [Instance(self, i, self.cfgs[m]) for i, m in enumerate(self.model_of)]
+
+    def _call(self, name, *args, handle=True):
+        rc = getattr(self.lib, "tti_" + name)(*args)
+        if rc != OK:
+            msg = self.lib.tti_batch_last_error(self._b if handle else None)
+            raise TTIError(rc, (msg or b"").decode(errors="replace"))
+        return rc
+
+    def close(self):
+        if self._b:
+            for inst in getattr(self, "instances", []):
+                inst.close()
+            self.lib.tti_batch_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload_model(self, m, vp, vs, rho, epsilon, delta, theta):
+        inst = self.instances[self.model_of.index(m)]
+        arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (vp, vs, rho, epsilon, delta, theta)]
+        for a in arrs:
+            if a.shape != (inst.Nx, inst.Nz):
+                raise ValueError(f"model arrays must be padded (Nx, Nz) = {(inst.Nx, inst.Nz)}, got {a.shape}")
+        self._call("batch_upload_model", self._b, m, *[_f(a) for a in arrs])
+
+    def set_order(self, group: int, graph_steps: int):
+        """Shots interleaved per tile in groups of `group` (0: all); graph of `graph_steps` steps (0: none)."""
+        self._call("batch_set_order", self._b, group, graph_steps)
+
+    def autotune(self, nsteps: int) -> dict:
+        """Times the schedules on nsteps steps, keeps the fastest, resets the batch."""
+        g, gs, ms = C.c_int(), C.c_int(), C.c_float()
+        self._call("batch_autotune", self._b, nsteps, C.byref(g), C.byref(gs), C.byref(ms))
+        return {"group": g.value, "graph_steps": gs.value, "ms_per_step": ms.value}
+
+    def reset(self):
+        self._call("batch_reset", self._b)
+
+    def step(self, n: int):
+        self._call("batch_step", self._b, n)
+
+    def run(self):
+        self._call("batch_run", self._b)
+
+    @property
+    def elapsed_ms(self) -> float:
+        v = C.c_float()
+        self._call("batch_elapsed_ms", self._b, C.byref(v))
+        return v.value
+
+    @property
+    def kernel_launches(self) -> int:
+        v = C.c_longlong()
+        self._call("batch_kernel_launches", self._b, C.byref(v))
+        return v.value
