@@ -183,6 +183,34 @@ int tti_fetch_field(tti_handle *h, int which, float *out);
 /* Energy per step (energy = 1): Ek[nt], Ep[nt] (coord:898-924, 942-968). */
 int tti_fetch_energy(tti_handle *h, float *ek, float *ep);
 
+/* ---- Adjoint-state gradient ---------------------------------------------------
+ * The reference has no adjoint; these entry points add one for the coordinate
+ * formulation with the stress source (stype 1). Misfit
+ *   J = 1/2 sum over the recorded samples of (d - dobs)^2
+ * (the components seistype records). tti_grad_run runs the forward loop,
+ * keeping `ncheck` checkpoints, then the discrete adjoint of the loop
+ * backwards, recomputing the forward states segment by segment from the
+ * checkpoints, and ADDS the shot's gradient to the handle's sums (so several
+ * shots accumulate; tti_grad_zero clears them). Conventions: vs and rho are
+ * held fixed; the MEAL arrays coef1, coef2, Beta stay those of the uploaded
+ * model. Gradients are per padded cell, [Nx][Nz], theta in degrees. */
+#define TTI_G_VP 0
+#define TTI_G_EPS 1
+#define TTI_G_DELTA 2
+#define TTI_G_THETA 3
+/* Observed traces of one recorded component, [ntrace][(nt-1)/mt+1]. */
+int tti_grad_set_observed(tti_handle *h, int kind, const float *dobs);
+int tti_grad_zero(tti_handle *h);
+int tti_grad_run(tti_handle *h, int ncheck, double *misfit);
+int tti_grad_fetch(tti_handle *h, int which, float *out);
+/* dJ/d(source samples) of the last run, [nsrc][nt]. */
+int tti_grad_fetch_source(tti_handle *h, float *out);
+/* Device pointers of the 7 gradient sums (c11, c13, c33, c55, theta at the
+ * stress node, sin/cos theta at the velocity node), each `count` floats of
+ * [Nx][pitch] layout: a multi-GPU caller all-reduces them in place (the chain
+ * rule in tti_grad_fetch is linear in them). */
+int tti_grad_accumulators(tti_handle *h, float **dev, size_t *count, size_t *pitch);
+
 /* ---- Batched execution ------------------------------------------------------
  * Many shots (and many models, of different sizes and nt) advanced together:
  * each half-step is one launch over every instance's tiles, and the time loop

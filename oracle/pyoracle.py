@@ -146,3 +146,103 @@ def ref_binary(variant: str, strict: bool = True) -> str | None:
     """Path of the reference program built from the reference's sources, or None."""
     p = os.path.join(REF_DIR, "strict" if strict else "bin", f"sufdmod2dTTIelastic_{variant}")
     return p if os.path.exists(p) else None
+
+
+# ---------------------------------------------------------------- adjoint (double precision)
+_DP = C.POINTER(C.c_double)
+_ADJ_SIG = {
+    "adj_create": (C.c_void_p, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
+                                C.c_int, C.c_int, C.c_double]),
+    "adj_destroy": (None, [C.c_void_p]),
+    "adj_grid": (None, [C.c_void_p, _IP, _IP, _IP]),
+    "adj_set_meal": (None, [C.c_void_p, _FP, _FP, _FP]),
+    "adj_set_model": (None, [C.c_void_p] + [_DP] * 6),
+    "adj_set_source": (None, [C.c_void_p, C.c_int, _IP, _IP, _DP]),
+    "adj_set_receivers": (None, [C.c_void_p, C.c_int, C.c_int, _IP, _IP]),
+    "adj_forward": (None, [C.c_void_p, C.POINTER(_DP)]),
+    "adj_gradient": (C.c_double, [C.c_void_p, C.POINTER(_DP), _DP, _DP, _DP, _DP, _DP]),
+}
+
+
+def _d(a):
+    return a.ctypes.data_as(_DP)
+
+
+class AdjointOracle:
+    """Double-precision forward and adjoint-state gradient of the coordinate
+    formulation (oracle/ttifd_adjoint.c), stress source only. MEAL coef1, coef2
+    and Beta are frozen from the float setup of `meal_model` (padded arrays);
+    vs and rho stay fixed; the model (vp, eps, delta, theta) can be changed
+    with set_model for finite differences."""
+
+    def __init__(self, cfg: dict, meal_model):
+        lib = load()
+        for name, (res, args) in _ADJ_SIG.items():
+            fn = getattr(lib, name)
+            fn.restype, fn.argtypes = res, args
+        self.lib = lib
+        self.cfg = dict(cfg)
+        c = self.cfg
+        self._c = lib.adj_create(c["nz"], c["nx"], c["nt"], c["dx"], c["dz"], c["dt"], c["ealThick"],
+                                 c.get("freesurface", 0), c.get("mt", 1), c["seistype"], c.get("scalar", 1.0))
+        nz, nx, nts = C.c_int(), C.c_int(), C.c_int()
+        lib.adj_grid(self._c, C.byref(nz), C.byref(nx), C.byref(nts))
+        self.Nz, self.Nx, self.nts = nz.value, nx.value, nts.value
+        with Oracle(**dict(c, variant="coordinate_rotation", stype=1, wsave=0, energy=0)) as o:
+            o.upload_model(*meal_model)
+            meal = [np.ascontiguousarray(o.fetch_param(p)) for p in ("coef1", "coef2", "Beta")]
+        lib.adj_set_meal(self._c, *[_f(a) for a in meal])
+        self._nrec = {}
+        self.nsrc = 0
+
+    def close(self):
+        if self._c:
+            self.lib.adj_destroy(self._c)
+            self._c = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_model(self, vp, vs, rho, eps, delta, theta):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (vp, vs, rho, eps, delta, theta)]
+        for a in arrs:
+            assert a.shape == (self.Nx, self.Nz)
+        self._model = arrs
+        self.lib.adj_set_model(self._c, *[_d(a) for a in arrs])
+
+    def set_source(self, sx, sz, w):
+        w = np.ascontiguousarray(np.atleast_2d(w), dtype=np.float64)
+        x = np.ascontiguousarray(np.atleast_1d(sx), dtype=np.int32)
+        z = np.ascontiguousarray(np.atleast_1d(sz), dtype=np.int32)
+        self._src = w
+        self.nsrc = x.size
+        self.lib.adj_set_source(self._c, x.size, _i(x), _i(z), _d(w))
+
+    def set_receivers(self, kind, gx, gz):
+        x = np.ascontiguousarray(gx, dtype=np.int32)
+        z = np.ascontiguousarray(np.broadcast_to(gz, x.shape), dtype=np.int32)
+        self._nrec[kind] = x.size
+        self.lib.adj_set_receivers(self._c, kind, x.size, _i(x), _i(z))
+
+    def _rec_arrays(self):
+        out = [np.zeros((self._nrec.get(k, 0), self.nts)) if self._nrec.get(k) else None for k in range(3)]
+        ptrs = (_DP * 3)(*[_d(a) if a is not None else _DP() for a in out])
+        return out, ptrs
+
+    def forward(self):
+        """Traces per component ([ntrace][nts] or None)."""
+        out, ptrs = self._rec_arrays()
+        self.lib.adj_forward(self._c, ptrs)
+        return out
+
+    def gradient(self, dobs):
+        """(J, {vp, eps, delta, theta: [Nx][Nz]}, g_src[nsrc][nt])."""
+        obs = [np.ascontiguousarray(d, dtype=np.float64) if d is not None else None for d in dobs]
+        ptrs = (_DP * 3)(*[_d(a) if a is not None else _DP() for a in obs])
+        g = {k: np.zeros((self.Nx, self.Nz)) for k in ("vp", "eps", "delta", "theta")}
+        gs = np.zeros((max(self.nsrc, 1), self.cfg["nt"]))
+        J = self.lib.adj_gradient(self._c, ptrs, _d(g["vp"]), _d(g["eps"]), _d(g["delta"]), _d(g["theta"]), _d(gs))
+        return J, g, gs[:self.nsrc]

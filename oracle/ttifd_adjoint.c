@@ -1,0 +1,552 @@
+/*
+ * ttifd_adjoint.c -- CPU reference of the adjoint-state gradient, in double
+ * precision (TEST INFRASTRUCTURE: the checker of the device gradient, never
+ * part of the product path).
+ *
+ * The reference (wavetomo/TTI-FDModeling) has no adjoint. This file states the
+ * discrete adjoint of its coordinate-rotation time step
+ * (src/main/sufdmod2dTTIelastic/sufdmod2dTTIelastic_coordinate_rotation.c:
+ * velocity update :614-672, stress update :804-845, free surface :847-863,
+ * stress source :865-886, receivers isoelastic.c:103-144) and of its
+ * stiffness build (:497-537), so that
+ *   J = 1/2 sum over recorded samples (d - dobs)^2
+ * has gradients with respect to vp, epsilon, delta and theta (degrees) at
+ * every padded cell. Conventions: vs and rho are held fixed; the MEAL arrays
+ * coef1, coef2 and Beta are frozen (given, from the float setup of a
+ * reference model); stiffness uses vp/Beta, vs/Beta, rho*Beta (meal.c:450-490).
+ * Only the stress source (stype 1) is modelled. The forward states are all
+ * kept in memory (small test grids).
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "ttifd_adjoint.h"
+
+#define NH 5
+static const double RSGC[5] = {1.24362739770907f, -0.114021164233934f, 0.0272965993810630f, -0.00699199493927320f,
+                               0.00132022981661381f};
+
+struct adj_ctx {
+  int nz, nx, nt, E, Nz, Nx, izs, fs, mt, seistype, nts;
+  double dx, dz, dt, scalar;
+  size_t Np;
+  /* frozen MEAL */
+  double *coef1, *coef2, *beta;
+  /* model and derived arrays */
+  double *vp, *vs, *rho, *eps, *delta, *theta;  /* as given (padded) */
+  double *c11, *c13, *c33, *c55, *sn, *cs, *snv, *csv, *ir;
+  /* geometry */
+  int nsrc, *sx, *sz;
+  double *src; /* [nsrc][nt] */
+  int nrec[3], *rx[3], *rz[3];
+};
+
+#define A2(a, ix, iz) ((a)[(size_t)(ix) * (size_t)c->Nz + (size_t)(iz)])
+
+static double *dalloc(size_t n) { return (double *)calloc(n ? n : 1, sizeof(double)); }
+
+adj_ctx *adj_create(int nz, int nx, int nt, double dx, double dz, double dt, int ealThick, int freesurface, int mt,
+                    int seistype, double scalar)
+{
+  adj_ctx *c = (adj_ctx *)calloc(1, sizeof(adj_ctx));
+  c->nz = nz;
+  c->nx = nx;
+  c->nt = nt;
+  c->E = ealThick + NH;
+  c->Nz = nz + 2 * c->E;
+  c->Nx = nx + 2 * c->E;
+  c->izs = freesurface ? c->E : NH;
+  c->fs = freesurface;
+  c->mt = mt;
+  c->seistype = seistype;
+  c->nts = (nt - 1) / mt + 1;
+  c->dx = dx;
+  c->dz = dz;
+  c->dt = dt;
+  c->scalar = scalar;
+  c->Np = (size_t)c->Nz * c->Nx;
+  double **arrs[] = {&c->coef1, &c->coef2, &c->beta, &c->vp, &c->vs, &c->rho, &c->eps, &c->delta, &c->theta,
+                     &c->c11,   &c->c13,   &c->c33,  &c->c55, &c->sn, &c->cs,  &c->snv, &c->csv,   &c->ir};
+  for (size_t k = 0; k < sizeof arrs / sizeof arrs[0]; ++k) *arrs[k] = dalloc(c->Np);
+  return c;
+}
+
+void adj_destroy(adj_ctx *c)
+{
+  if (!c) return;
+  double *arrs[] = {c->coef1, c->coef2, c->beta, c->vp, c->vs,  c->rho, c->eps, c->delta, c->theta,
+                    c->c11,   c->c13,   c->c33,  c->c55, c->sn, c->cs,  c->snv, c->csv,   c->ir};
+  for (size_t k = 0; k < sizeof arrs / sizeof arrs[0]; ++k) free(arrs[k]);
+  free(c->sx);
+  free(c->sz);
+  free(c->src);
+  for (int k = 0; k < 3; ++k) {
+    free(c->rx[k]);
+    free(c->rz[k]);
+  }
+  free(c);
+}
+
+void adj_grid(const adj_ctx *c, int *Nz, int *Nx, int *nts)
+{
+  *Nz = c->Nz;
+  *Nx = c->Nx;
+  *nts = c->nts;
+}
+
+void adj_set_meal(adj_ctx *c, const float *coef1, const float *coef2, const float *beta)
+{
+  for (size_t i = 0; i < c->Np; ++i) {
+    c->coef1[i] = coef1[i];
+    c->coef2[i] = coef2[i];
+    c->beta[i] = beta[i];
+  }
+}
+
+/* stiffness and angles (coord:497-537) from the model in double */
+void adj_set_model(adj_ctx *c, const double *vp, const double *vs, const double *rho, const double *eps,
+                   const double *delta, const double *theta)
+{
+  const size_t Np = c->Np;
+  memcpy(c->vp, vp, Np * sizeof(double));
+  memcpy(c->vs, vs, Np * sizeof(double));
+  memcpy(c->rho, rho, Np * sizeof(double));
+  memcpy(c->eps, eps, Np * sizeof(double));
+  memcpy(c->delta, delta, Np * sizeof(double));
+  memcpy(c->theta, theta, Np * sizeof(double));
+  for (size_t i = 0; i < Np; ++i) {
+    const double B = c->beta[i];
+    const double p = vp[i] / B, s = vs[i] / B, r = rho[i] * B;
+    const double f = 1.0 - (s / p) * (s / p);
+    c->c11[i] = r * p * p * (1.0 + 2.0 * eps[i]);
+    c->c13[i] = r * (p * p * sqrt(f * (f + 2.0 * delta[i])) - s * s);
+    c->c33[i] = r * p * p;
+    c->c55[i] = r * s * s;
+    const double th = c->scalar * theta[i] / 180.0 * M_PI;
+    c->sn[i] = sin(th);
+    c->cs[i] = cos(th);
+  }
+  for (int ix = 0; ix < c->Nx; ++ix)
+    for (int iz = 0; iz < c->Nz; ++iz) {
+      const int inner = ix < c->Nx - 1 && iz < c->Nz - 1;
+#define RB(x, z) (A2(c->rho, x, z) * A2(c->beta, x, z))
+      if (inner) {
+        A2(c->ir, ix, iz) = 4.0 / (RB(ix, iz) + RB(ix + 1, iz) + RB(ix, iz + 1) + RB(ix + 1, iz + 1));
+        A2(c->snv, ix, iz) =
+            0.25 * (A2(c->sn, ix, iz) + A2(c->sn, ix + 1, iz) + A2(c->sn, ix, iz + 1) + A2(c->sn, ix + 1, iz + 1));
+        A2(c->csv, ix, iz) =
+            0.25 * (A2(c->cs, ix, iz) + A2(c->cs, ix + 1, iz) + A2(c->cs, ix, iz + 1) + A2(c->cs, ix + 1, iz + 1));
+      } else {
+        A2(c->ir, ix, iz) = 1.0 / RB(ix, iz);
+        A2(c->snv, ix, iz) = A2(c->sn, ix, iz);
+        A2(c->csv, ix, iz) = A2(c->cs, ix, iz);
+      }
+#undef RB
+    }
+}
+
+void adj_set_source(adj_ctx *c, int n, const int *sx, const int *sz, const double *w)
+{
+  free(c->sx);
+  free(c->sz);
+  free(c->src);
+  c->nsrc = n;
+  c->sx = (int *)malloc(sizeof(int) * (n ? n : 1));
+  c->sz = (int *)malloc(sizeof(int) * (n ? n : 1));
+  c->src = dalloc((size_t)n * c->nt);
+  memcpy(c->sx, sx, sizeof(int) * n);
+  memcpy(c->sz, sz, sizeof(int) * n);
+  memcpy(c->src, w, sizeof(double) * (size_t)n * c->nt);
+}
+
+void adj_set_receivers(adj_ctx *c, int kind, int n, const int *gx, const int *gz)
+{
+  free(c->rx[kind]);
+  free(c->rz[kind]);
+  c->nrec[kind] = n;
+  c->rx[kind] = (int *)malloc(sizeof(int) * (n ? n : 1));
+  c->rz[kind] = (int *)malloc(sizeof(int) * (n ? n : 1));
+  memcpy(c->rx[kind], gx, sizeof(int) * n);
+  memcpy(c->rz[kind], gz, sizeof(int) * n);
+}
+
+/* ---------------------------------------------------------------- stencils */
+/* velocity-node pair (coord:621-630) and stress-node pair (coord:811-816) */
+static void dv(const adj_ctx *c, const double *a, int ix, int iz, double *d1, double *d2)
+{
+  double s1 = 0.0, s2 = 0.0;
+  for (int k = 1; k <= NH; ++k) {
+    s1 += RSGC[k - 1] * (A2(a, ix + k, iz + k) - A2(a, ix - k + 1, iz - k + 1));
+    s2 += RSGC[k - 1] * (A2(a, ix + k, iz - k + 1) - A2(a, ix - k + 1, iz + k));
+  }
+  *d1 = s1;
+  *d2 = s2;
+}
+
+static void ds(const adj_ctx *c, const double *a, int ix, int iz, double *d1, double *d2)
+{
+  double s1 = 0.0, s2 = 0.0;
+  for (int k = 1; k <= NH; ++k) {
+    s1 += RSGC[k - 1] * (A2(a, ix + k - 1, iz + k - 1) - A2(a, ix - k, iz - k));
+    s2 += RSGC[k - 1] * (A2(a, ix + k - 1, iz - k) - A2(a, ix - k, iz + k - 1));
+  }
+  *d1 = s1;
+  *d2 = s2;
+}
+
+static double src_weight(const adj_ctx *c, int a, int b)
+{
+  const double alpha = log(0.8) / (c->dx * c->dx + c->dz * c->dz);
+  const double rx = a * c->dx, rz = b * c->dz;
+  return exp(alpha * (rx * rx + rz * rz)) / (c->dx * c->dz) * c->dt;
+}
+
+/* ---------------------------------------------------------------- forward */
+typedef struct {
+  double *vx, *vz, *sxx, *szz, *sxz;
+} state;
+
+static void velocity_half(const adj_ctx *c, state *u)
+{
+  const double hx = 0.5 / c->dx, hz = 0.5 / c->dz;
+  for (int ix = NH; ix < c->Nx - NH; ++ix)
+    for (int iz = c->izs; iz < c->Nz - NH; ++iz) {
+      double a1, a2, b1, b2, e1, e2;
+      dv(c, u->sxx, ix, iz, &a1, &a2);
+      dv(c, u->szz, ix, iz, &b1, &b2);
+      dv(c, u->sxz, ix, iz, &e1, &e2);
+      const double sxx_x = hx * (a1 + a2), sxx_z = hx * (a1 - a2); /* coord:633 uses 1/dx */
+      const double szz_x = hx * (b1 + b2), szz_z = hz * (b1 - b2);
+      const double sxz_x = hx * (e1 + e2), sxz_z = hz * (e1 - e2);
+      const size_t i = (size_t)ix * c->Nz + iz;
+      const double cv = c->csv[i], sv = c->snv[i], br = c->coef2[i] * c->ir[i];
+      u->vx[i] = c->coef1[i] * u->vx[i] + br * (cv * sxx_x - sv * sxx_z + sv * sxz_x + cv * sxz_z);
+      u->vz[i] = c->coef1[i] * u->vz[i] + br * (cv * sxz_x - sv * sxz_z + sv * szz_x + cv * szz_z);
+    }
+}
+
+static void stress_half(const adj_ctx *c, state *u)
+{
+  const double hx = 0.5 / c->dx, hz = 0.5 / c->dz;
+  for (int ix = NH; ix < c->Nx - NH; ++ix)
+    for (int iz = c->izs; iz < c->Nz - NH; ++iz) {
+      double a1, a2, b1, b2;
+      ds(c, u->vx, ix, iz, &a1, &a2);
+      ds(c, u->vz, ix, iz, &b1, &b2);
+      double vxx = hx * (a1 + a2), vxz = hz * (a1 - a2), vzx = hx * (b1 + b2), vzz = hz * (b1 - b2);
+      const size_t i = (size_t)ix * c->Nz + iz;
+      const double s = c->sn[i], co = c->cs[i];
+      const double rxx = co * vxx - s * vxz, rxz = s * vxx + co * vxz;
+      const double rzx = co * vzx - s * vzz, rzz = s * vzx + co * vzz;
+      const double a = c->coef1[i], b = c->coef2[i];
+      u->sxx[i] = a * u->sxx[i] + b * (c->c11[i] * rxx + c->c13[i] * rzz);
+      u->szz[i] = a * u->szz[i] + b * (c->c13[i] * rxx + c->c33[i] * rzz);
+      u->sxz[i] = a * u->sxz[i] + b * c->c55[i] * (rzx + rxz);
+    }
+}
+
+static void free_surface(const adj_ctx *c, state *u)
+{
+  const int s = c->izs;
+  for (int ix = NH; ix < c->Nx - NH; ++ix) {
+    A2(u->sxz, ix, s) = 0.0;
+    A2(u->szz, ix, s) = 0.0;
+    for (int k = 1; k <= NH; ++k) {
+      A2(u->sxx, ix, s - k) = 2.0 * A2(u->sxx, ix, s) - A2(u->sxx, ix, s + k);
+      A2(u->szz, ix, s - k) = -A2(u->szz, ix, s + k);
+      A2(u->sxz, ix, s - k) = -A2(u->sxz, ix, s + k);
+    }
+  }
+}
+
+static void stress_source(const adj_ctx *c, state *u, int it)
+{
+  for (int n = 0; n < c->nsrc; ++n) {
+    const int x0 = c->sx[n] + c->E, z0 = c->sz[n] + c->E;
+    const double w = c->src[(size_t)n * c->nt + it];
+    for (int a = -NH; a <= NH; ++a)
+      for (int b = -NH; b <= NH; ++b) {
+        const int ix = x0 + a, iz = z0 + b;
+        if (ix < 0 || ix >= c->Nx || iz < 0 || iz >= c->Nz) continue;
+        const double k = 0.5 * src_weight(c, a, b) * w;
+        A2(u->sxx, ix, iz) += k;
+        A2(u->szz, ix, iz) += k;
+      }
+  }
+}
+
+static int want(const adj_ctx *c, int k)
+{
+  return k < 2 ? (c->seistype == 1 || c->seistype == 3) : (c->seistype == 2 || c->seistype == 3);
+}
+
+static void record(const adj_ctx *c, const state *u, int it, double *rec[3])
+{
+  if (c->seistype <= 0 || it % c->mt != 0) return;
+  const int j = it / c->mt;
+  for (int k = 0; k < 3; ++k) {
+    if (!want(c, k) || !rec[k]) continue;
+    for (int t = 0; t < c->nrec[k]; ++t) {
+      const int x = c->rx[k][t] + c->E, z = c->rz[k][t] + c->E;
+      double v;
+      if (k == 0) v = A2(u->vx, x, z);
+      else if (k == 1) v = A2(u->vz, x, z);
+      else v = 0.5 * (A2(u->sxx, x, z) + A2(u->szz, x, z));
+      rec[k][(size_t)t * c->nts + j] = v;
+    }
+  }
+}
+
+static state state_alloc(size_t n)
+{
+  state s = {dalloc(n), dalloc(n), dalloc(n), dalloc(n), dalloc(n)};
+  return s;
+}
+
+static void state_free(state *s)
+{
+  free(s->vx);
+  free(s->vz);
+  free(s->sxx);
+  free(s->szz);
+  free(s->sxz);
+}
+
+/* one step; `keep` (may be NULL) receives (v after the velocity half, sigma
+ * before the stress half), the two states the adjoint step reads */
+static void step(const adj_ctx *c, state *u, int it, double *rec[3], state *keep)
+{
+  velocity_half(c, u);
+  if (keep) {
+    memcpy(keep->vx, u->vx, c->Np * sizeof(double));
+    memcpy(keep->vz, u->vz, c->Np * sizeof(double));
+    memcpy(keep->sxx, u->sxx, c->Np * sizeof(double));
+    memcpy(keep->szz, u->szz, c->Np * sizeof(double));
+    memcpy(keep->sxz, u->sxz, c->Np * sizeof(double));
+  }
+  stress_half(c, u);
+  if (c->fs) free_surface(c, u);
+  stress_source(c, u, it);
+  record(c, u, it, rec);
+}
+
+void adj_forward(adj_ctx *c, double *rec[3])
+{
+  state u = state_alloc(c->Np);
+  for (int it = 0; it < c->nt; ++it) step(c, &u, it, rec, NULL);
+  state_free(&u);
+}
+
+/* ---------------------------------------------------------------- adjoint */
+double adj_gradient(adj_ctx *c, const double *dobs[3], double *g_vp, double *g_eps, double *g_delta,
+                    double *g_theta, double *g_src)
+{
+  const size_t Np = c->Np;
+  const int Nz = c->Nz, Nx = c->Nx, izs = c->izs;
+  const double hx = 0.5 / c->dx, hz = 0.5 / c->dz;
+  double *rec[3] = {NULL, NULL, NULL};
+  for (int k = 0; k < 3; ++k)
+    if (want(c, k) && c->nrec[k] > 0) rec[k] = dalloc((size_t)c->nrec[k] * c->nts);
+  /* forward, keeping every step's (v_new, sigma_old) */
+  state *keep = (state *)malloc(sizeof(state) * c->nt);
+  state u = state_alloc(Np);
+  for (int it = 0; it < c->nt; ++it) {
+    keep[it] = state_alloc(Np);
+    step(c, &u, it, rec, &keep[it]);
+  }
+  state_free(&u);
+  /* residuals and misfit */
+  double J = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    if (!rec[k]) continue;
+    for (size_t q = 0; q < (size_t)c->nrec[k] * c->nts; ++q) {
+      rec[k][q] -= dobs[k][q];
+      J += 0.5 * rec[k][q] * rec[k][q];
+    }
+  }
+  /* adjoint state and work arrays */
+  state L = state_alloc(Np);
+  double *T[6];
+  for (int k = 0; k < 6; ++k) T[k] = dalloc(Np);
+  double *gc11 = dalloc(Np), *gc13 = dalloc(Np), *gc33 = dalloc(Np), *gc55 = dalloc(Np), *gth = dalloc(Np);
+  double *gsv = dalloc(Np), *gcv = dalloc(Np);
+  if (g_src) memset(g_src, 0, sizeof(double) * (size_t)c->nsrc * c->nt);
+  for (int it = c->nt - 1; it >= 0; --it) {
+    const state *f = &keep[it];
+    /* residual injection (adjoint of record) */
+    if (c->seistype > 0 && it % c->mt == 0) {
+      const int j = it / c->mt;
+      for (int k = 0; k < 3; ++k) {
+        if (!rec[k]) continue;
+        for (int t = 0; t < c->nrec[k]; ++t) {
+          const int x = c->rx[k][t] + c->E, z = c->rz[k][t] + c->E;
+          const double r = rec[k][(size_t)t * c->nts + j];
+          if (k == 0) A2(L.vx, x, z) += r;
+          else if (k == 1) A2(L.vz, x, z) += r;
+          else {
+            A2(L.sxx, x, z) += 0.5 * r;
+            A2(L.szz, x, z) += 0.5 * r;
+          }
+        }
+      }
+    }
+    /* source-wavelet gradient (adjoint of the stress source) */
+    if (g_src)
+      for (int n = 0; n < c->nsrc; ++n) {
+        const int x0 = c->sx[n] + c->E, z0 = c->sz[n] + c->E;
+        double acc = 0.0;
+        for (int a = -NH; a <= NH; ++a)
+          for (int b = -NH; b <= NH; ++b) {
+            const int ix = x0 + a, iz = z0 + b;
+            if (ix < 0 || ix >= Nx || iz < 0 || iz >= Nz) continue;
+            acc += 0.5 * src_weight(c, a, b) * (A2(L.sxx, ix, iz) + A2(L.szz, ix, iz));
+          }
+        g_src[(size_t)n * c->nt + it] = acc;
+      }
+    /* adjoint of the free surface */
+    if (c->fs)
+      for (int ix = NH; ix < Nx - NH; ++ix) {
+        for (int k = 1; k <= NH; ++k) {
+          A2(L.sxx, ix, izs) += 2.0 * A2(L.sxx, ix, izs - k);
+          A2(L.sxx, ix, izs + k) -= A2(L.sxx, ix, izs - k);
+          A2(L.sxx, ix, izs - k) = 0.0;
+          A2(L.szz, ix, izs + k) -= A2(L.szz, ix, izs - k);
+          A2(L.szz, ix, izs - k) = 0.0;
+          A2(L.sxz, ix, izs + k) -= A2(L.sxz, ix, izs - k);
+          A2(L.sxz, ix, izs - k) = 0.0;
+        }
+        A2(L.sxz, ix, izs) = 0.0;
+        A2(L.szz, ix, izs) = 0.0;
+      }
+    /* adjoint of the stress half: gradient terms, then T = d(sigma)/d(strain)^T lambda */
+    for (int k = 0; k < 4; ++k) memset(T[k], 0, Np * sizeof(double));
+    for (int ix = NH; ix < Nx - NH; ++ix)
+      for (int iz = izs; iz < Nz - NH; ++iz) {
+        const size_t i = (size_t)ix * Nz + iz;
+        double a1, a2, b1, b2;
+        ds(c, f->vx, ix, iz, &a1, &a2);
+        ds(c, f->vz, ix, iz, &b1, &b2);
+        const double vxx = hx * (a1 + a2), vxz = hz * (a1 - a2), vzx = hx * (b1 + b2), vzz = hz * (b1 - b2);
+        const double s = c->sn[i], co = c->cs[i];
+        const double rxx = co * vxx - s * vxz, rxz = s * vxx + co * vxz;
+        const double rzx = co * vzx - s * vzz, rzz = s * vzx + co * vzz;
+        const double la = L.sxx[i], lb = L.szz[i], le = L.sxz[i], b = c->coef2[i];
+        const double c11 = c->c11[i], c13 = c->c13[i], c33 = c->c33[i], c55 = c->c55[i];
+        gc11[i] += b * la * rxx;
+        gc13[i] += b * (la * rzz + lb * rxx);
+        gc33[i] += b * lb * rzz;
+        gc55[i] += b * le * (rzx + rxz);
+        gth[i] += b * (la * (-c11 * rxz + c13 * rzx) + lb * (-c13 * rxz + c33 * rzx) + le * c55 * (rxx - rzz));
+        const double Lxx = b * (c11 * la + c13 * lb), Lzz = b * (c13 * la + c33 * lb), Lq = b * c55 * le;
+        T[0][i] = co * Lxx + s * Lq;   /* d/d vxx */
+        T[1][i] = -s * Lxx + co * Lq;  /* d/d vxz */
+        T[2][i] = co * Lq + s * Lzz;   /* d/d vzx */
+        T[3][i] = -s * Lq + co * Lzz;  /* d/d vzz */
+        L.sxx[i] *= c->coef1[i];
+        L.szz[i] *= c->coef1[i];
+        L.sxz[i] *= c->coef1[i];
+      }
+    /* transposed stress stencils onto the velocity nodes: minus the velocity-node pair */
+    for (int ix = NH; ix < Nx - NH; ++ix)
+      for (int iz = izs; iz < Nz - NH; ++iz) {
+        const size_t i = (size_t)ix * Nz + iz;
+        double p1, p2, q1, q2, r1, r2, s1, s2;
+        dv(c, T[0], ix, iz, &p1, &p2);
+        dv(c, T[1], ix, iz, &q1, &q2);
+        dv(c, T[2], ix, iz, &r1, &r2);
+        dv(c, T[3], ix, iz, &s1, &s2);
+        L.vx[i] -= hx * (p1 + p2) + hz * (q1 - q2);
+        L.vz[i] -= hx * (r1 + r2) + hz * (s1 - s2);
+      }
+    /* adjoint of the velocity half */
+    for (int k = 0; k < 6; ++k) memset(T[k], 0, Np * sizeof(double));
+    for (int ix = NH; ix < Nx - NH; ++ix)
+      for (int iz = izs; iz < Nz - NH; ++iz) {
+        const size_t i = (size_t)ix * Nz + iz;
+        double a1, a2, b1, b2, e1, e2;
+        dv(c, f->sxx, ix, iz, &a1, &a2);
+        dv(c, f->szz, ix, iz, &b1, &b2);
+        dv(c, f->sxz, ix, iz, &e1, &e2);
+        const double sxx_x = hx * (a1 + a2), sxx_z = hx * (a1 - a2);
+        const double szz_x = hx * (b1 + b2), szz_z = hz * (b1 - b2);
+        const double sxz_x = hx * (e1 + e2), sxz_z = hz * (e1 - e2);
+        const double br = c->coef2[i] * c->ir[i];
+        const double Fx = br * L.vx[i], Fz = br * L.vz[i];
+        const double cv = c->csv[i], sv = c->snv[i];
+        gsv[i] += Fx * (-sxx_z + sxz_x) + Fz * (-sxz_z + szz_x);
+        gcv[i] += Fx * (sxx_x + sxz_z) + Fz * (sxz_x + szz_z);
+        const double Axx_x = cv * Fx, Axx_z = -sv * Fx;
+        const double Axz_x = sv * Fx + cv * Fz, Axz_z = cv * Fx - sv * Fz;
+        const double Azz_x = sv * Fz, Azz_z = cv * Fz;
+        T[0][i] = hx * (Axx_x + Axx_z); /* sxx: both derivatives scaled by 1/dx */
+        T[1][i] = hx * (Axx_x - Axx_z);
+        T[2][i] = hx * Azz_x + hz * Azz_z;
+        T[3][i] = hx * Azz_x - hz * Azz_z;
+        T[4][i] = hx * Axz_x + hz * Axz_z;
+        T[5][i] = hx * Axz_x - hz * Axz_z;
+        L.vx[i] *= c->coef1[i];
+        L.vz[i] *= c->coef1[i];
+      }
+    /* transposed velocity stencils onto the stress nodes: minus the stress-node pair
+     * (rows above izStart included: the free-surface image reads them) */
+    const int z_lo = c->fs ? izs - NH : izs;
+    for (int ix = NH; ix < Nx - NH; ++ix)
+      for (int iz = z_lo; iz < Nz - NH; ++iz) {
+        const size_t i = (size_t)ix * Nz + iz;
+        /* sigma_xx: d1 pair of T0 plus d2 pair of T1 (likewise for zz, xz) */
+        double p1, p2, q1, q2, r1, r2, unused;
+        ds(c, T[0], ix, iz, &p1, &unused);
+        ds(c, T[1], ix, iz, &unused, &p2);
+        ds(c, T[2], ix, iz, &q1, &unused);
+        ds(c, T[3], ix, iz, &unused, &q2);
+        ds(c, T[4], ix, iz, &r1, &unused);
+        ds(c, T[5], ix, iz, &unused, &r2);
+        L.sxx[i] -= p1 + p2;
+        L.szz[i] -= q1 + q2;
+        L.sxz[i] -= r1 + r2;
+      }
+  }
+  /* chain rule: stiffness -> (vp, eps, delta); angles -> theta (degrees) */
+  const double rad = c->scalar * M_PI / 180.0;
+  for (int ix = 0; ix < Nx; ++ix)
+    for (int iz = 0; iz < Nz; ++iz) {
+      const size_t i = (size_t)ix * Nz + iz;
+      const double B = c->beta[i];
+      const double p = c->vp[i] / B, s = c->vs[i] / B, r = c->rho[i] * B;
+      const double f = 1.0 - (s / p) * (s / p), e = c->eps[i], d = c->delta[i];
+      const double q = sqrt(f * (f + 2.0 * d));
+      const double dc11_dp = 2.0 * r * p * (1.0 + 2.0 * e), dc33_dp = 2.0 * r * p;
+      const double dc13_dp = r * (2.0 * p * q + p * p * (f + d) / q * 2.0 * s * s / (p * p * p));
+      g_vp[i] = (gc11[i] * dc11_dp + gc13[i] * dc13_dp + gc33[i] * dc33_dp) / B;
+      g_eps[i] = gc11[i] * 2.0 * r * p * p;
+      g_delta[i] = gc13[i] * r * p * p * f / q;
+      /* theta at the stress node, plus the velocity-node averages that read it */
+      double gt = gth[i];
+      const double sn = c->sn[i], cs = c->cs[i];
+      for (int a = 0; a <= 1; ++a)
+        for (int b = 0; b <= 1; ++b) {
+          const int vx = ix - a, vz = iz - b;
+          if (vx < 0 || vz < 0) continue;
+          const int inner = vx < Nx - 1 && vz < Nz - 1;
+          if (!inner && (a || b)) continue;
+          const double w = inner ? 0.25 : 1.0;
+          const size_t j = (size_t)vx * Nz + vz;
+          gt += w * (gsv[j] * cs - gcv[j] * sn);
+        }
+      g_theta[i] = gt * rad;
+    }
+  for (int it = 0; it < c->nt; ++it) state_free(&keep[it]);
+  free(keep);
+  state_free(&L);
+  for (int k = 0; k < 6; ++k) free(T[k]);
+  free(gc11);
+  free(gc13);
+  free(gc33);
+  free(gc55);
+  free(gth);
+  free(gsv);
+  free(gcv);
+  for (int k = 0; k < 3; ++k) free(rec[k]);
+  return J;
+}

@@ -1,0 +1,80 @@
+"""The double-precision CPU reference of the adjoint-state gradient
+(oracle/ttifd_adjoint.c), pinned the two ways an adjoint can be checked
+without a reference implementation: the dot-product test <L s, r> = <s, L^T r>
+of the source-to-trace map (the adjoint propagation, free surface and
+receivers), and central finite differences of the misfit at seeded cells for
+each of vp, epsilon, delta and theta (the stiffness chain rule)."""
+import numpy as np
+import pytest
+
+import synthetic
+from pyoracle import AdjointOracle
+
+CFG = dict(nz=36, nx=48, nt=220, dx=10.0, dz=10.0, dt=0.001, fpeak=15.0, ealThick=8, seistype=3, mt=1)
+
+
+def _setup(fs, seed=5):
+    cfg = dict(CFG, freesurface=fs)
+    m = synthetic.layered_model(cfg["nz"], cfg["nx"], seed=seed, nlayers=4)
+    pads = synthetic.padded(m, cfg["ealThick"])
+    adj = AdjointOracle(cfg, pads)
+    adj.set_model(*pads)
+    w = synthetic.ricker(cfg["nt"], cfg["dt"], cfg["fpeak"])
+    adj.set_source([24], [3], w[None, :])
+    gx = np.arange(0, cfg["nx"], 3)
+    for k in (0, 1, 2):
+        adj.set_receivers(k, gx, 2)
+    return cfg, adj, pads, w
+
+
+@pytest.mark.parametrize("fs", [0, 1])
+def test_dot_product(fs):
+    cfg, adj, pads, w = _setup(fs)
+    with adj:
+        d = adj.forward()
+        rng = np.random.default_rng(1)
+        r = [rng.standard_normal(a.shape) for a in d]
+        J, g, gsrc = adj.gradient([a - b for a, b in zip(d, r)])
+        lhs = sum(float(np.sum(a * b)) for a, b in zip(d, r))
+        rhs = float(np.sum(gsrc[0] * w))
+        assert J == pytest.approx(0.5 * sum(float(np.sum(b * b)) for b in r), rel=1e-12)
+        assert abs(lhs - rhs) <= 1e-10 * abs(lhs), (lhs, rhs)
+
+
+def _misfit(adj, model, dobs):
+    adj.set_model(*model)
+    d = adj.forward()
+    return 0.5 * sum(float(np.sum((a - b) ** 2)) for a, b in zip(d, dobs))
+
+
+@pytest.mark.parametrize("fs", [0, 1])
+def test_gradient_matches_central_differences(fs):
+    cfg, adj, pads, w = _setup(fs)
+    E = cfg["ealThick"] + 5
+    with adj:
+        # observed data from a model with a perturbed patch; gradient at the start model
+        true = [np.array(a, dtype=np.float64) for a in pads]
+        true[0][E + 20:E + 30, E + 12:E + 20] *= 1.04
+        true[5][E + 20:E + 30, E + 12:E + 20] += 6.0
+        adj.set_model(*true)
+        dobs = adj.forward()
+        start = [np.array(a, dtype=np.float64) for a in pads]
+        adj.set_model(*start)
+        J0, g, _ = adj.gradient(dobs)
+        assert J0 > 0
+        rng = np.random.default_rng(3)
+        checks = []
+        for name, idx, h in (("vp", 0, 1e-3), ("eps", 3, 1e-3), ("delta", 4, 1e-3), ("theta", 5, 1e-2)):
+            for _ in range(3):
+                ix = E + 6 + int(rng.integers(0, cfg["nx"] - 12))
+                iz = E + 6 + int(rng.integers(0, cfg["nz"] - 12))
+                step = h * (start[0][ix, iz] if name == "vp" else 1.0)
+                mp = [a.copy() for a in start]
+                mm = [a.copy() for a in start]
+                mp[idx][ix, iz] += step
+                mm[idx][ix, iz] -= step
+                fd = (_misfit(adj, mp, dobs) - _misfit(adj, mm, dobs)) / (2 * step)
+                checks.append((name, ix, iz, fd, g[name][ix, iz]))
+        scale = {n: max(abs(c[4]) for c in checks if c[0] == n) for n in ("vp", "eps", "delta", "theta")}
+        for name, ix, iz, fd, an in checks:
+            assert abs(fd - an) <= 1e-3 * max(abs(an), 1e-2 * scale[name]), (name, ix, iz, fd, an)

@@ -1,0 +1,131 @@
+"""Device adjoint-state gradient (tti_grad_*) against the double-precision CPU
+reference (oracle/ttifd_adjoint.c, itself pinned by the dot-product test and
+central finite differences): misfit, the four model gradients and the source
+gradient; independence of the checkpoint count; shot accumulation; the
+dot-product test of the device adjoint."""
+import numpy as np
+import pytest
+
+import synthetic
+from pyoracle import AdjointOracle
+
+pytestmark = pytest.mark.gpu
+
+CFG = dict(nz=36, nx=48, nt=220, dx=10.0, dz=10.0, dt=0.001, fpeak=15.0, ealThick=8, seistype=3, mt=1)
+NAMES = ("vp", "eps", "delta", "theta")
+
+
+def _case(fs, sx=24):
+    cfg = dict(CFG, freesurface=fs)
+    m = synthetic.layered_model(cfg["nz"], cfg["nx"], seed=5, nlayers=4)
+    pads = synthetic.padded(m, cfg["ealThick"])
+    E = cfg["ealThick"] + 5
+    true = [np.array(a, dtype=np.float64) for a in pads]
+    true[0][E + 20:E + 30, E + 12:E + 20] *= 1.04
+    true[5][E + 20:E + 30, E + 12:E + 20] += 6.0
+    w = synthetic.ricker(cfg["nt"], cfg["dt"], cfg["fpeak"])
+    gx = np.arange(0, cfg["nx"], 3)
+    return cfg, pads, true, w, gx
+
+
+def _device(cfg, pads, w, gx, dobs, ncheck, sx=24, h=None):
+    import ttifd
+
+    own = h is None
+    if own:
+        h = ttifd.Modeling(variant="coordinate_rotation", stype=1, **cfg)
+        h.upload_model(*pads)
+        h.grad_zero()
+    h.set_source([sx], [3], w[None, :])
+    for k in (0, 1, 2):
+        h.set_receivers(k, gx, 2)
+        h.grad_set_observed(k, dobs[k])
+    J = h.grad_run(ncheck)
+    return h, J
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.mark.parametrize("fs", [0, 1])
+def test_gradient_matches_cpu_reference(fs, monkeypatch, gpu_lib):
+    monkeypatch.delenv("TTIFD_KERNEL", raising=False)
+    cfg, pads, true, w, gx = _case(fs)
+    with AdjointOracle(cfg, pads) as adj:
+        adj.set_model(*true)
+        adj.set_source([24], [3], w[None, :])
+        for k in (0, 1, 2):
+            adj.set_receivers(k, gx, 2)
+        dobs = adj.forward()
+        adj.set_model(*pads)
+        J_ref, g_ref, gs_ref = adj.gradient(dobs)
+    h, J = _device(cfg, pads, w, gx, [d.astype(np.float32) for d in dobs], ncheck=9)
+    with h:
+        assert J == pytest.approx(J_ref, rel=1e-4)
+        for name in NAMES:
+            err = _rel(h.grad_fetch(name), g_ref[name])
+            assert err <= 1e-3, (name, err)
+        assert _rel(h.grad_fetch_source(1), gs_ref) <= 1e-4
+
+
+def test_checkpoint_count_does_not_change_the_gradient(gpu_lib):
+    cfg, pads, true, w, gx = _case(1)
+    dobs = [np.zeros((gx.size, cfg["nt"]), np.float32) for _ in range(3)]
+    out = []
+    for ncheck in (1, 7, cfg["nt"]):
+        h, J = _device(cfg, pads, w, gx, dobs, ncheck)
+        with h:
+            out.append((J, [h.grad_fetch(n) for n in NAMES]))
+    for J, g in out[1:]:
+        assert J == pytest.approx(out[0][0], rel=1e-12)  # a double atomic sum: order-dependent last bit
+        for a, b in zip(g, out[0][1]):
+            assert np.array_equal(a, b)
+
+
+def test_shots_accumulate(gpu_lib):
+    cfg, pads, true, w, gx = _case(0)
+    rng = np.random.default_rng(2)
+    dobs = [1e-9 * rng.standard_normal((gx.size, cfg["nt"])).astype(np.float32) for _ in range(3)]
+    singles = []
+    for sx in (12, 30):
+        h, _ = _device(cfg, pads, w, gx, dobs, 5, sx=sx)
+        with h:
+            singles.append(h.grad_fetch("vp"))
+    h, _ = _device(cfg, pads, w, gx, dobs, 5, sx=12)
+    with h:
+        _device(cfg, pads, w, gx, dobs, 5, sx=30, h=h)
+        both = h.grad_fetch("vp")
+    assert _rel(both, singles[0] + singles[1]) <= 1e-6
+
+
+def test_device_dot_product(gpu_lib):
+    """<L w, r> = <w, L^T r> with the device forward and adjoint (float)."""
+    import ttifd
+
+    cfg, pads, true, w, gx = _case(1)
+    with ttifd.Modeling(variant="coordinate_rotation", stype=1, **cfg) as h:
+        h.upload_model(*pads)
+        h.set_source([24], [3], w[None, :])
+        for k in (0, 1, 2):
+            h.set_receivers(k, gx, 2)
+        h.run()
+        d = [h.fetch_traces(k).astype(np.float64) for k in (0, 1, 2)]
+    rng = np.random.default_rng(4)
+    scale = max(np.abs(x).max() for x in d)
+    r = [scale * rng.standard_normal(x.shape) for x in d]
+    h, _ = _device(cfg, pads, w, gx, [(a - b).astype(np.float32) for a, b in zip(d, r)], ncheck=4)
+    with h:
+        gsrc = h.grad_fetch_source(1).astype(np.float64)
+    lhs = sum(float(np.sum(a * b)) for a, b in zip(d, r))
+    rhs = float(np.sum(gsrc[0] * w))
+    assert abs(lhs - rhs) <= 2e-4 * abs(lhs), (lhs, rhs)
+
+
+def test_gradient_rejects_other_formulations(gpu_lib):
+    import ttifd
+
+    with ttifd.Modeling(variant="tensor_rotation", stype=1, **CFG) as h:
+        with pytest.raises(ttifd.TTIError) as e:
+            h.grad_zero()
+        assert e.value.code == ttifd.ERR_ARG

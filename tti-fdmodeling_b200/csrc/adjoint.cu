@@ -1,0 +1,564 @@
+// Adjoint-state gradient (tti_grad_*), coordinate-rotation formulation.
+//
+// Misfit J = 1/2 sum over the recorded samples of (d - dobs)^2. The forward
+// step (coord:611-926) is, per time step n:
+//   v'  = coef1 v + coef2 invrho R(theta_v) D_sigma sigma      velocity half (:614-672) + sources
+//   s'  = coef1 s + coef2 H(c11, c13, c33, c55, theta) D_v v'   stress half (:804-845)
+//   s'' = P_fs s' (free surface, :847-863), + stress source, record (isoelastic.c:103-144)
+// Its discrete adjoint, run backwards from n = nt-1, is per step:
+//   inject the residual at the receivers; P_fs^T; stress-half adjoint
+//   (gradient terms of c11..c55 and theta at the stress node, then the
+//   transposed stress stencils, which are minus the velocity-node stencils,
+//   into lambda_v); velocity-half adjoint (gradient terms of sin/cos theta_v,
+//   then the transposed velocity stencils, minus the stress-node stencils,
+//   into lambda_sigma). Each adjoint step needs the forward v after the
+//   velocity half and sigma before the stress half of the same step: the loop
+//   is recomputed segment by segment from checkpoints (ncheck full states
+//   saved in the first pass), the segment's states kept on the device.
+// The chain rule maps the stiffness and angle sums to vp, epsilon, delta and
+// theta (degrees) with vs and rho fixed and MEAL coef1, coef2, Beta frozen:
+// c11 = rho' vp'^2 (1 + 2 eps), c13 = rho' (vp'^2 sqrt(f (f + 2 delta)) - vs'^2),
+// c33 = rho' vp'^2, f = 1 - (vs'/vp')^2, vp' = vp / Beta (coord:497-515,
+// meal.c:450-490).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "tiled.cuh"
+
+using namespace ttifd;
+
+struct GradState {
+  int ncheck = 0, seg = 0;  // checkpoints, steps per segment
+  float *lam[5] = {};       // adjoint vx vz sxx szz sxz
+  float *T[6] = {};         // per-cell adjoint strain / stress-derivative terms
+  float *acc[7] = {};       // sums: c11 c13 c33 c55 theta(stress node) sin_v cos_v
+  float *out[4] = {};       // vp eps delta theta
+  float *ckpt = nullptr;    // ncheck x 5 fields
+  float *keep = nullptr;    // seg x 5 fields
+  float *obs[3] = {};       // observed traces, time-major [nts][ntrace]
+  float *res[3] = {};       // residuals, time-major
+  float *gsrc = nullptr;    // [nsrc][nt]
+  int gsrc_n = 0;
+  double *d_J = nullptr;
+  bool have_obs[3] = {};
+};
+
+namespace {
+
+constexpr int BZ = 32, BX = 8;
+
+struct AdjArgs {
+  Grid g;
+  Params p;
+  float *lam[5];
+  float *T[6];
+  float *acc[7];
+  const float *keep[5];
+  float hx, hz;
+  int z_lo;  // first row of the transposed velocity stencils
+};
+
+__device__ __forceinline__ void pair_v(const float *a, size_t L, int ix, int iz, float &d1, float &d2)
+{
+  float s1 = 0.0f, s2 = 0.0f;
+#pragma unroll
+  for (int k = 1; k <= NH; ++k) {
+    s1 += rsg(k - 1) * (a[(size_t)(ix + k) * L + iz + k] - a[(size_t)(ix - k + 1) * L + iz - k + 1]);
+    s2 += rsg(k - 1) * (a[(size_t)(ix + k) * L + iz - k + 1] - a[(size_t)(ix - k + 1) * L + iz + k]);
+  }
+  d1 = s1;
+  d2 = s2;
+}
+
+__device__ __forceinline__ void pair_s(const float *a, size_t L, int ix, int iz, float &d1, float &d2)
+{
+  float s1 = 0.0f, s2 = 0.0f;
+#pragma unroll
+  for (int k = 1; k <= NH; ++k) {
+    s1 += rsg(k - 1) * (a[(size_t)(ix + k - 1) * L + iz + k - 1] - a[(size_t)(ix - k) * L + iz - k]);
+    s2 += rsg(k - 1) * (a[(size_t)(ix + k - 1) * L + iz - k] - a[(size_t)(ix - k) * L + iz + k - 1]);
+  }
+  d1 = s1;
+  d2 = s2;
+}
+
+__device__ __forceinline__ bool interior(const Grid &g, int ix, int iz)
+{
+  return ix >= NH && ix < g.Nx - NH && iz >= g.izStart && iz < g.Nz - NH;
+}
+
+// residual injection (adjoint of the receiver sampling)
+__global__ void k_inject(Grid g, AdjArgs a, const int *rx, const int *rz, const float *res, int n, int kind)
+{
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const size_t c = (size_t)rx[t] * g.ldz + rz[t];
+  const float r = res[t];
+  if (kind == TTI_REC_VX) atomicAdd(a.lam[0] + c, r);
+  else if (kind == TTI_REC_VZ) atomicAdd(a.lam[1] + c, r);
+  else {
+    atomicAdd(a.lam[2] + c, 0.5f * r);
+    atomicAdd(a.lam[3] + c, 0.5f * r);
+  }
+}
+
+// dJ/d(source sample): adjoint of the stress source, one block per source
+struct K1 {
+  float k1[121];
+};
+__global__ void k_source_grad(Grid g, AdjArgs a, SourceSet s, K1 tab, float *gsrc, int it)
+{
+  __shared__ float part[128];
+  const int n = blockIdx.x, t = threadIdx.x;
+  float v = 0.0f;
+  if (t < 121) {
+    const int ix = s.x[n] + t / 11 - NH, iz = s.z[n] + t % 11 - NH;
+    if (ix >= 0 && ix < g.Nx && iz >= 0 && iz < g.Nz) {
+      const size_t c = (size_t)ix * g.ldz + iz;
+      v = tab.k1[t] * (a.lam[2][c] + a.lam[3][c]);
+    }
+  }
+  part[t] = v;
+  __syncthreads();
+  for (int o = 64; o > 0; o >>= 1) {
+    if (t < o) part[t] += part[t + o];
+    __syncthreads();
+  }
+  if (t == 0) gsrc[(size_t)n * s.nt + it] = part[0];
+}
+
+// adjoint of the free-surface image (one thread per column)
+__global__ void k_adj_free_surface(Grid g, AdjArgs a)
+{
+  const int ix = NH + blockIdx.x * blockDim.x + threadIdx.x;
+  if (ix >= g.Nx - NH) return;
+  const size_t c = (size_t)ix * g.ldz + g.izStart;
+  float *xx = a.lam[2], *zz = a.lam[3], *xz = a.lam[4];
+  for (int k = 1; k <= NH; ++k) {
+    xx[c] += 2.0f * xx[c - k];
+    xx[c + k] -= xx[c - k];
+    xx[c - k] = 0.0f;
+    zz[c + k] -= zz[c - k];
+    zz[c - k] = 0.0f;
+    xz[c + k] -= xz[c - k];
+    xz[c - k] = 0.0f;
+  }
+  xz[c] = 0.0f;
+  zz[c] = 0.0f;
+}
+
+// stress-half adjoint, local part: gradient sums, T0..T3, lambda_sigma *= coef1
+__global__ void __launch_bounds__(BZ *BX) k_adj_stress_local(AdjArgs a)
+{
+  const Grid &g = a.g;
+  const int iz = blockIdx.x * BZ + threadIdx.x, ix = blockIdx.y * BX + threadIdx.y;
+  if (!interior(g, ix, iz)) return;
+  const size_t L = g.ldz, i = (size_t)ix * L + iz;
+  float a1, a2, b1, b2;
+  pair_s(a.keep[0], L, ix, iz, a1, a2);
+  pair_s(a.keep[1], L, ix, iz, b1, b2);
+  const float vxx = a.hx * (a1 + a2), vxz = a.hz * (a1 - a2), vzx = a.hx * (b1 + b2), vzz = a.hz * (b1 - b2);
+  const float s = a.p.sn[i], co = a.p.cs[i];
+  const float rxx = co * vxx - s * vxz, rxz = s * vxx + co * vxz;
+  const float rzx = co * vzx - s * vzz, rzz = s * vzx + co * vzz;
+  const float la = a.lam[2][i], lb = a.lam[3][i], le = a.lam[4][i], b = a.p.coef2[i];
+  const float c11 = a.p.c11[i], c13 = a.p.c13[i], c33 = a.p.c33[i], c55 = a.p.c55[i];
+  a.acc[0][i] += b * la * rxx;
+  a.acc[1][i] += b * (la * rzz + lb * rxx);
+  a.acc[2][i] += b * lb * rzz;
+  a.acc[3][i] += b * le * (rzx + rxz);
+  a.acc[4][i] += b * (la * (c13 * rzx - c11 * rxz) + lb * (c33 * rzx - c13 * rxz) + le * c55 * (rxx - rzz));
+  const float Lxx = b * (c11 * la + c13 * lb), Lzz = b * (c13 * la + c33 * lb), Lq = b * c55 * le;
+  a.T[0][i] = co * Lxx + s * Lq;
+  a.T[1][i] = co * Lq - s * Lxx;
+  a.T[2][i] = co * Lq + s * Lzz;
+  a.T[3][i] = co * Lzz - s * Lq;
+  const float c1 = a.p.coef1[i];
+  a.lam[2][i] = c1 * la;
+  a.lam[3][i] = c1 * lb;
+  a.lam[4][i] = c1 * le;
+}
+
+// transposed stress stencils into lambda_v (minus the velocity-node pairs)
+__global__ void __launch_bounds__(BZ *BX) k_adj_stress_stencil(AdjArgs a)
+{
+  const Grid &g = a.g;
+  const int iz = blockIdx.x * BZ + threadIdx.x, ix = blockIdx.y * BX + threadIdx.y;
+  if (!interior(g, ix, iz)) return;
+  const size_t L = g.ldz, i = (size_t)ix * L + iz;
+  float p1, p2, q1, q2, r1, r2, s1, s2;
+  pair_v(a.T[0], L, ix, iz, p1, p2);
+  pair_v(a.T[1], L, ix, iz, q1, q2);
+  pair_v(a.T[2], L, ix, iz, r1, r2);
+  pair_v(a.T[3], L, ix, iz, s1, s2);
+  a.lam[0][i] -= a.hx * (p1 + p2) + a.hz * (q1 - q2);
+  a.lam[1][i] -= a.hx * (r1 + r2) + a.hz * (s1 - s2);
+}
+
+// velocity-half adjoint, local part: sin/cos theta_v sums, T0..T5, lambda_v *= coef1
+__global__ void __launch_bounds__(BZ *BX) k_adj_velocity_local(AdjArgs a)
+{
+  const Grid &g = a.g;
+  const int iz = blockIdx.x * BZ + threadIdx.x, ix = blockIdx.y * BX + threadIdx.y;
+  if (!interior(g, ix, iz)) return;
+  const size_t L = g.ldz, i = (size_t)ix * L + iz;
+  float a1, a2, b1, b2, e1, e2;
+  pair_v(a.keep[2], L, ix, iz, a1, a2);
+  pair_v(a.keep[3], L, ix, iz, b1, b2);
+  pair_v(a.keep[4], L, ix, iz, e1, e2);
+  const float hx = a.hx, hz = a.hz;
+  const float sxx_x = hx * (a1 + a2), sxx_z = hx * (a1 - a2);  // 1/dx for both, as coord:633
+  const float szz_x = hx * (b1 + b2), szz_z = hz * (b1 - b2);
+  const float sxz_x = hx * (e1 + e2), sxz_z = hz * (e1 - e2);
+  const float br = a.p.coef2[i] * a.p.invrho[i];
+  const float Fx = br * a.lam[0][i], Fz = br * a.lam[1][i];
+  const float cv = a.p.csv[i], sv = a.p.snv[i];
+  a.acc[5][i] += Fx * (sxz_x - sxx_z) + Fz * (szz_x - sxz_z);
+  a.acc[6][i] += Fx * (sxx_x + sxz_z) + Fz * (sxz_x + szz_z);
+  const float Axx_x = cv * Fx, Axx_z = -sv * Fx;
+  const float Axz_x = sv * Fx + cv * Fz, Axz_z = cv * Fx - sv * Fz;
+  const float Azz_x = sv * Fz, Azz_z = cv * Fz;
+  a.T[0][i] = hx * (Axx_x + Axx_z);
+  a.T[1][i] = hx * (Axx_x - Axx_z);
+  a.T[2][i] = hx * Azz_x + hz * Azz_z;
+  a.T[3][i] = hx * Azz_x - hz * Azz_z;
+  a.T[4][i] = hx * Axz_x + hz * Axz_z;
+  a.T[5][i] = hx * Axz_x - hz * Axz_z;
+  const float c1 = a.p.coef1[i];
+  a.lam[0][i] *= c1;
+  a.lam[1][i] *= c1;
+}
+
+// transposed velocity stencils into lambda_sigma (minus the stress-node pairs);
+// with a free surface also the image rows above izStart
+__global__ void __launch_bounds__(BZ *BX) k_adj_velocity_stencil(AdjArgs a)
+{
+  const Grid &g = a.g;
+  const int iz = blockIdx.x * BZ + threadIdx.x, ix = blockIdx.y * BX + threadIdx.y;
+  if (ix < NH || ix >= g.Nx - NH || iz < a.z_lo || iz >= g.Nz - NH) return;
+  const size_t L = g.ldz, i = (size_t)ix * L + iz;
+  float p1, p2, q1, q2, r1, r2, u;
+  pair_s(a.T[0], L, ix, iz, p1, u);
+  pair_s(a.T[1], L, ix, iz, u, p2);
+  pair_s(a.T[2], L, ix, iz, q1, u);
+  pair_s(a.T[3], L, ix, iz, u, q2);
+  pair_s(a.T[4], L, ix, iz, r1, u);
+  pair_s(a.T[5], L, ix, iz, u, r2);
+  a.lam[2][i] -= p1 + p2;
+  a.lam[3][i] -= q1 + q2;
+  a.lam[4][i] -= r1 + r2;
+}
+
+// residuals d - dobs (time-major) and J
+__global__ void k_residual(const float *rec, const float *obs, float *res, size_t n, double *J)
+{
+  double acc = 0.0;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const float r = rec[q] - obs[q];
+    res[q] = r;
+    acc += 0.5 * (double)r * (double)r;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(J, acc);
+}
+
+// chain rule to vp, epsilon, delta, theta (degrees), every cell
+__global__ void k_chain(Grid g, Params p, const float *vp, const float *vs, const float *rho, const float *beta,
+                        const float *eps, const float *delta, GradState gs, float rad)
+{
+  const int iz = blockIdx.x * BZ + threadIdx.x, ix = blockIdx.y * BX + threadIdx.y;
+  if (iz >= g.Nz || ix >= g.Nx) return;
+  const size_t L = g.ldz, i = (size_t)ix * L + iz;
+  const double B = beta[i], P = vp[i], S = vs[i], R = rho[i];  // vp/Beta, vs/Beta, rho*Beta
+  const double f = 1.0 - (S / P) * (S / P), e = eps[i], d = delta[i];
+  const double q = sqrt(f * (f + 2.0 * d));
+  const double dc11 = 2.0 * R * P * (1.0 + 2.0 * e), dc33 = 2.0 * R * P;
+  const double dc13 = q > 0.0 ? R * (2.0 * P * q + (f + d) / q * 2.0 * S * S / P) : 0.0;
+  const double g11 = gs.acc[0][i], g13 = gs.acc[1][i], g33 = gs.acc[2][i];
+  gs.out[0][i] = (float)((g11 * dc11 + g13 * dc13 + g33 * dc33) / B);
+  gs.out[1][i] = (float)(g11 * 2.0 * R * P * P);
+  gs.out[2][i] = (float)(q > 0.0 ? g13 * R * P * P * f / q : 0.0);
+  double gt = gs.acc[4][i];
+  const double sn = p.sn[i], cs = p.cs[i];
+  for (int a = 0; a <= 1; ++a)
+    for (int b = 0; b <= 1; ++b) {
+      const int vx = ix - a, vz = iz - b;
+      if (vx < 0 || vz < 0) continue;
+      const bool inner = vx < g.Nx - 1 && vz < g.Nz - 1;
+      if (!inner && (a || b)) continue;
+      const size_t j = (size_t)vx * L + vz;
+      gt += (inner ? 0.25 : 1.0) * (gs.acc[5][j] * cs - gs.acc[6][j] * sn);
+    }
+  gs.out[3][i] = (float)(gt * rad);
+}
+
+int gerr(tti_handle *h, int code, const char *msg) { return handle_error(h, code, msg); }
+
+#define GCK(h, call)                                                                    \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return gerr((h), e_ == cudaErrorMemoryAllocation ? TTI_ERR_NOMEM : TTI_ERR_CUDA, \
+                  cudaGetErrorString(e_));                                              \
+  } while (0)
+
+int grad_check(tti_handle *h)
+{
+  if (h->cfg.variant != TTI_COORDINATE)
+    return gerr(h, TTI_ERR_ARG, "the adjoint-state gradient is implemented for the coordinate formulation");
+  if (h->use_fused) return gerr(h, TTI_ERR_STATE, "the gradient runs on the tiled or per-cell kernels");
+  if (!h->have_model || !h->m_eps) return gerr(h, TTI_ERR_STATE, "model not uploaded");
+  if (h->cfg.stype != 1) return gerr(h, TTI_ERR_ARG, "the gradient models the stress source (stype = 1)");
+  return TTI_OK;
+}
+
+int grad_alloc(tti_handle *h)
+{
+  if (h->grad) return TTI_OK;
+  GradState *s = new GradState();
+  h->grad = s;
+  const size_t n = h->g.n;
+  auto al = [&](float **p) {
+    if (cudaMalloc(p, n * sizeof(float)) != cudaSuccess) return false;
+    return cudaMemsetAsync(*p, 0, n * sizeof(float), h->stream) == cudaSuccess;
+  };
+  bool ok = true;
+  for (auto &p : s->lam) ok = ok && al(&p);
+  for (auto &p : s->T) ok = ok && al(&p);
+  for (auto &p : s->acc) ok = ok && al(&p);
+  for (auto &p : s->out) ok = ok && al(&p);
+  ok = ok && cudaMalloc(&s->d_J, sizeof(double)) == cudaSuccess;
+  if (!ok) return gerr(h, TTI_ERR_NOMEM, "device allocation of the gradient buffers failed");
+  GCK(h, cudaStreamSynchronize(h->stream));
+  return TTI_OK;
+}
+
+AdjArgs adj_args(tti_handle *h, int slot)
+{
+  GradState *s = h->grad;
+  AdjArgs a;
+  a.g = h->g;
+  a.p = handle_step_args(h).p;
+  for (int k = 0; k < 5; ++k) a.lam[k] = s->lam[k];
+  for (int k = 0; k < 6; ++k) a.T[k] = s->T[k];
+  for (int k = 0; k < 7; ++k) a.acc[k] = s->acc[k];
+  for (int k = 0; k < 5; ++k) a.keep[k] = s->keep + ((size_t)slot * 5 + k) * h->g.n;
+  a.hx = 0.5f * h->invdx;
+  a.hz = 0.5f * h->invdz;
+  a.z_lo = h->cfg.freesurface ? std::max(NH, h->g.izStart - NH) : h->g.izStart;
+  return a;
+}
+
+// adjoint of forward step index n (time index it), segment slot `slot`
+int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
+{
+  const tti_config &c = h->cfg;
+  GradState *s = h->grad;
+  const int it = c.mode == 2 ? c.nt - 1 - n : n;
+  const AdjArgs a = adj_args(h, slot);
+  const Grid &g = h->g;
+  if (c.seistype > 0 && it % c.mt == 0)
+    for (int k = 0; k < 3; ++k)
+      if (s->res[k] && h->nrec[k] > 0)
+        k_inject<<<(h->nrec[k] + 127) / 128, 128, 0, h->stream>>>(
+            g, a, h->d_rx[k], h->d_rz[k], s->res[k] + (size_t)(it / c.mt) * h->nrec[k], h->nrec[k], k);
+  if (h->nsrc > 0) {
+    K1 k1;
+    memcpy(k1.k1, tab.k1, sizeof k1.k1);
+    k_source_grad<<<h->nsrc, 128, 0, h->stream>>>(g, a, SourceSet{h->nsrc, h->d_sx, h->d_sz, h->d_src, c.nt}, k1,
+                                                   s->gsrc, it);
+  }
+  if (c.freesurface == 1) k_adj_free_surface<<<(g.Nx + 127) / 128, 128, 0, h->stream>>>(g, a);
+  const dim3 blk(BZ, BX), grd((g.Nz + BZ - 1) / BZ, (g.Nx + BX - 1) / BX);
+  k_adj_stress_local<<<grd, blk, 0, h->stream>>>(a);
+  k_adj_stress_stencil<<<grd, blk, 0, h->stream>>>(a);
+  k_adj_velocity_local<<<grd, blk, 0, h->stream>>>(a);
+  k_adj_velocity_stencil<<<grd, blk, 0, h->stream>>>(a);
+  h->launches += 4 + (c.freesurface == 1) + (h->nsrc > 0);
+  GCK(h, cudaGetLastError());
+  return TTI_OK;
+}
+
+}  // namespace
+
+namespace ttifd {
+void grad_release(tti_handle *h)
+{
+  GradState *s = h->grad;
+  if (!s) return;
+  for (auto p : s->lam) cudaFree(p);
+  for (auto p : s->T) cudaFree(p);
+  for (auto p : s->acc) cudaFree(p);
+  for (auto p : s->out) cudaFree(p);
+  for (auto p : s->obs) cudaFree(p);
+  for (auto p : s->res) cudaFree(p);
+  cudaFree(s->ckpt);
+  cudaFree(s->keep);
+  cudaFree(s->gsrc);
+  cudaFree(s->d_J);
+  delete s;
+  h->grad = nullptr;
+}
+}  // namespace ttifd
+
+extern "C" {
+
+int tti_grad_set_observed(tti_handle *h, int kind, const float *dobs)
+{
+  if (!h || kind < 0 || kind > 2 || !dobs) return TTI_ERR_ARG;
+  int rc = grad_check(h);
+  if (rc) return rc;
+  if (h->nrec[kind] <= 0) return gerr(h, TTI_ERR_STATE, "set the receivers of this component first");
+  GCK(h, cudaSetDevice(h->device));
+  if ((rc = grad_alloc(h))) return rc;
+  GradState *s = h->grad;
+  const int n = h->nrec[kind], nts = h->nts;
+  cudaFree(s->obs[kind]);
+  cudaFree(s->res[kind]);
+  s->obs[kind] = s->res[kind] = nullptr;
+  GCK(h, cudaMalloc(&s->obs[kind], sizeof(float) * (size_t)n * nts));
+  GCK(h, cudaMalloc(&s->res[kind], sizeof(float) * (size_t)n * nts));
+  std::vector<float> tm((size_t)n * nts);  // [ntrace][nts] -> time-major
+  for (int r = 0; r < n; ++r)
+    for (int t = 0; t < nts; ++t) tm[(size_t)t * n + r] = dobs[(size_t)r * nts + t];
+  GCK(h, cudaMemcpy(s->obs[kind], tm.data(), sizeof(float) * tm.size(), cudaMemcpyHostToDevice));
+  s->have_obs[kind] = true;
+  return TTI_OK;
+}
+
+int tti_grad_zero(tti_handle *h)
+{
+  if (!h) return TTI_ERR_ARG;
+  int rc = grad_check(h);
+  if (rc) return rc;
+  GCK(h, cudaSetDevice(h->device));
+  if ((rc = grad_alloc(h))) return rc;
+  for (auto p : h->grad->acc) GCK(h, cudaMemsetAsync(p, 0, h->g.n * sizeof(float), h->stream));
+  GCK(h, cudaStreamSynchronize(h->stream));
+  return TTI_OK;
+}
+
+int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
+{
+  if (!h || ncheck < 1) return TTI_ERR_ARG;
+  int rc = grad_check(h);
+  if (rc) return rc;
+  GCK(h, cudaSetDevice(h->device));
+  if ((rc = grad_alloc(h))) return rc;
+  GradState *s = h->grad;
+  const tti_config &c = h->cfg;
+  const bool want_v = c.seistype == 1 || c.seistype == 3, want_p = c.seistype == 2 || c.seistype == 3;
+  for (int k = 0; k < 3; ++k) {
+    const bool rec = (k < 2 ? want_v : want_p) && h->nrec[k] > 0;
+    if (rec && !s->have_obs[k]) return gerr(h, TTI_ERR_STATE, "observed traces missing for a recorded component");
+  }
+  const int nt = c.nt;
+  ncheck = std::min(ncheck, nt);
+  const int seg = (nt + ncheck - 1) / ncheck, nseg = (nt + seg - 1) / seg;
+  const size_t n = h->g.n, state = 5 * n;
+  if (s->ncheck != nseg || s->seg != seg) {
+    cudaFree(s->ckpt);
+    cudaFree(s->keep);
+    s->ckpt = s->keep = nullptr;
+    if (cudaMalloc(&s->ckpt, sizeof(float) * state * nseg) != cudaSuccess ||
+        cudaMalloc(&s->keep, sizeof(float) * state * seg) != cudaSuccess) {
+      s->ncheck = s->seg = 0;
+      return gerr(h, TTI_ERR_NOMEM, "device allocation of the checkpoints failed (use fewer steps per segment)");
+    }
+    s->ncheck = nseg;
+    s->seg = seg;
+  }
+  if (s->gsrc_n != h->nsrc * nt) {
+    cudaFree(s->gsrc);
+    s->gsrc = nullptr;
+    s->gsrc_n = 0;
+    if (h->nsrc > 0) GCK(h, cudaMalloc(&s->gsrc, sizeof(float) * (size_t)h->nsrc * nt));
+    s->gsrc_n = h->nsrc * nt;
+  }
+  SourceTables tab;
+  handle_source_tables(h, &tab);
+  // pass 1: forward with checkpoints at every segment start
+  if ((rc = tti_reset(h))) return rc;
+  for (int q = 0; q < nseg; ++q) {
+    for (int f = 0; f < 5; ++f)
+      GCK(h, cudaMemcpyAsync(s->ckpt + ((size_t)q * 5 + f) * n, h->fld[f], n * sizeof(float),
+                             cudaMemcpyDeviceToDevice, h->stream));
+    for (int k = q * seg; k < std::min(nt, (q + 1) * seg); ++k)
+      if ((rc = handle_step(h, tab, nullptr))) return rc;
+  }
+  // residuals and misfit
+  GCK(h, cudaMemsetAsync(s->d_J, 0, sizeof(double), h->stream));
+  for (int k = 0; k < 3; ++k) {
+    const bool rec = (k < 2 ? want_v : want_p) && h->nrec[k] > 0;
+    if (!rec) continue;
+    const size_t m = (size_t)h->nrec[k] * h->nts;
+    k_residual<<<std::min<size_t>(1024, (m + 255) / 256), 256, 0, h->stream>>>(h->d_rec[k], s->obs[k], s->res[k], m,
+                                                                               s->d_J);
+  }
+  double J = 0.0;
+  GCK(h, cudaMemcpyAsync(&J, s->d_J, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  // adjoint, segment by segment from the last
+  for (auto p : s->lam) GCK(h, cudaMemsetAsync(p, 0, n * sizeof(float), h->stream));
+  for (auto p : s->T) GCK(h, cudaMemsetAsync(p, 0, n * sizeof(float), h->stream));
+  for (int q = nseg - 1; q >= 0; --q) {
+    const int k0 = q * seg, k1 = std::min(nt, (q + 1) * seg);
+    for (int f = 0; f < 5; ++f)
+      GCK(h, cudaMemcpyAsync(h->fld[f], s->ckpt + ((size_t)q * 5 + f) * n, n * sizeof(float),
+                             cudaMemcpyDeviceToDevice, h->stream));
+    h->step_index = k0;
+    for (int k = k0; k < k1; ++k) {
+      float *keep[5];
+      for (int f = 0; f < 5; ++f) keep[f] = s->keep + ((size_t)(k - k0) * 5 + f) * n;
+      if ((rc = handle_step(h, tab, keep))) return rc;
+    }
+    for (int k = k1 - 1; k >= k0; --k)
+      if ((rc = adjoint_step(h, k, k - k0, tab))) return rc;
+  }
+  GCK(h, cudaStreamSynchronize(h->stream));
+  h->step_index = nt;
+  if (misfit) *misfit = J;
+  return handle_check_flag(h);
+}
+
+int tti_grad_fetch(tti_handle *h, int which, float *out)
+{
+  if (!h || !out || which < 0 || which > 3) return TTI_ERR_ARG;
+  if (!h->grad) return gerr(h, TTI_ERR_STATE, "no gradient computed");
+  GCK(h, cudaSetDevice(h->device));
+  GradState *s = h->grad;
+  const Grid &g = h->g;
+  const dim3 blk(BZ, BX), grd((g.Nz + BZ - 1) / BZ, (g.Nx + BX - 1) / BX);
+  const float rad = (float)(h->cfg.scalar * M_PI / 180.0);
+  k_chain<<<grd, blk, 0, h->stream>>>(g, handle_step_args(h).p, h->par[TTI_P_VP], h->par[TTI_P_VS],
+                                      h->par[TTI_P_RHO], h->par[TTI_P_BETA], h->m_eps, h->m_delta, *s, rad);
+  h->launches++;
+  GCK(h, cudaGetLastError());
+  GCK(h, cudaMemcpy2DAsync(out, (size_t)g.Nz * sizeof(float), s->out[which], (size_t)g.ldz * sizeof(float),
+                           (size_t)g.Nz * sizeof(float), g.Nx, cudaMemcpyDeviceToHost, h->stream));
+  GCK(h, cudaStreamSynchronize(h->stream));
+  return TTI_OK;
+}
+
+int tti_grad_fetch_source(tti_handle *h, float *out)
+{
+  if (!h || !out) return TTI_ERR_ARG;
+  if (!h->grad || !h->grad->gsrc) return gerr(h, TTI_ERR_STATE, "no source gradient computed");
+  GCK(h, cudaSetDevice(h->device));
+  GCK(h, cudaMemcpy(out, h->grad->gsrc, sizeof(float) * (size_t)h->grad->gsrc_n, cudaMemcpyDeviceToHost));
+  return TTI_OK;
+}
+
+int tti_grad_accumulators(tti_handle *h, float **dev, size_t *count, size_t *pitch)
+{
+  if (!h || !dev) return TTI_ERR_ARG;
+  if (!h->grad) return gerr(h, TTI_ERR_STATE, "no gradient buffers");
+  for (int k = 0; k < 7; ++k) dev[k] = h->grad->acc[k];
+  if (count) *count = h->g.n;
+  if (pitch) *pitch = h->g.ldz;
+  return TTI_OK;
+}
+
+}  // extern "C"

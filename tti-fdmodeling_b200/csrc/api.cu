@@ -120,8 +120,10 @@ int current_it(const tti_handle *h) { return h->cfg.mode == 2 ? h->cfg.nt - 1 - 
 
 // Launches one time step (coord:611-926 body). With `ev` (5 events) the
 // phases are bracketed for tti_profile_steps: ev[0] | velocity | ev[1] |
-// velocity sources | ev[2] | stress | ev[3] | the rest | ev[4].
-int launch_one_step(tti_handle *h, const SourceTables &tab, cudaEvent_t *ev = nullptr)
+// velocity sources | ev[2] | stress | ev[3] | the rest | ev[4]. With `keep`
+// (5 device arrays, the gradient's recompute pass) vx, vz, sxx, szz, sxz are
+// copied there between the velocity sources and the stress update.
+int launch_one_step(tti_handle *h, const SourceTables &tab, cudaEvent_t *ev = nullptr, float *const *keep = nullptr)
 {
   const tti_config &c = h->cfg;
   const int it = current_it(h);
@@ -199,6 +201,9 @@ int launch_one_step(tti_handle *h, const SourceTables &tab, cudaEvent_t *ev = nu
   else launch_velocity(a, h->stream);
   if (ev) CK(h, cudaEventRecord(ev[1], h->stream));
   if (vsrc) launch_sources(a, s, &tab, c.stype, 0, it, h->stream);
+  if (keep)
+    for (int f = 0; f < 5; ++f)
+      CK(h, cudaMemcpyAsync(keep[f], h->fld[f], h->g.n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
   if (ev) CK(h, cudaEventRecord(ev[2], h->stream));
   if (h->use_tiled) {
     const CUtensorMap *tm = static_cast<const CUtensorMap *>(h->tmaps);
@@ -311,6 +316,11 @@ int copy_out_pitched(tti_handle *h, const float *src, float *out)
 namespace ttifd {
 StepArgs handle_step_args(const tti_handle *h) { return step_args(h); }
 void handle_source_tables(const tti_handle *h, SourceTables *t) { source_tables(h, t); }
+int handle_step(tti_handle *h, const SourceTables &tab, float *const *keep)
+{
+  if (keep && h->use_fused) return set_err(h, TTI_ERR_STATE, "the fused step has no hook between its half-steps");
+  return launch_one_step(h, tab, nullptr, keep);
+}
 int handle_check_flag(tti_handle *h) { return check_flag(h); }
 int handle_error(tti_handle *h, int code, const char *msg) { return set_err(h, code, "%s", msg); }
 }  // namespace ttifd
@@ -489,6 +499,9 @@ int tti_destroy(tti_handle *h)
   cudaFree(h->d_sz);
   cudaFree(h->d_src);
   cudaFree(h->d_energy);
+  cudaFree(h->m_eps);
+  cudaFree(h->m_delta);
+  grad_release(h);
   cudaFree(h->d_flag);
   cudaFree(h->d_snap);
   if (h->h_snap) cudaFreeHost(h->h_snap);
@@ -582,6 +595,18 @@ int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const floa
     }
   }
   cudaStreamSynchronize(h->stream);
+  // the gradient's chain rule needs epsilon and delta as given
+  if (rc == TTI_OK && c.variant == TTI_COORDINATE) {
+    for (int k = 0; k < 2; ++k) {
+      float *&dst = k == 0 ? h->m_eps : h->m_delta;
+      if (!dst && cudaMalloc(&dst, g.n * sizeof(float)) != cudaSuccess) {
+        rc = set_err(h, TTI_ERR_NOMEM, "device allocation failed");
+        break;
+      }
+      cudaMemcpyAsync(dst, raw[3 + k], g.n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream);
+    }
+    cudaStreamSynchronize(h->stream);
+  }
   for (auto p : raw) cudaFree(p);
   cudaFree(d_w);
   if (rc == TTI_OK && (h->use_fused || h->use_tiled)) {

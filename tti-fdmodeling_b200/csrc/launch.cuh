@@ -97,6 +97,11 @@ void launch_snapshot(const StepArgs &a, int kind, int savew, float *dst, cudaStr
 StepArgs handle_step_args(const tti_handle *h);
 void handle_source_tables(const tti_handle *h, SourceTables *t);
 int handle_check_flag(tti_handle *h);
+// one time step; `keep` (5 device arrays or null) receives vx vz sxx szz sxz
+// between the velocity sources and the stress update
+int handle_step(tti_handle *h, const SourceTables &tab, float *const *keep);
+// frees the gradient's device memory of h (adjoint.cu)
+void grad_release(tti_handle *h);
 int create_handle(tti_handle **out, const tti_config *cfg, int device, const tti_handle *share, bool force_tiled);
 int handle_error(tti_handle *h, int code, const char *msg);
 

@@ -76,7 +76,15 @@ _SIGNATURES = {
     "profile_steps": (C.c_int, [C.c_void_p, C.c_int, _FP]),
     "kernel_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
     "snapshot_static": (C.c_int, [C.c_void_p, C.c_int, _FP]),
+    "grad_set_observed": (C.c_int, [C.c_void_p, C.c_int, _FP]),
+    "grad_zero": (C.c_int, [C.c_void_p]),
+    "grad_run": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double)]),
+    "grad_fetch": (C.c_int, [C.c_void_p, C.c_int, _FP]),
+    "grad_fetch_source": (C.c_int, [C.c_void_p, _FP]),
+    "grad_accumulators": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t),
+                                    C.POINTER(C.c_size_t)]),
 }
+GRADS = {"vp": 0, "eps": 1, "delta": 2, "theta": 3}
 
 _BATCH_SIGNATURES = {
     "batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(Config), C.c_int, _IP, C.c_int]),
@@ -249,6 +257,39 @@ class Modeling:
         out = np.empty((self.Nx, self.Nz), np.float32)
         self._call("fetch_field", self._h, which, _f(out))
         return out
+
+    # -- adjoint-state gradient (coordinate formulation, stype 1)
+    def grad_set_observed(self, kind, dobs):
+        d = np.ascontiguousarray(dobs, dtype=np.float32)
+        if d.shape != (self._nrec.get(kind, 0), self.nts):
+            raise ValueError(f"observed traces must be [ntrace][nts] = {(self._nrec.get(kind, 0), self.nts)}")
+        self._call("grad_set_observed", self._h, kind, _f(d))
+
+    def grad_zero(self):
+        self._call("grad_zero", self._h)
+
+    def grad_run(self, ncheck: int) -> float:
+        """Adds this shot's gradient to the sums; returns its misfit J."""
+        J = C.c_double()
+        self._call("grad_run", self._h, ncheck, C.byref(J))
+        return J.value
+
+    def grad_fetch(self, name) -> np.ndarray:
+        out = np.empty((self.Nx, self.Nz), np.float32)
+        self._call("grad_fetch", self._h, GRADS[name] if isinstance(name, str) else name, _f(out))
+        return out
+
+    def grad_fetch_source(self, nsrc: int) -> np.ndarray:
+        out = np.empty((nsrc, self.cfg.nt), np.float32)
+        self._call("grad_fetch_source", self._h, _f(out))
+        return out
+
+    def grad_accumulators(self):
+        """(7 device pointers, floats per array, pitch): the sums a multi-GPU run all-reduces."""
+        ptrs = (C.c_void_p * 7)()
+        n, pitch = C.c_size_t(), C.c_size_t()
+        self._call("grad_accumulators", self._h, ptrs, C.byref(n), C.byref(pitch))
+        return [p for p in ptrs], n.value, pitch.value
 
     def fetch_energy(self):
         ek = np.empty(self.cfg.nt, np.float32)
