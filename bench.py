@@ -302,6 +302,69 @@ def run_batched(args, local_rank):
             "clocks": clk.summary()}
 
 
+# ---------------------------------------------------------------- gradient arm
+GRAD_WORKLOAD = dict(nz=600, nx=1200, dx=10.0, dz=10.0, dt=0.0008, fpeak=12.0, ealThick=40, freesurface=0, stype=1,
+                     seistype=1, mt=1, wsave=0, savew=0, mode=1, scalar=1.0, energy=0)
+
+
+def run_gradient(args, local_rank):
+    """One shot of the adjoint-state gradient (forward with checkpoints,
+    recomputation, adjoint) against the plain forward of the same shot.
+    True model: the layered generator at nz=600 nx=1200 (seed 3); start
+    model: Gaussian blur (sigma 15 cells) of vp, epsilon, delta, theta, vs and
+    rho derived from the blurred vp; surface shot at the centre, receivers at
+    every x on z=5; `grad_steps` time steps with `grad_ncheck` checkpoints."""
+    from scipy.ndimage import gaussian_filter
+
+    import ttifd
+
+    K, ncheck = args.grad_steps, args.grad_ncheck
+    gw = dict(GRAD_WORKLOAD)
+    true = synthetic.layered_model(gw["nz"], gw["nx"], seed=3)
+    blur = [gaussian_filter(np.asarray(a, np.float64), 15.0).astype(np.float32)
+            for a in (true.vp, true.epsilon, true.delta, true.theta)]
+    vs = (blur[0] / 1.8).astype(np.float32)
+    rho = (310.0 * blur[0] ** 0.25).astype(np.float32)
+    start = synthetic.Model(blur[0], vs, rho, blur[1], blur[2], blur[3])
+    true = synthetic.Model(true.vp, vs, rho, true.epsilon, true.delta, true.theta)
+    cfg = dict(gw, variant="coordinate_rotation", nt=K)
+    wav = synthetic.ricker(K, cfg["dt"], cfg["fpeak"])[None, :]
+    gx = np.arange(gw["nx"], dtype=np.int32)
+    with ttifd.Modeling(device=local_rank, **cfg) as h:
+        h.upload_model(*synthetic.padded(true, gw["ealThick"]))
+        h.set_source([gw["nx"] // 2], [2], wav)
+        for k in (0, 1):
+            h.set_receivers(k, gx, 5)
+        h.run()
+        dobs = [h.fetch_traces(k) for k in (0, 1)]
+    with ttifd.Modeling(device=local_rank, **cfg) as h:
+        h.upload_model(*synthetic.padded(start, gw["ealThick"]))
+        h.set_source([gw["nx"] // 2], [2], wav)
+        for k in (0, 1):
+            h.set_receivers(k, gx, 5)
+            h.grad_set_observed(k, dobs[k])
+        h.reset()
+        h.step(K)
+        fwd_ms = h.elapsed_ms
+        h.grad_zero()
+        h.grad_run(ncheck)  # warm-up (allocations)
+        h.grad_zero()
+        J = h.grad_run(ncheck)
+        grad_ms = h.elapsed_ms
+        h.grad_zero()
+        h.grad_run(30)  # the 30-checkpoint schedule: 29 segments recomputed
+        grad30_ms = h.elapsed_ms
+        cells = h.Nz * h.Nx
+        gvp = h.grad_fetch("vp").astype(np.float64)  # values near 1e-20: norm in double
+        gnorm, gmax = float(np.linalg.norm(gvp)), float(np.abs(gvp).max())
+    return {"workload": f"adjoint-state gradient, coordinate_rotation, one surface shot on the layered 600x1200 "
+                        f"model (padded {h.Nz}x{h.Nx}), blurred start model, {K} steps, {ncheck} checkpoints",
+            "steps": K, "ncheck": ncheck, "forward_ms": fwd_ms, "gradient_ms": grad_ms,
+            "cost_vs_forward": grad_ms / fwd_ms, "value": cells * K / (grad_ms / 1e3) / 1e9, "unit": "Gcell/s",
+            "ncheck30_ms": grad30_ms, "ncheck30_cost_vs_forward": grad30_ms / fwd_ms,
+            "misfit": J, "grad_vp_norm": gnorm, "grad_vp_max_abs": gmax}
+
+
 # ---------------------------------------------------------------- reference arm
 def ref_program(variant: str):
     for sub in ("bin", "strict"):
@@ -387,6 +450,10 @@ def main():
     ap.add_argument("--batch-shots", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=200)
     ap.add_argument("--no-batch", action="store_true", help="skip the batched measurement")
+    ap.add_argument("--grad-steps", type=int, default=3000)
+    ap.add_argument("--grad-ncheck", type=int, default=1,
+                    help="gradient segments (1: every state kept, as the 600x1200 case fits in HBM)")
+    ap.add_argument("--no-grad", action="store_true", help="skip the gradient measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     WORKLOAD["nx"] = args.nx
@@ -413,6 +480,8 @@ def main():
     line = run_ours(args, rank, world, local_rank)
     if not args.no_batch and world == 1:
         line["batched"] = run_batched(args, local_rank)
+    if not args.no_grad and world == 1:
+        line["gradient"] = run_gradient(args, local_rank)
     if rank == 0:
         if not args.no_cpu_baseline:
             try:

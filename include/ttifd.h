@@ -187,10 +187,13 @@ int tti_fetch_energy(tti_handle *h, float *ek, float *ep);
  * The reference has no adjoint; these entry points add one for the coordinate
  * formulation with the stress source (stype 1). Misfit
  *   J = 1/2 sum over the recorded samples of (d - dobs)^2
- * (the components seistype records). tti_grad_run runs the forward loop,
- * keeping `ncheck` checkpoints, then the discrete adjoint of the loop
- * backwards, recomputing the forward states segment by segment from the
- * checkpoints, and ADDS the shot's gradient to the handle's sums (so several
+ * (the components seistype records). tti_grad_run cuts the loop into
+ * `ncheck` segments: a forward pass saves the state at each segment start
+ * (the checkpoints) and keeps the last segment's states, then the discrete
+ * adjoint runs backwards, recomputing each earlier segment from its
+ * checkpoint. Memory: (ncheck - 1) + ceil(nt / ncheck) states of 5 fields;
+ * ncheck = 1 keeps every state and recomputes nothing. The shot's gradient is
+ * ADDED to the handle's sums (so several
  * shots accumulate; tti_grad_zero clears them). Conventions: vs and rho are
  * held fixed; the MEAL arrays coef1, coef2, Beta stay those of the uploaded
  * model. Gradients are per padded cell, [Nx][Nz], theta in degrees. */
@@ -201,6 +204,7 @@ int tti_fetch_energy(tti_handle *h, float *ek, float *ep);
 /* Observed traces of one recorded component, [ntrace][(nt-1)/mt+1]. */
 int tti_grad_set_observed(tti_handle *h, int kind, const float *dobs);
 int tti_grad_zero(tti_handle *h);
+/* tti_elapsed_ms afterwards gives the device time of the whole run. */
 int tti_grad_run(tti_handle *h, int ncheck, double *misfit);
 int tti_grad_fetch(tti_handle *h, int which, float *out);
 /* dJ/d(source samples) of the last run, [nsrc][nt]. */

@@ -129,3 +129,26 @@ def test_gradient_rejects_other_formulations(gpu_lib):
         with pytest.raises(ttifd.TTIError) as e:
             h.grad_zero()
         assert e.value.code == ttifd.ERR_ARG
+
+
+def test_gradient_sums_are_device_views(gpu_lib):
+    """shots.gradient_sums wraps the library's device sums without a copy (what
+    reduce_gradient all-reduces over NCCL): scaling them through torch scales
+    the fetched gradient."""
+    import torch
+
+    import shots
+
+    cfg, pads, true, w, gx = _case(0)
+    rng = np.random.default_rng(6)
+    dobs = [1e-9 * rng.standard_normal((gx.size, cfg["nt"])).astype(np.float32) for _ in range(3)]
+    h, _ = _device(cfg, pads, w, gx, dobs, 5)
+    with h:
+        before = {n: h.grad_fetch(n) for n in NAMES}
+        sums = shots.gradient_sums(h)
+        assert len(sums) == 7 and all(t.is_cuda and t.dtype == torch.float32 for t in sums)
+        for t in sums:
+            t.mul_(2.0)
+        torch.cuda.synchronize()
+        for n in NAMES:
+            np.testing.assert_allclose(h.grad_fetch(n), 2.0 * before[n], rtol=1e-6)

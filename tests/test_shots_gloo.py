@@ -92,3 +92,70 @@ def test_two_ranks_gloo(tmp_path, oracle_lib):
             h.set_receivers(2, np.arange(60), 1)
             h.run()
             np.testing.assert_array_equal(res["traces"][s], h.fetch_traces(2))
+
+
+GRAD_WORKER = r'''
+import os, sys, pickle
+sys.path.insert(0, os.path.join(sys.argv[1], "tti-fdmodeling_b200"))
+sys.path.insert(0, os.path.join(sys.argv[1], "oracle"))
+import numpy as np, torch
+import shots, synthetic, pyoracle
+g = shots.Group(backend="gloo", timeout_s=60)
+cfg = dict(nz=30, nx=40, nt=150, dx=10.0, dz=10.0, dt=0.001, fpeak=15.0, ealThick=6, seistype=1, mt=1)
+m = synthetic.layered_model(30, 40, seed=7, nlayers=3)
+pads = synthetic.padded(m, 6)
+w = synthetic.ricker(150, 0.001, 15.0)
+acc = torch.zeros((4,) + pads[0].shape, dtype=torch.float64)
+with pyoracle.AdjointOracle(cfg, pads) as adj:
+    adj.set_model(*pads)
+    for k in (0, 1):
+        adj.set_receivers(k, np.arange(0, 40, 2), 2)
+    for s in shots.assign(3, g.rank, g.world):
+        adj.set_source([6 + 12 * s], [2], w[None, :])
+        dobs = [np.zeros((20, 150)), np.zeros((20, 150)), None]
+        J, grad, _ = adj.gradient(dobs)
+        for i, name in enumerate(("vp", "eps", "delta", "theta")):
+            acc[i] += torch.from_numpy(grad[name])
+g.allreduce_([acc])
+if g.rank == 0:
+    pickle.dump(acc.numpy(), open(sys.argv[2], "wb"))
+g.close()
+'''
+
+
+def test_gradient_sum_over_two_ranks_gloo(tmp_path, oracle_lib):
+    """Each rank adds the gradients of its shots; the in-place all-reduce gives
+    the gradient of all shots (oracle gradients on CPU standing in for the
+    device sums that reduce_gradient all-reduces over NCCL)."""
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    script = tmp_path / "gworker.py"
+    script.write_text(GRAD_WORKER)
+    out = tmp_path / "grad.pkl"
+    env = dict(os.environ, MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE="2", OMP_NUM_THREADS="2")
+    procs = [subprocess.Popen([sys.executable, str(script), ROOT, str(out)],
+                              env=dict(env, RANK=str(r), LOCAL_RANK=str(r)),
+                              stdout=subprocess.PIPE, stderr=subprocess.PIPE) for r in range(2)]
+    for p in procs:
+        _, err = p.communicate(timeout=240)
+        assert p.returncode == 0, err.decode()[-2000:]
+    got = pickle.load(open(out, "rb"))
+    import pyoracle
+    import synthetic
+
+    cfg = dict(nz=30, nx=40, nt=150, dx=10.0, dz=10.0, dt=0.001, fpeak=15.0, ealThick=6, seistype=1, mt=1)
+    m = synthetic.layered_model(30, 40, seed=7, nlayers=3)
+    pads = synthetic.padded(m, 6)
+    w = synthetic.ricker(150, 0.001, 15.0)
+    ref = np.zeros_like(got)
+    with pyoracle.AdjointOracle(cfg, pads) as adj:
+        adj.set_model(*pads)
+        for k in (0, 1):
+            adj.set_receivers(k, np.arange(0, 40, 2), 2)
+        for s in range(3):
+            adj.set_source([6 + 12 * s], [2], w[None, :])
+            _, grad, _ = adj.gradient([np.zeros((20, 150)), np.zeros((20, 150)), None])
+            for i, name in enumerate(("vp", "eps", "delta", "theta")):
+                ref[i] += grad[name]
+    np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-30)

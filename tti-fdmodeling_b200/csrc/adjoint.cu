@@ -13,8 +13,10 @@
 //   then the transposed velocity stencils, minus the stress-node stencils,
 //   into lambda_sigma). Each adjoint step needs the forward v after the
 //   velocity half and sigma before the stress half of the same step: the loop
-//   is recomputed segment by segment from checkpoints (ncheck full states
-//   saved in the first pass), the segment's states kept on the device.
+//   is cut into ncheck segments; the first pass saves the full state at the
+//   start of each segment but the last and keeps the last segment's states,
+//   and the reverse pass recomputes each earlier segment from its checkpoint
+//   (ncheck = 1 keeps every state and recomputes nothing).
 // The chain rule maps the stiffness and angle sums to vp, epsilon, delta and
 // theta (degrees) with vs and rho fixed and MEAL coef1, coef2, Beta frozen:
 // c11 = rho' vp'^2 (1 + 2 eps), c13 = rho' (vp'^2 sqrt(f (f + 2 delta)) - vs'^2),
@@ -32,7 +34,8 @@ using namespace ttifd;
 struct GradState {
   int ncheck = 0, seg = 0;  // checkpoints, steps per segment
   float *lam[5] = {};       // adjoint vx vz sxx szz sxz
-  float *T[6] = {};         // per-cell adjoint strain / stress-derivative terms
+  float *T[4] = {};         // stress-half adjoint strain terms (read by the transposed stress stencils)
+  float *TV[6] = {};        // velocity-half adjoint derivative terms (read by the transposed velocity stencils)
   float *acc[7] = {};       // sums: c11 c13 c33 c55 theta(stress node) sin_v cos_v
   float *out[4] = {};       // vp eps delta theta
   float *ckpt = nullptr;    // ncheck x 5 fields
@@ -53,7 +56,8 @@ struct AdjArgs {
   Grid g;
   Params p;
   float *lam[5];
-  float *T[6];
+  float *T[4];
+  float *TV[6];
   float *acc[7];
   const float *keep[5];
   float hx, hz;
@@ -89,15 +93,20 @@ __device__ __forceinline__ bool interior(const Grid &g, int ix, int iz)
   return ix >= NH && ix < g.Nx - NH && iz >= g.izStart && iz < g.Nz - NH;
 }
 
-// residual injection (adjoint of the receiver sampling)
-__global__ void k_inject(Grid g, AdjArgs a, const int *rx, const int *rz, const float *res, int n, int kind)
+// residual injection (adjoint of the receiver sampling), blockIdx.y = component
+struct Inject {
+  const int *rx[3], *rz[3];
+  const float *res[3];  // this step's residual row of each component (null: not recorded)
+  int n[3];
+};
+__global__ void k_inject(Grid g, AdjArgs a, Inject in)
 {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  const size_t c = (size_t)rx[t] * g.ldz + rz[t];
-  const float r = res[t];
-  if (kind == TTI_REC_VX) atomicAdd(a.lam[0] + c, r);
-  else if (kind == TTI_REC_VZ) atomicAdd(a.lam[1] + c, r);
+  const int k = blockIdx.y, t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (!in.res[k] || t >= in.n[k]) return;
+  const size_t c = (size_t)in.rx[k][t] * g.ldz + in.rz[k][t];
+  const float r = in.res[k][t];
+  if (k == TTI_REC_VX) atomicAdd(a.lam[0] + c, r);
+  else if (k == TTI_REC_VZ) atomicAdd(a.lam[1] + c, r);
   else {
     atomicAdd(a.lam[2] + c, 0.5f * r);
     atomicAdd(a.lam[3] + c, 0.5f * r);
@@ -181,54 +190,50 @@ __global__ void __launch_bounds__(BZ *BX) k_adj_stress_local(AdjArgs a)
   a.lam[4][i] = c1 * le;
 }
 
-// transposed stress stencils into lambda_v (minus the velocity-node pairs)
-__global__ void __launch_bounds__(BZ *BX) k_adj_stress_stencil(AdjArgs a)
+// Transposed stress stencils into lambda_v (minus the velocity-node pairs),
+// then the velocity-half adjoint at the same cell: sin/cos theta_v sums,
+// TV0..TV5, lambda_v *= coef1. Both act on one cell's lambda_v, so one pass.
+__global__ void __launch_bounds__(BZ *BX) k_adj_velocity(AdjArgs a)
 {
   const Grid &g = a.g;
   const int iz = blockIdx.x * BZ + threadIdx.x, ix = blockIdx.y * BX + threadIdx.y;
   if (!interior(g, ix, iz)) return;
   const size_t L = g.ldz, i = (size_t)ix * L + iz;
-  float p1, p2, q1, q2, r1, r2, s1, s2;
-  pair_v(a.T[0], L, ix, iz, p1, p2);
-  pair_v(a.T[1], L, ix, iz, q1, q2);
-  pair_v(a.T[2], L, ix, iz, r1, r2);
-  pair_v(a.T[3], L, ix, iz, s1, s2);
-  a.lam[0][i] -= a.hx * (p1 + p2) + a.hz * (q1 - q2);
-  a.lam[1][i] -= a.hx * (r1 + r2) + a.hz * (s1 - s2);
-}
-
-// velocity-half adjoint, local part: sin/cos theta_v sums, T0..T5, lambda_v *= coef1
-__global__ void __launch_bounds__(BZ *BX) k_adj_velocity_local(AdjArgs a)
-{
-  const Grid &g = a.g;
-  const int iz = blockIdx.x * BZ + threadIdx.x, ix = blockIdx.y * BX + threadIdx.y;
-  if (!interior(g, ix, iz)) return;
-  const size_t L = g.ldz, i = (size_t)ix * L + iz;
+  const float hx = a.hx, hz = a.hz;
+  float lx, lz;
+  {
+    float p1, p2, q1, q2, r1, r2, s1, s2;
+    pair_v(a.T[0], L, ix, iz, p1, p2);
+    pair_v(a.T[1], L, ix, iz, q1, q2);
+    pair_v(a.T[2], L, ix, iz, r1, r2);
+    pair_v(a.T[3], L, ix, iz, s1, s2);
+    lx = a.lam[0][i] - (hx * (p1 + p2) + hz * (q1 - q2));
+    lz = a.lam[1][i] - (hx * (r1 + r2) + hz * (s1 - s2));
+  }
   float a1, a2, b1, b2, e1, e2;
   pair_v(a.keep[2], L, ix, iz, a1, a2);
   pair_v(a.keep[3], L, ix, iz, b1, b2);
   pair_v(a.keep[4], L, ix, iz, e1, e2);
-  const float hx = a.hx, hz = a.hz;
   const float sxx_x = hx * (a1 + a2), sxx_z = hx * (a1 - a2);  // 1/dx for both, as coord:633
   const float szz_x = hx * (b1 + b2), szz_z = hz * (b1 - b2);
   const float sxz_x = hx * (e1 + e2), sxz_z = hz * (e1 - e2);
   const float br = a.p.coef2[i] * a.p.invrho[i];
-  const float Fx = br * a.lam[0][i], Fz = br * a.lam[1][i];
+  const float Fx = br * lx, Fz = br * lz;
   const float cv = a.p.csv[i], sv = a.p.snv[i];
   a.acc[5][i] += Fx * (sxz_x - sxx_z) + Fz * (szz_x - sxz_z);
   a.acc[6][i] += Fx * (sxx_x + sxz_z) + Fz * (sxz_x + szz_z);
   const float Axx_x = cv * Fx, Axx_z = -sv * Fx;
   const float Axz_x = sv * Fx + cv * Fz, Axz_z = cv * Fx - sv * Fz;
   const float Azz_x = sv * Fz, Azz_z = cv * Fz;
-  a.T[0][i] = hx * (Axx_x + Axx_z);
-  a.T[1][i] = hx * (Axx_x - Axx_z);
-  a.T[2][i] = hx * Azz_x + hz * Azz_z;
-  a.T[3][i] = hx * Azz_x - hz * Azz_z;
-  a.T[4][i] = hx * Axz_x + hz * Axz_z;
-  a.T[5][i] = hx * Axz_x - hz * Axz_z;
+  a.TV[0][i] = hx * (Axx_x + Axx_z);
+  a.TV[1][i] = hx * (Axx_x - Axx_z);
+  a.TV[2][i] = hx * Azz_x + hz * Azz_z;
+  a.TV[3][i] = hx * Azz_x - hz * Azz_z;
+  a.TV[4][i] = hx * Axz_x + hz * Axz_z;
+  a.TV[5][i] = hx * Axz_x - hz * Axz_z;
   const float c1 = a.p.coef1[i];
-  a.lam[0][i] *= c1;
-  a.lam[1][i] *= c1;
+  a.lam[0][i] = c1 * lx;
+  a.lam[1][i] = c1 * lz;
 }
 
 // transposed velocity stencils into lambda_sigma (minus the stress-node pairs);
@@ -240,12 +245,12 @@ __global__ void __launch_bounds__(BZ *BX) k_adj_velocity_stencil(AdjArgs a)
   if (ix < NH || ix >= g.Nx - NH || iz < a.z_lo || iz >= g.Nz - NH) return;
   const size_t L = g.ldz, i = (size_t)ix * L + iz;
   float p1, p2, q1, q2, r1, r2, u;
-  pair_s(a.T[0], L, ix, iz, p1, u);
-  pair_s(a.T[1], L, ix, iz, u, p2);
-  pair_s(a.T[2], L, ix, iz, q1, u);
-  pair_s(a.T[3], L, ix, iz, u, q2);
-  pair_s(a.T[4], L, ix, iz, r1, u);
-  pair_s(a.T[5], L, ix, iz, u, r2);
+  pair_s(a.TV[0], L, ix, iz, p1, u);
+  pair_s(a.TV[1], L, ix, iz, u, p2);
+  pair_s(a.TV[2], L, ix, iz, q1, u);
+  pair_s(a.TV[3], L, ix, iz, u, q2);
+  pair_s(a.TV[4], L, ix, iz, r1, u);
+  pair_s(a.TV[5], L, ix, iz, u, r2);
   a.lam[2][i] -= p1 + p2;
   a.lam[3][i] -= q1 + q2;
   a.lam[4][i] -= r1 + r2;
@@ -328,6 +333,7 @@ int grad_alloc(tti_handle *h)
   bool ok = true;
   for (auto &p : s->lam) ok = ok && al(&p);
   for (auto &p : s->T) ok = ok && al(&p);
+  for (auto &p : s->TV) ok = ok && al(&p);
   for (auto &p : s->acc) ok = ok && al(&p);
   for (auto &p : s->out) ok = ok && al(&p);
   ok = ok && cudaMalloc(&s->d_J, sizeof(double)) == cudaSuccess;
@@ -343,7 +349,8 @@ AdjArgs adj_args(tti_handle *h, int slot)
   a.g = h->g;
   a.p = handle_step_args(h).p;
   for (int k = 0; k < 5; ++k) a.lam[k] = s->lam[k];
-  for (int k = 0; k < 6; ++k) a.T[k] = s->T[k];
+  for (int k = 0; k < 4; ++k) a.T[k] = s->T[k];
+  for (int k = 0; k < 6; ++k) a.TV[k] = s->TV[k];
   for (int k = 0; k < 7; ++k) a.acc[k] = s->acc[k];
   for (int k = 0; k < 5; ++k) a.keep[k] = s->keep + ((size_t)slot * 5 + k) * h->g.n;
   a.hx = 0.5f * h->invdx;
@@ -360,11 +367,22 @@ int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
   const int it = c.mode == 2 ? c.nt - 1 - n : n;
   const AdjArgs a = adj_args(h, slot);
   const Grid &g = h->g;
-  if (c.seistype > 0 && it % c.mt == 0)
-    for (int k = 0; k < 3; ++k)
-      if (s->res[k] && h->nrec[k] > 0)
-        k_inject<<<(h->nrec[k] + 127) / 128, 128, 0, h->stream>>>(
-            g, a, h->d_rx[k], h->d_rz[k], s->res[k] + (size_t)(it / c.mt) * h->nrec[k], h->nrec[k], k);
+  if (c.seistype > 0 && it % c.mt == 0) {
+    Inject in;
+    int nmax = 0;
+    for (int k = 0; k < 3; ++k) {
+      const bool on = s->res[k] && h->nrec[k] > 0;
+      in.rx[k] = h->d_rx[k];
+      in.rz[k] = h->d_rz[k];
+      in.res[k] = on ? s->res[k] + (size_t)(it / c.mt) * h->nrec[k] : nullptr;
+      in.n[k] = on ? h->nrec[k] : 0;
+      nmax = std::max(nmax, in.n[k]);
+    }
+    if (nmax > 0) {
+      k_inject<<<dim3((nmax + 127) / 128, 3), 128, 0, h->stream>>>(g, a, in);
+      h->launches++;
+    }
+  }
   if (h->nsrc > 0) {
     K1 k1;
     memcpy(k1.k1, tab.k1, sizeof k1.k1);
@@ -374,10 +392,9 @@ int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
   if (c.freesurface == 1) k_adj_free_surface<<<(g.Nx + 127) / 128, 128, 0, h->stream>>>(g, a);
   const dim3 blk(BZ, BX), grd((g.Nz + BZ - 1) / BZ, (g.Nx + BX - 1) / BX);
   k_adj_stress_local<<<grd, blk, 0, h->stream>>>(a);
-  k_adj_stress_stencil<<<grd, blk, 0, h->stream>>>(a);
-  k_adj_velocity_local<<<grd, blk, 0, h->stream>>>(a);
+  k_adj_velocity<<<grd, blk, 0, h->stream>>>(a);
   k_adj_velocity_stencil<<<grd, blk, 0, h->stream>>>(a);
-  h->launches += 4 + (c.freesurface == 1) + (h->nsrc > 0);
+  h->launches += 3 + (c.freesurface == 1) + (h->nsrc > 0);
   GCK(h, cudaGetLastError());
   return TTI_OK;
 }
@@ -391,6 +408,7 @@ void grad_release(tti_handle *h)
   if (!s) return;
   for (auto p : s->lam) cudaFree(p);
   for (auto p : s->T) cudaFree(p);
+  for (auto p : s->TV) cudaFree(p);
   for (auto p : s->acc) cudaFree(p);
   for (auto p : s->out) cudaFree(p);
   for (auto p : s->obs) cudaFree(p);
@@ -463,7 +481,7 @@ int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
     cudaFree(s->ckpt);
     cudaFree(s->keep);
     s->ckpt = s->keep = nullptr;
-    if (cudaMalloc(&s->ckpt, sizeof(float) * state * nseg) != cudaSuccess ||
+    if (cudaMalloc(&s->ckpt, sizeof(float) * state * std::max(1, nseg - 1)) != cudaSuccess ||
         cudaMalloc(&s->keep, sizeof(float) * state * seg) != cudaSuccess) {
       s->ncheck = s->seg = 0;
       return gerr(h, TTI_ERR_NOMEM, "device allocation of the checkpoints failed (use fewer steps per segment)");
@@ -480,14 +498,21 @@ int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
   }
   SourceTables tab;
   handle_source_tables(h, &tab);
-  // pass 1: forward with checkpoints at every segment start
+  // pass 1: forward with a checkpoint at every segment start but the last,
+  // whose states are kept directly (ncheck = 1: all states, no recomputation)
   if ((rc = tti_reset(h))) return rc;
+  GCK(h, cudaEventRecord(h->ev0, h->stream));
   for (int q = 0; q < nseg; ++q) {
-    for (int f = 0; f < 5; ++f)
-      GCK(h, cudaMemcpyAsync(s->ckpt + ((size_t)q * 5 + f) * n, h->fld[f], n * sizeof(float),
-                             cudaMemcpyDeviceToDevice, h->stream));
-    for (int k = q * seg; k < std::min(nt, (q + 1) * seg); ++k)
-      if ((rc = handle_step(h, tab, nullptr))) return rc;
+    const bool last = q == nseg - 1;
+    if (!last)
+      for (int f = 0; f < 5; ++f)
+        GCK(h, cudaMemcpyAsync(s->ckpt + ((size_t)q * 5 + f) * n, h->fld[f], n * sizeof(float),
+                               cudaMemcpyDeviceToDevice, h->stream));
+    for (int k = q * seg; k < std::min(nt, (q + 1) * seg); ++k) {
+      float *keep[5];
+      for (int f = 0; f < 5; ++f) keep[f] = s->keep + ((size_t)(k - q * seg) * 5 + f) * n;
+      if ((rc = handle_step(h, tab, last ? keep : nullptr))) return rc;
+    }
   }
   // residuals and misfit
   GCK(h, cudaMemsetAsync(s->d_J, 0, sizeof(double), h->stream));
@@ -503,21 +528,26 @@ int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
   // adjoint, segment by segment from the last
   for (auto p : s->lam) GCK(h, cudaMemsetAsync(p, 0, n * sizeof(float), h->stream));
   for (auto p : s->T) GCK(h, cudaMemsetAsync(p, 0, n * sizeof(float), h->stream));
+  for (auto p : s->TV) GCK(h, cudaMemsetAsync(p, 0, n * sizeof(float), h->stream));
   for (int q = nseg - 1; q >= 0; --q) {
     const int k0 = q * seg, k1 = std::min(nt, (q + 1) * seg);
-    for (int f = 0; f < 5; ++f)
-      GCK(h, cudaMemcpyAsync(h->fld[f], s->ckpt + ((size_t)q * 5 + f) * n, n * sizeof(float),
-                             cudaMemcpyDeviceToDevice, h->stream));
-    h->step_index = k0;
-    for (int k = k0; k < k1; ++k) {
-      float *keep[5];
-      for (int f = 0; f < 5; ++f) keep[f] = s->keep + ((size_t)(k - k0) * 5 + f) * n;
-      if ((rc = handle_step(h, tab, keep))) return rc;
+    if (q < nseg - 1) {  // recompute the segment from its checkpoint
+      for (int f = 0; f < 5; ++f)
+        GCK(h, cudaMemcpyAsync(h->fld[f], s->ckpt + ((size_t)q * 5 + f) * n, n * sizeof(float),
+                               cudaMemcpyDeviceToDevice, h->stream));
+      h->step_index = k0;
+      for (int k = k0; k < k1; ++k) {
+        float *keep[5];
+        for (int f = 0; f < 5; ++f) keep[f] = s->keep + ((size_t)(k - k0) * 5 + f) * n;
+        if ((rc = handle_step(h, tab, keep))) return rc;
+      }
     }
     for (int k = k1 - 1; k >= k0; --k)
       if ((rc = adjoint_step(h, k, k - k0, tab))) return rc;
   }
-  GCK(h, cudaStreamSynchronize(h->stream));
+  GCK(h, cudaEventRecord(h->ev1, h->stream));
+  GCK(h, cudaEventSynchronize(h->ev1));
+  GCK(h, cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
   h->step_index = nt;
   if (misfit) *misfit = J;
   return handle_check_flag(h);

@@ -201,9 +201,10 @@ int launch_one_step(tti_handle *h, const SourceTables &tab, cudaEvent_t *ev = nu
   else launch_velocity(a, h->stream);
   if (ev) CK(h, cudaEventRecord(ev[1], h->stream));
   if (vsrc) launch_sources(a, s, &tab, c.stype, 0, it, h->stream);
-  if (keep)
-    for (int f = 0; f < 5; ++f)
-      CK(h, cudaMemcpyAsync(keep[f], h->fld[f], h->g.n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+  if (keep) {
+    launch_copy5(h->fld, keep, h->g.n, h->stream);
+    h->launches++;
+  }
   if (ev) CK(h, cudaEventRecord(ev[2], h->stream));
   if (h->use_tiled) {
     const CUtensorMap *tm = static_cast<const CUtensorMap *>(h->tmaps);
@@ -847,11 +848,15 @@ int tti_fetch_traces(tti_handle *h, int kind, float *out)
   if (!h->d_rec[kind]) return set_err(h, TTI_ERR_ARG, "no receivers of kind %d", kind);
   CK(h, cudaSetDevice(h->device));
   const int n = h->nrec[kind], nts = h->nts;
-  std::vector<float> tm((size_t)n * nts);
-  CK(h, cudaMemcpyAsync(tm.data(), h->d_rec[kind], sizeof(float) * tm.size(), cudaMemcpyDeviceToHost, h->stream));
+  // transpose on the device, then one copy into the caller's [ntrace][nts] block
+  float *tmp = nullptr;
+  CK(h, cudaMallocAsync(&tmp, sizeof(float) * (size_t)n * nts, h->stream));
+  launch_transpose(h->d_rec[kind], tmp, nts, n, h->stream);
+  h->launches++;
+  cudaError_t e = cudaMemcpyAsync(out, tmp, sizeof(float) * (size_t)n * nts, cudaMemcpyDeviceToHost, h->stream);
+  cudaFreeAsync(tmp, h->stream);
+  CK(h, e);
   CK(h, cudaStreamSynchronize(h->stream));
-  for (int t = 0; t < nts; ++t)
-    for (int r = 0; r < n; ++r) out[(size_t)r * nts + t] = tm[(size_t)t * n + r];
   return TTI_OK;
 }
 

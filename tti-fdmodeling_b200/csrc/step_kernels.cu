@@ -1,6 +1,8 @@
 // Per-step kernels of the RSG time loop: velocity and stress updates along
 // the two grid diagonals, free surface, sources, receivers, energy, snapshot
 // packing.
+#include <algorithm>
+
 #include "launch.cuh"
 
 namespace ttifd {
@@ -293,46 +295,46 @@ __global__ void k_energy(Grid g, Fields f, Params p, int nz, int nx, double *out
   }
 }
 
-// After the stress update, one thread per padded-grid column applies, in the
-// reference's order for every cell of that column: the free-surface image
-// (coord:847-863), the stress source stype 1 of each source in turn
-// (coord:865-886; tensor:871-895 also adds to tau) and the receiver samples
-// (isoelastic.c:103-144, after the step). Columns do not interact, so one
-// launch replaces three.
+// After the stress update, one warp per padded-grid column applies, in the
+// reference's order for that column: the free-surface image (coord:847-863;
+// lanes 1-5 take the mirrored rows), the stress source stype 1 of each source
+// in turn (coord:865-886, tensor:871-895 also adds to tau; lanes over the 11
+// rows of the window), and the receiver samples (isoelastic.c:103-144; lanes
+// over the column's receivers). Columns do not interact, so one launch
+// replaces three; the warp makes each phase one memory round trip.
 __device__ void post_column(const Grid &g, const Fields &f, const PostArgs &p, int ix, int it, int irec)
 {
+  const int lane = threadIdx.x & 31;
   const size_t col = (size_t)ix * g.ldz;
   if (p.freesurface && ix >= NH && ix < g.Nx - NH) {
     const size_t c = col + g.izStart;
     const float sxx0 = f.sxx[c];
-    float xx[NH], zz[NH], xz[NH];
-#pragma unroll
-    for (int k = 1; k <= NH; ++k) {
-      xx[k - 1] = f.sxx[c + k];
-      zz[k - 1] = f.szz[c + k];
-      xz[k - 1] = f.sxz[c + k];
+    float xx = 0.0f, zz = 0.0f, xz = 0.0f;
+    if (lane >= 1 && lane <= NH) {
+      xx = f.sxx[c + lane];
+      zz = f.szz[c + lane];
+      xz = f.sxz[c + lane];
     }
-    f.sxz[c] = 0.0f;
-    f.szz[c] = 0.0f;
-#pragma unroll
-    for (int k = 1; k <= NH; ++k) {
-      f.sxx[c - k] = __fsub_rn(__fmul_rn(2.0f, sxx0), xx[k - 1]);
-      f.szz[c - k] = -zz[k - 1];
-      f.sxz[c - k] = -xz[k - 1];
+    __syncwarp();
+    if (lane >= 1 && lane <= NH) {
+      f.sxx[c - lane] = __fsub_rn(__fmul_rn(2.0f, sxx0), xx);
+      f.szz[c - lane] = -zz;
+      f.sxz[c - lane] = -xz;
+    } else if (lane == 0) {
+      f.sxz[c] = 0.0f;
+      f.szz[c] = 0.0f;
     }
+    __syncwarp();
   }
   if (p.stype == 1) {
     for (int n = 0; n < p.src.n; ++n) {
       const int dx = ix - p.src.x[n];
       if (dx < -NH || dx > NH) continue;
-      const int z0 = p.src.z[n];
-      const float a = p.src.w[(size_t)n * p.src.nt + it];
-      for (int dz = -NH; dz <= NH; ++dz) {
-        const int iz = z0 + dz;
-        if (iz < 0 || iz >= g.Nz) continue;
-        const float k1 = p.k1[(dx + NH) * 11 + (dz + NH)];
+      const int iz = p.src.z[n] + lane - NH;
+      if (lane <= 2 * NH && iz >= 0 && iz < g.Nz) {
+        const float a = p.src.w[(size_t)n * p.src.nt + it];
+        const float ws = __fmul_rn(p.k1[(dx + NH) * 11 + lane], a);
         const size_t c = col + iz;
-        const float ws = __fmul_rn(k1, a);
         f.sxx[c] = __fadd_rn(f.sxx[c], ws);
         f.szz[c] = __fadd_rn(f.szz[c], ws);
         if (p.tensor) {
@@ -340,13 +342,14 @@ __device__ void post_column(const Grid &g, const Fields &f, const PostArgs &p, i
           f.tzz[c] = __fadd_rn(f.tzz[c], ws);
         }
       }
+      __syncwarp();
     }
   }
   if (irec >= 0) {
     for (int k = 0; k < 3; ++k) {
       if (!p.colptr[k]) continue;
       const int b = p.colptr[k][ix], e = p.colptr[k][ix + 1];
-      for (int j = b; j < e; ++j) {
+      for (int j = b + lane; j < e; j += 32) {
         const size_t c = col + p.rz[k][j];
         float v;
         if (k == TTI_REC_VX) v = f.vx[c];
@@ -361,7 +364,7 @@ __device__ void post_column(const Grid &g, const Fields &f, const PostArgs &p, i
 
 __global__ void k_post(Grid g, Fields f, PostArgs p)
 {
-  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ix = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (ix >= g.Nx) return;
   post_column(g, f, p, ix, p.it, p.irec);
 }
@@ -375,7 +378,7 @@ __global__ void k_post_batch(const BatchPost *bp, const int *step)
   const int it = b.mode2 ? b.nt - 1 - n : n;
   const int irec = b.rec_on && it % b.mt == 0 ? it / b.mt : -1;
   if (!b.p.freesurface && b.p.stype != 1 && irec < 0) return;
-  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ix = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (ix >= b.g.Nx) return;
   post_column(b.g, b.f, b.p, ix, it, irec);
 }
@@ -451,17 +454,62 @@ void launch_energy(const StepArgs &a, int nz, int nx, double *out2, cudaStream_t
 
 void launch_post(const StepArgs &a, const PostArgs &p, cudaStream_t st)
 {
-  k_post<<<(a.g.Nx + 127) / 128, 128, 0, st>>>(a.g, a.f, p);
+  k_post<<<(a.g.Nx + 3) / 4, 128, 0, st>>>(a.g, a.f, p);  // 4 columns (warps) per block
 }
 
 void launch_post_batch(const BatchPost *d, int n, int maxNx, const int *step, cudaStream_t st)
 {
-  if (n > 0) k_post_batch<<<dim3((maxNx + 127) / 128, n), 128, 0, st>>>(d, step);
+  if (n > 0) k_post_batch<<<dim3((maxNx + 3) / 4, n), 128, 0, st>>>(d, step);
 }
 
 void launch_sources_batch(const BatchSrc *d, int n, const int *step, cudaStream_t st)
 {
   if (n > 0) k_sources_batch<<<n, 128, 0, st>>>(d, step);
+}
+
+// five state arrays copied in one launch (the gradient's kept states)
+struct Copy5 {
+  const float4 *src[5];
+  float4 *dst[5];
+};
+__global__ void k_copy5(Copy5 c, size_t n4)
+{
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n4; q += (size_t)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int f = 0; f < 5; ++f) c.dst[f][q] = c.src[f][q];
+  }
+}
+
+void launch_copy5(float *const *src, float *const *dst, size_t n, cudaStream_t st)
+{
+  Copy5 c;
+  for (int f = 0; f < 5; ++f) {
+    c.src[f] = reinterpret_cast<const float4 *>(src[f]);
+    c.dst[f] = reinterpret_cast<float4 *>(dst[f]);
+  }
+  const size_t n4 = n / 4;
+  k_copy5<<<(unsigned)std::min<size_t>((n4 + 255) / 256, 148 * 16), 256, 0, st>>>(c, n4);
+}
+
+// time-major [nts][n] receiver block -> [n][nts] (Receiver2D.recv layout), 32x32 tiles
+__global__ void k_transpose(const float *in, float *out, int nts, int n)
+{
+  __shared__ float t[32][33];
+  const int r0 = blockIdx.x * 32, t0 = blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int tt = t0 + k, r = r0 + threadIdx.x;
+    if (tt < nts && r < n) t[k][threadIdx.x] = in[(size_t)tt * n + r];
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int r = r0 + k, tt = t0 + threadIdx.x;
+    if (tt < nts && r < n) out[(size_t)r * nts + tt] = t[threadIdx.x][k];
+  }
+}
+
+void launch_transpose(const float *in, float *out, int nts, int n, cudaStream_t st)
+{
+  k_transpose<<<dim3((n + 31) / 32, (nts + 31) / 32), dim3(32, 8), 0, st>>>(in, out, nts, n);
 }
 
 void launch_advance(int *step, cudaStream_t st) { k_advance<<<1, 1, 0, st>>>(step); }

@@ -4,7 +4,10 @@ Shots are independent in forward modelling (no exchange during propagation),
 so a multi-GPU run gives each rank its own shots and needs no collective on
 the data path. The collectives here are host-side plumbing over
 torch.distributed: a barrier, the max over ranks of a timing, the sum of a
-per-rank quantity, and gathering per-shot results on rank 0.
+per-rank quantity, and gathering per-shot results on rank 0. The one exchange
+of real data is the gradient: each rank adds its shots' adjoint-state
+gradients into the sums held by its handle, and reduce_gradient sums those
+device arrays over ranks in place (NCCL over NVLink; no host copy).
 """
 from __future__ import annotations
 
@@ -59,6 +62,13 @@ class Group:
     def sum(self, x: float) -> float:
         return x if self.dist is None else self._reduce(x, self.dist.ReduceOp.SUM)
 
+    def allreduce_(self, tensors) -> None:
+        """Sums torch tensors over ranks in place (GPU tensors over NCCL)."""
+        if self.dist is None:
+            return
+        for t in tensors:
+            self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+
     def gather(self, obj):
         """List of every rank's `obj` on rank 0 (None elsewhere)."""
         if self.dist is None:
@@ -71,3 +81,31 @@ class Group:
         if self.dist is not None:
             self.dist.destroy_process_group()
             self.dist = None
+
+
+class _DeviceArray:
+    """A float32 device buffer of the library, exposed to torch without a copy."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f4", "data": (int(ptr), False), "version": 3,
+                                         "strides": None}
+
+
+def gradient_sums(h):
+    """The 7 gradient sums of handle `h` (ttifd.Modeling) as torch views of its device memory."""
+    import torch
+
+    ptrs, n, _ = h.grad_accumulators()
+    return [torch.as_tensor(_DeviceArray(p, n), device=f"cuda:{h.device}") for p in ptrs]
+
+
+def reduce_gradient(group: Group, h) -> None:
+    """Sums the gradient of every rank's shots in place; afterwards tti_grad_fetch
+    on any rank returns the gradient of all shots (the chain rule is linear in the sums)."""
+    if group.dist is None:
+        return
+    import torch
+
+    torch.cuda.synchronize(h.device)
+    group.allreduce_(gradient_sums(h))
+    torch.cuda.synchronize(h.device)

@@ -136,6 +136,7 @@ class Modeling:
     def __init__(self, device: int = 0, lib: C.CDLL | None = None, **cfg):
         self.lib = lib or load()
         self.cfg = Config.make(**cfg)
+        self.device = device
         self._h = C.c_void_p()
         self._call("create", C.byref(self._h), C.byref(self.cfg), device, handle=False)
         nz, nx, e = C.c_int(), C.c_int(), C.c_int()
@@ -305,6 +306,7 @@ class Instance(Modeling):
     def __init__(self, batch: "Batch", index: int, cfg: Config):
         self.lib = batch.lib
         self.cfg = cfg
+        self.device = batch.device
         self._batch = batch  # keeps the batch (and the handle) alive
         self._h = C.c_void_p(self.lib.tti_batch_instance(batch._b, index))
         if not self._h:
@@ -326,6 +328,7 @@ class Batch:
 
     def __init__(self, models, model_of, device: int = 0, lib: C.CDLL | None = None):
         self.lib = lib or load()
+        self.device = device
         self.cfgs = [Config.make(**m) for m in models]
         arr = (Config * len(self.cfgs))(*self.cfgs)
         mo = np.ascontiguousarray(model_of, dtype=np.int32)
