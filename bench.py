@@ -175,20 +175,27 @@ def run_ours(args, rank, world, local_rank):
     cfg_e = dict(WORKLOAD, variant=variant, nt=K)
     wav_e = wav[:K]
     dist_barrier()
+    phases = {}
     t0 = time.perf_counter()
     with ttifd.Modeling(device=local_rank, **cfg_e) as he:
+        phases["create"] = time.perf_counter() - t0
         he.upload_model(*pads)
+        phases["upload"] = time.perf_counter() - t0 - sum(phases.values())
         he.set_source([sx], [sz], wav_e[None, :])
         for k in (0, 1, 2):
             he.set_receivers(k, gx, gz)
+        phases["geometry"] = time.perf_counter() - t0 - sum(phases.values())
         snaps = []
         he.run(lambda it, kind, a: snaps.append(a.nbytes))
+        phases["run"] = time.perf_counter() - t0 - sum(phases.values())
         trs = [he.fetch_traces(k) for k in (0, 1, 2)]
+        phases["fetch"] = time.perf_counter() - t0 - sum(phases.values())
     t_e2e = dist_max(time.perf_counter() - t0)
+    phases["destroy"] = t_e2e - sum(phases.values())
     h2d = sum(a.nbytes for a in pads) + wav_e.nbytes + 3 * 2 * gx.nbytes
     d2h = sum(snaps) + sum(t.nbytes for t in trs)
     e2e = {"value": cells * K * world / t_e2e / 1e9, "unit": "Gcell/s", "h2d_bytes_per_step": h2d / K,
-           "d2h_bytes_per_step": d2h / K, "wall_s": t_e2e,
+           "d2h_bytes_per_step": d2h / K, "wall_s": t_e2e, "phases_s": phases,
            "includes": "tti_create..tti_destroy: model upload + device precompute, geometry, K steps, snapshots to host, traces"}
 
     # roofline of the dominant kernel (per-launch algorithmic bytes / event time)

@@ -48,9 +48,14 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
+@pytest.mark.parametrize("kernel", ["tiled", "naive"])
 @pytest.mark.parametrize("fs", [0, 1])
-def test_gradient_matches_cpu_reference(fs, monkeypatch, gpu_lib):
-    monkeypatch.delenv("TTIFD_KERNEL", raising=False)
+def test_gradient_matches_cpu_reference(fs, kernel, monkeypatch, gpu_lib):
+    """Both adjoint paths: TMA-tiled (default) and one thread per cell (TTIFD_KERNEL=naive)."""
+    if kernel == "naive":
+        monkeypatch.setenv("TTIFD_KERNEL", "naive")
+    else:
+        monkeypatch.delenv("TTIFD_KERNEL", raising=False)
     cfg, pads, true, w, gx = _case(fs)
     with AdjointOracle(cfg, pads) as adj:
         adj.set_model(*true)

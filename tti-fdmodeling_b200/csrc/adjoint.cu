@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "tiled.cuh"
@@ -36,7 +37,7 @@ struct GradState {
   float *lam[5] = {};       // adjoint vx vz sxx szz sxz
   float *T[4] = {};         // stress-half adjoint strain terms (read by the transposed stress stencils)
   float *TV[6] = {};        // velocity-half adjoint derivative terms (read by the transposed velocity stencils)
-  float *acc[7] = {};       // sums: c11 c13 c33 c55 theta(stress node) sin_v cos_v
+  float *acc[7] = {};       // sums: c11 c13 c33 (c55: kept zero, vs and rho are fixed) theta(stress node) sin_v cos_v
   float *out[4] = {};       // vp eps delta theta
   float *ckpt = nullptr;    // ncheck x 5 fields
   float *keep = nullptr;    // seg x 5 fields
@@ -46,6 +47,9 @@ struct GradState {
   int gsrc_n = 0;
   double *d_J = nullptr;
   bool have_obs[3] = {};
+  CUtensorMap *maps = nullptr;  // host copies, 64-byte aligned: T0..T3, TV0..TV5
+  CUtensorMap *slot_maps = nullptr;  // kept sxx, szz, sxz of every segment slot (seg x 3)
+  int slot_maps_n = 0;
 };
 
 namespace {
@@ -177,7 +181,6 @@ __global__ void __launch_bounds__(BZ *BX) k_adj_stress_local(AdjArgs a)
   a.acc[0][i] += b * la * rxx;
   a.acc[1][i] += b * (la * rzz + lb * rxx);
   a.acc[2][i] += b * lb * rzz;
-  a.acc[3][i] += b * le * (rzx + rxz);
   a.acc[4][i] += b * (la * (c13 * rzx - c11 * rxz) + lb * (c33 * rzx - c13 * rxz) + le * c55 * (rxx - rzz));
   const float Lxx = b * (c11 * la + c13 * lb), Lzz = b * (c13 * la + c33 * lb), Lq = b * c55 * le;
   a.T[0][i] = co * Lxx + s * Lq;
@@ -254,6 +257,179 @@ __global__ void __launch_bounds__(BZ *BX) k_adj_velocity_stencil(AdjArgs a)
   a.lam[2][i] -= p1 + p2;
   a.lam[3][i] -= q1 + q2;
   a.lam[4][i] -= r1 + r2;
+}
+
+// ---------------------------------------------------------------- tiled adjoint
+// The three adjoint passes on the forward path's 128 x 16 tiles: every stencil
+// tap comes from a TMA halo box in shared memory (one 2D copy per field, the
+// box origin rounded down to a 16-byte boundary, zeros outside the array),
+// per-cell parameters from the packed arrays.
+struct alignas(64) AdjTile {
+  CUtensorMap map[7];
+  AdjArgs a;
+  fused::Packed pk;
+  int z_base;  // first tile row (multiple of 4)
+  int *err;    // bit 4: a TMA wait timed out
+};
+
+struct TileCells {
+  int x0, z0, xc, z;
+};
+__device__ __forceinline__ TileCells tile_cells(int z_base)
+{
+  TileCells c;
+  c.z0 = z_base + blockIdx.x * tiled::TZ;
+  c.x0 = NH + blockIdx.y * tiled::TX;
+  c.xc = c.x0 + (tiled::TX / 4) * (threadIdx.x >> 7);
+  c.z = c.z0 + (threadIdx.x & 127);
+  return c;
+}
+
+// stress-node pair of shared field q centred on (x, z): q[m * BZ + n] = value at (x + m, z + n)
+__device__ __forceinline__ void spair(const float *q, float &d1, float &d2)
+{
+  constexpr int B = tiled::BZ;
+  float s1 = rsg(0) * (q[0] - q[-B - 1]), s2 = rsg(0) * (q[-1] - q[-B]);
+#pragma unroll
+  for (int k = 2; k <= NH; ++k) {
+    s1 += rsg(k - 1) * (q[(k - 1) * B + k - 1] - q[-k * B - k]);
+    s2 += rsg(k - 1) * (q[(k - 1) * B - k] - q[-k * B + k - 1]);
+  }
+  d1 = s1;
+  d2 = s2;
+}
+
+// velocity-node pair of shared field q centred on (x, z)
+__device__ __forceinline__ void vpair(const float *q, float &d1, float &d2)
+{
+  constexpr int B = tiled::BZ;
+  float s1 = rsg(0) * (q[B + 1] - q[0]), s2 = rsg(0) * (q[B] - q[1]);
+#pragma unroll
+  for (int k = 2; k <= NH; ++k) {
+    s1 += rsg(k - 1) * (q[k * B + k] - q[(1 - k) * B + 1 - k]);
+    s2 += rsg(k - 1) * (q[k * B + 1 - k] - q[(1 - k) * B + k]);
+  }
+  d1 = s1;
+  d2 = s2;
+}
+
+// transposed stress stencils into lambda_v, then the velocity-half adjoint
+// (maps: T0..T3, kept sxx, szz, sxz)
+__global__ void __launch_bounds__(tiled::NT, 2) k_adj_velocity_tiled(const __grid_constant__ AdjTile at)
+{
+  constexpr int F = tiled::FIELD, B = tiled::BZ;
+  extern __shared__ __align__(128) float sm[];
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm + 7 * F);
+  const AdjArgs &a = at.a;
+  const Grid &g = a.g;
+  const TileCells c = tile_cells(at.z_base);
+  tiled::tma::issue_tiles(at.map, sm, bar, 7, c.z0, c.x0, 4);
+  const int z = c.z;
+  const bool zin = z >= g.izStart && z < g.Nz - NH;
+  if (!tiled::tma::wait_tiles(at.err, bar)) return;
+  if (!zin) return;
+  const float hx = a.hx, hz = a.hz;
+#pragma unroll
+  for (int j = 0; j < tiled::TX / 4; ++j) {
+    const int x = c.xc + j;
+    if (x >= g.Nx - NH) break;
+    const size_t i = (size_t)x * g.ldz + z;
+    const float *q = sm + (x - c.x0 + 4) * B + (z - c.z0 + 8);
+    float lx, lz;
+    {
+      float p1, p2, q1, q2;
+      vpair(q, p1, p2);
+      vpair(q + F, q1, q2);
+      lx = a.lam[0][i] - (hx * (p1 + p2) + hz * (q1 - q2));
+      vpair(q + 2 * F, p1, p2);
+      vpair(q + 3 * F, q1, q2);
+      lz = a.lam[1][i] - (hx * (p1 + p2) + hz * (q1 - q2));
+    }
+    float a1, a2, b1, b2, e1, e2;
+    vpair(q + 4 * F, a1, a2);
+    vpair(q + 5 * F, b1, b2);
+    vpair(q + 6 * F, e1, e2);
+    const float sxx_x = hx * (a1 + a2), sxx_z = hx * (a1 - a2);  // 1/dx for both, as coord:633
+    const float szz_x = hx * (b1 + b2), szz_z = hz * (b1 - b2);
+    const float sxz_x = hx * (e1 + e2), sxz_z = hz * (e1 - e2);
+    const float2 cf = __ldg(at.pk.cf + i), vsc = __ldg(at.pk.vsc + i);
+    const float br = cf.y * __ldg(a.p.invrho + i);
+    const float Fx = br * lx, Fz = br * lz;
+    const float sv = vsc.x, cv = vsc.y;
+    a.acc[5][i] += Fx * (sxz_x - sxx_z) + Fz * (szz_x - sxz_z);
+    a.acc[6][i] += Fx * (sxx_x + sxz_z) + Fz * (sxz_x + szz_z);
+    const float Axx_x = cv * Fx, Axx_z = -sv * Fx;
+    const float Axz_x = sv * Fx + cv * Fz, Axz_z = cv * Fx - sv * Fz;
+    const float Azz_x = sv * Fz, Azz_z = cv * Fz;
+    a.TV[0][i] = hx * (Axx_x + Axx_z);
+    a.TV[1][i] = hx * (Axx_x - Axx_z);
+    a.TV[2][i] = hx * Azz_x + hz * Azz_z;
+    a.TV[3][i] = hx * Azz_x - hz * Azz_z;
+    a.TV[4][i] = hx * Axz_x + hz * Axz_z;
+    a.TV[5][i] = hx * Axz_x - hz * Axz_z;
+    a.lam[0][i] = cf.x * lx;
+    a.lam[1][i] = cf.x * lz;
+  }
+}
+
+// transposed velocity stencils into lambda_sigma (maps: TV0..TV5), rows from z_lo
+__global__ void __launch_bounds__(tiled::NT, 2) k_adj_vstencil_tiled(const __grid_constant__ AdjTile at)
+{
+  constexpr int F = tiled::FIELD, B = tiled::BZ;
+  extern __shared__ __align__(128) float sm[];
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm + 6 * F);
+  const AdjArgs &a = at.a;
+  const Grid &g = a.g;
+  const TileCells c = tile_cells(at.z_base);
+  tiled::tma::issue_tiles(at.map, sm, bar, 6, c.z0, c.x0, 5);
+  const int z = c.z;
+  const bool zin = z >= a.z_lo && z < g.Nz - NH;
+  if (!tiled::tma::wait_tiles(at.err, bar)) return;
+  if (!zin) return;
+#pragma unroll
+  for (int j = 0; j < tiled::TX / 4; ++j) {
+    const int x = c.xc + j;
+    if (x >= g.Nx - NH) break;
+    const size_t i = (size_t)x * g.ldz + z;
+    const float *q = sm + (x - c.x0 + 5) * B + (z - c.z0 + 8);
+    float p1, p2, q1, q2, r1, r2, u;
+    spair(q, p1, u);
+    spair(q + F, u, p2);
+    spair(q + 2 * F, q1, u);
+    spair(q + 3 * F, u, q2);
+    spair(q + 4 * F, r1, u);
+    spair(q + 5 * F, u, r2);
+    a.lam[2][i] -= p1 + p2;
+    a.lam[3][i] -= q1 + q2;
+    a.lam[4][i] -= r1 + r2;
+  }
+}
+
+template <typename K>
+cudaError_t launch_adj_tile(K kernel, const AdjTile &at, int nfields, int z_first, const Grid &g, cudaStream_t st)
+{
+  const size_t bytes = (size_t)nfields * tiled::FIELD * sizeof(float) + 16;
+  static std::mutex mu;
+  static const void *done[8];
+  static int ndone = 0;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    bool seen = false;
+    for (int k = 0; k < ndone; ++k) seen = seen || done[k] == (const void *)kernel;
+    if (!seen) {
+      cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+      if (e != cudaSuccess) return e;
+      if (ndone < 8) done[ndone++] = (const void *)kernel;
+    }
+  }
+  AdjTile b = at;
+  b.z_base = z_first & ~3;
+  const int nz = g.Nz - NH - b.z_base, nx = g.Nx - 2 * NH;
+  if (nz <= 0 || nx <= 0) return cudaSuccess;
+  kernel<<<dim3((nz + tiled::TZ - 1) / tiled::TZ, (nx + tiled::TX - 1) / tiled::TX), tiled::NT, bytes, st>>>(b);
+  return cudaGetLastError();
 }
 
 // residuals d - dobs (time-major) and J
@@ -338,6 +514,15 @@ int grad_alloc(tti_handle *h)
   for (auto &p : s->out) ok = ok && al(&p);
   ok = ok && cudaMalloc(&s->d_J, sizeof(double)) == cudaSuccess;
   if (!ok) return gerr(h, TTI_ERR_NOMEM, "device allocation of the gradient buffers failed");
+  if (h->use_tiled) {
+    void *mem = nullptr;
+    if (posix_memalign(&mem, 64, 10 * sizeof(CUtensorMap)) != 0)
+      return gerr(h, TTI_ERR_NOMEM, "host allocation failed");
+    s->maps = static_cast<CUtensorMap *>(mem);
+    for (int k = 0; k < 10; ++k)
+      if (!tiled::encode_map(s->maps + k, h->g, k < 4 ? s->T[k] : s->TV[k - 4]))
+        return gerr(h, TTI_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+  }
   GCK(h, cudaStreamSynchronize(h->stream));
   return TTI_OK;
 }
@@ -390,11 +575,28 @@ int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
                                                    s->gsrc, it);
   }
   if (c.freesurface == 1) k_adj_free_surface<<<(g.Nx + 127) / 128, 128, 0, h->stream>>>(g, a);
+  h->launches += 3 + (c.freesurface == 1) + (h->nsrc > 0);
+  if (h->use_tiled) {  // TMA halo tiles (the per-cell kernels below serve TTIFD_KERNEL=naive)
+    // the stress-half adjoint stays one thread per cell: it is bound by its
+    // per-cell reads and writes, not by its two stencil fields
+    const dim3 blk(BZ, BX), grd((g.Nz + BZ - 1) / BZ, (g.Nx + BX - 1) / BX);
+    k_adj_stress_local<<<grd, blk, 0, h->stream>>>(a);
+    AdjTile at;
+    memset(&at, 0, sizeof at);
+    at.a = a;
+    at.pk = fused::Packed{h->pk_cf, h->pk_vsc, h->pk_sc, h->pk_c4};
+    at.err = h->d_flag;
+    for (int k = 0; k < 4; ++k) at.map[k] = s->maps[k];
+    for (int f = 0; f < 3; ++f) at.map[4 + f] = s->slot_maps[(size_t)slot * 3 + f];  // kept sxx, szz, sxz
+    GCK(h, launch_adj_tile(k_adj_velocity_tiled, at, 7, g.izStart, g, h->stream));
+    for (int k = 0; k < 6; ++k) at.map[k] = s->maps[4 + k];
+    GCK(h, launch_adj_tile(k_adj_vstencil_tiled, at, 6, a.z_lo, g, h->stream));
+    return TTI_OK;
+  }
   const dim3 blk(BZ, BX), grd((g.Nz + BZ - 1) / BZ, (g.Nx + BX - 1) / BX);
   k_adj_stress_local<<<grd, blk, 0, h->stream>>>(a);
   k_adj_velocity<<<grd, blk, 0, h->stream>>>(a);
   k_adj_velocity_stencil<<<grd, blk, 0, h->stream>>>(a);
-  h->launches += 3 + (c.freesurface == 1) + (h->nsrc > 0);
   GCK(h, cudaGetLastError());
   return TTI_OK;
 }
@@ -417,6 +619,8 @@ void grad_release(tti_handle *h)
   cudaFree(s->keep);
   cudaFree(s->gsrc);
   cudaFree(s->d_J);
+  free(s->maps);
+  free(s->slot_maps);
   delete s;
   h->grad = nullptr;
 }
@@ -481,6 +685,7 @@ int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
     cudaFree(s->ckpt);
     cudaFree(s->keep);
     s->ckpt = s->keep = nullptr;
+    s->slot_maps_n = 0;  // the kept-state tensor maps point into the old buffer
     if (cudaMalloc(&s->ckpt, sizeof(float) * state * std::max(1, nseg - 1)) != cudaSuccess ||
         cudaMalloc(&s->keep, sizeof(float) * state * seg) != cudaSuccess) {
       s->ncheck = s->seg = 0;
@@ -488,6 +693,20 @@ int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
     }
     s->ncheck = nseg;
     s->seg = seg;
+  }
+  if (h->use_tiled && s->slot_maps_n != seg) {
+    free(s->slot_maps);
+    s->slot_maps = nullptr;
+    s->slot_maps_n = 0;
+    void *mem = nullptr;
+    if (posix_memalign(&mem, 64, sizeof(CUtensorMap) * 3 * (size_t)seg) != 0)
+      return gerr(h, TTI_ERR_NOMEM, "host allocation failed");
+    s->slot_maps = static_cast<CUtensorMap *>(mem);
+    for (int k = 0; k < seg; ++k)
+      for (int f = 0; f < 3; ++f)
+        if (!tiled::encode_map(s->slot_maps + (size_t)k * 3 + f, h->g, s->keep + ((size_t)k * 5 + 2 + f) * n))
+          return gerr(h, TTI_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    s->slot_maps_n = seg;
   }
   if (s->gsrc_n != h->nsrc * nt) {
     cudaFree(s->gsrc);

@@ -24,50 +24,6 @@ namespace tiled {
 
 namespace {
 
-__device__ __forceinline__ unsigned smem_u32(const void *p)
-{
-  return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count)
-{
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, unsigned bytes)
-{
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-               : "memory");
-}
-
-// bounded wait (about a second) so a copy that never lands cannot hang the GPU
-__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, unsigned limit = 1u << 20)
-{
-  const unsigned a = smem_u32(bar);
-  for (unsigned n = 0; n < limit; ++n) {
-    unsigned ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (ok) return true;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void tma_load_2d(float *dst, const CUtensorMap *map, int c_inner, int c_outer,
-                                            unsigned long long *bar)
-{
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-          smem_u32(dst)),
-      "l"(reinterpret_cast<unsigned long long>(map)), "r"(c_inner), "r"(c_outer), "r"(smem_u32(bar))
-      : "memory");
-}
-
-static_assert((BZ * 4) % 16 == 0, "TMA inner box extent must be a multiple of 16 bytes");
-
 // tile cells handled by a thread: row zr, columns xc .. xc + TX/4 - 1
 struct Cells {
   int x0, z0, xc, zr;
@@ -81,38 +37,6 @@ __device__ __forceinline__ Cells cells_of(const HalfArgs &a, int tz, int tx)
   c.xc = c.x0 + (TX / 4) * (t >> 7);
   c.zr = c.z0 + (t & 127);
   return c;
-}
-
-// Issues the TMA copies of the halo boxes of `n` fields (origin row z0 - 8,
-// column x0 - xoff); waited for by wait_tiles.
-__device__ __forceinline__ void issue_tiles(const CUtensorMap *map, float *sm, unsigned long long *bar, int n, int z0,
-                                            int x0, int xoff)
-{
-  constexpr unsigned BOX_BYTES = BX * BZ * 4;
-  const int t = threadIdx.x;
-  if (t == 0) {
-    mbar_init(bar, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-  if (t == 0) {
-    mbar_arrive_expect_tx(bar, n * BOX_BYTES);
-    for (int f = 0; f < n; ++f) tma_load_2d(sm + f * FIELD, map + f, z0 - 8, x0 - xoff, bar);
-  }
-}
-
-// returns false (all threads) after a timed-out wait
-__device__ __forceinline__ bool wait_tiles(const HalfArgs &a, unsigned long long *bar)
-{
-  const bool ok = mbar_wait(bar, 0);
-  if (__syncthreads_or(!ok)) {
-    if (threadIdx.x == 0) {
-      atomicOr(a.err, 4);
-      mbar_wait(bar, 0, 1u << 16);  // give the copies in flight a bounded time
-    }
-    return false;
-  }
-  return true;
 }
 
 // true when every cell of the tile lies where coef1 = 1 and coef2 = dt
@@ -131,12 +55,12 @@ __device__ __forceinline__ void velocity_tile(const HalfArgs &a, const CUtensorM
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm + 3 * FIELD);
   const Grid &g = a.g;
   const Cells c = cells_of(a, tz, tx);
-  issue_tiles(map, sm, bar, 3, c.z0, c.x0, 4);
+  tma::issue_tiles(map, sm, bar, 3, c.z0, c.x0, 4);
   const int L = g.ldz;
   const bool und = tile_undamped(a, c);
   const int z = c.zr;
   const bool zin = z >= g.izStart && z < g.Nz - NH;
-  if (!wait_tiles(a, bar)) return;
+  if (!tma::wait_tiles(a.err, bar)) return;
   if (!zin) return;
   const float invdx = a.invdx, invdz = a.invdz;
 #pragma unroll
@@ -276,11 +200,11 @@ __device__ __forceinline__ void stress_tile(const HalfArgs &a, const CUtensorMap
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm + 2 * FIELD);
   const Grid &g = a.g;
   const Cells c = cells_of(a, tz, tx);
-  issue_tiles(map, sm, bar, 2, c.z0, c.x0, 5);
+  tma::issue_tiles(map, sm, bar, 2, c.z0, c.x0, 5);
   const bool und = tile_undamped(a, c);
   const int z = c.zr;
   const bool zin = z >= g.izStart && z < g.Nz - NH;
-  if (!wait_tiles(a, bar)) return;
+  if (!tma::wait_tiles(a.err, bar)) return;
   if (!zin) return;
   const float invdx = a.invdx, invdz = a.invdz;
 #pragma unroll
