@@ -506,6 +506,10 @@ int tti_destroy(tti_handle *h)
   cudaFree(h->d_flag);
   cudaFree(h->d_snap);
   if (h->h_snap) cudaFreeHost(h->h_snap);
+  for (int b = 0; b < 2; ++b) {
+    cudaFree(h->d_stage[b]);
+    if (h->h_stage[b]) cudaFreeHost(h->h_stage[b]);
+  }
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   free(h->tmaps);
@@ -848,15 +852,35 @@ int tti_fetch_traces(tti_handle *h, int kind, float *out)
   if (!h->d_rec[kind]) return set_err(h, TTI_ERR_ARG, "no receivers of kind %d", kind);
   CK(h, cudaSetDevice(h->device));
   const int n = h->nrec[kind], nts = h->nts;
-  // transpose on the device, then one copy into the caller's [ntrace][nts] block
-  float *tmp = nullptr;
-  CK(h, cudaMallocAsync(&tmp, sizeof(float) * (size_t)n * nts, h->stream));
-  launch_transpose(h->d_rec[kind], tmp, nts, n, h->stream);
-  h->launches++;
-  cudaError_t e = cudaMemcpyAsync(out, tmp, sizeof(float) * (size_t)n * nts, cudaMemcpyDeviceToHost, h->stream);
-  cudaFreeAsync(tmp, h->stream);
-  CK(h, e);
-  CK(h, cudaStreamSynchronize(h->stream));
+  // Chunks of receivers: transposed on the device into one of two staging
+  // buffers, copied to pinned memory, and copied on the host into the caller's
+  // [ntrace][nts] block while the next chunk is in flight.
+  constexpr size_t STAGE = (size_t)4 << 20;  // floats per chunk
+  for (int b = 0; b < 2; ++b) {
+    if (!h->d_stage[b]) CK(h, cudaMalloc(&h->d_stage[b], STAGE * sizeof(float)));
+    if (!h->h_stage[b]) CK(h, cudaMallocHost(&h->h_stage[b], STAGE * sizeof(float)));
+  }
+  if (!h->pev[5]) CK(h, cudaEventCreateWithFlags(&h->pev[5], cudaEventDisableTiming));
+  if (!h->pev[6]) CK(h, cudaEventCreateWithFlags(&h->pev[6], cudaEventDisableTiming));
+  if ((size_t)nts > STAGE || nts > 65535 * 32)
+    return set_err(h, TTI_ERR_ARG, "trace of %d samples is longer than the fetch supports", nts);
+  const int per = (int)std::max<size_t>(1, STAGE / (size_t)nts);  // receivers per chunk
+  const int nchunk = (n + per - 1) / per;
+  for (int c = 0; c <= nchunk; ++c) {
+    if (c < nchunk) {
+      const int r0 = c * per, nr = std::min(per, n - r0), b = c & 1;
+      launch_transpose(h->d_rec[kind], h->d_stage[b], nts, n, r0, nr, h->stream);
+      h->launches++;
+      CK(h, cudaMemcpyAsync(h->h_stage[b], h->d_stage[b], sizeof(float) * (size_t)nr * nts, cudaMemcpyDeviceToHost,
+                            h->stream));
+      CK(h, cudaEventRecord(h->pev[5 + b], h->stream));
+    }
+    if (c > 0) {  // the previous chunk to the caller
+      const int p = c - 1, r0 = p * per, nr = std::min(per, n - r0), b = p & 1;
+      CK(h, cudaEventSynchronize(h->pev[5 + b]));
+      memcpy(out + (size_t)r0 * nts, h->h_stage[b], sizeof(float) * (size_t)nr * nts);
+    }
+  }
   return TTI_OK;
 }
 

@@ -91,8 +91,8 @@ void launch_sources_batch(const BatchSrc *d, int n, const int *step, cudaStream_
 void launch_advance(int *step, cudaStream_t st);
 // dst[f][0..n) = src[f][0..n), f < 5 (n a multiple of 4, 16-byte aligned arrays)
 void launch_copy5(float *const *src, float *const *dst, size_t n, cudaStream_t st);
-// out[r][t] = in[t][r] for t < nts, r < n
-void launch_transpose(const float *in, float *out, int nts, int n, cudaStream_t st);
+// out[r - r0][t] = in[t][r] for t < nts, r0 <= r < r0 + nr (in has n columns)
+void launch_transpose(const float *in, float *out, int nts, int n, int r0, int nr, cudaStream_t st);
 // Pack a snapshot (kind 1..7) of the physical (savew = 0) or padded area
 // into a dense [nx_out][nz_out] buffer.
 void launch_snapshot(const StepArgs &a, int kind, int savew, float *dst, cudaStream_t st);

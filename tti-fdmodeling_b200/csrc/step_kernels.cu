@@ -491,25 +491,26 @@ void launch_copy5(float *const *src, float *const *dst, size_t n, cudaStream_t s
   k_copy5<<<(unsigned)std::min<size_t>((n4 + 255) / 256, 148 * 16), 256, 0, st>>>(c, n4);
 }
 
-// time-major [nts][n] receiver block -> [n][nts] (Receiver2D.recv layout), 32x32 tiles
-__global__ void k_transpose(const float *in, float *out, int nts, int n)
+// Receivers r0 .. r0 + nr - 1 of the time-major [nts][n] block, transposed to
+// [nr][nts] (the Receiver2D.recv layout), through 32 x 32 shared tiles.
+__global__ void k_transpose(const float *in, float *out, int nts, int n, int r0, int nr)
 {
   __shared__ float t[32][33];
-  const int r0 = blockIdx.x * 32, t0 = blockIdx.y * 32;
+  const int ra = blockIdx.x * 32, t0 = blockIdx.y * 32;
   for (int k = threadIdx.y; k < 32; k += blockDim.y) {
-    const int tt = t0 + k, r = r0 + threadIdx.x;
-    if (tt < nts && r < n) t[k][threadIdx.x] = in[(size_t)tt * n + r];
+    const int tt = t0 + k, r = ra + threadIdx.x;
+    if (tt < nts && r < nr) t[k][threadIdx.x] = in[(size_t)tt * n + r0 + r];
   }
   __syncthreads();
   for (int k = threadIdx.y; k < 32; k += blockDim.y) {
-    const int r = r0 + k, tt = t0 + threadIdx.x;
-    if (tt < nts && r < n) out[(size_t)r * nts + tt] = t[threadIdx.x][k];
+    const int r = ra + k, tt = t0 + threadIdx.x;
+    if (tt < nts && r < nr) out[(size_t)r * nts + tt] = t[threadIdx.x][k];
   }
 }
 
-void launch_transpose(const float *in, float *out, int nts, int n, cudaStream_t st)
+void launch_transpose(const float *in, float *out, int nts, int n, int r0, int nr, cudaStream_t st)
 {
-  k_transpose<<<dim3((n + 31) / 32, (nts + 31) / 32), dim3(32, 8), 0, st>>>(in, out, nts, n);
+  k_transpose<<<dim3((nr + 31) / 32, (nts + 31) / 32), dim3(32, 8), 0, st>>>(in, out, nts, n, r0, nr);
 }
 
 void launch_advance(int *step, cudaStream_t st) { k_advance<<<1, 1, 0, st>>>(step); }

@@ -110,6 +110,8 @@ struct tti_handle {
   int *d_flag = nullptr;       // nonfinite watchdog
   float *d_snap = nullptr;
   float *h_snap = nullptr;     // pinned
+  float *d_stage[2] = {};      // trace fetch: device chunks (TTI_STAGE_FLOATS each)
+  float *h_stage[2] = {};      // trace fetch: pinned host chunks
   size_t snap_cap = 0;
   bool have_model = false;
   int step_index = 0;
