@@ -191,6 +191,7 @@ int launch_one_step(tti_handle *h, const SourceTables &tab, cudaEvent_t *ev = nu
     ha.x_base = NH;
     ha.undamped_ok = h->undamped_ok;
     ha.freesurface = c.freesurface;
+    tiled::set_square(ha, h->exact);
     ha.err = h->d_flag;
     ha.map[0] = tm[2];  // sxx szz sxz for the velocity update
     ha.map[1] = tm[3];

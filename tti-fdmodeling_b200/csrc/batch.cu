@@ -29,6 +29,7 @@ struct tti_batch {
   std::vector<int> model_of;
   int max_nt = 0, max_Nx = 0;
   bool any_vsrc = false;
+  bool square = false;  // every instance uses the folded coefficients (FMA mode, dx == dz)
   // device tables (fixed addresses: a captured graph refers to them)
   tiled::HalfArgs *d_vel = nullptr, *d_str = nullptr;
   tiled::Work *d_work = nullptr;
@@ -81,6 +82,7 @@ int build_tables(tti_batch *b)
   std::vector<SourceTables> tab(nm);
   for (int m = 0; m < nm; ++m) handle_source_tables(b->models[m], &tab[m]);
   std::vector<int> tiles(n);
+  bool all_square = true;
   for (int i = 0; i < n; ++i) {
     tti_handle *h = b->inst[i];
     const tti_handle *mh = b->models[b->model_of[i]];
@@ -102,6 +104,8 @@ int build_tables(tti_batch *b)
     ha.x_base = NH;
     ha.undamped_ok = h->undamped_ok;
     ha.freesurface = c.freesurface;
+    tiled::set_square(ha, b->exact);
+    all_square = all_square && ha.square;
     ha.err = h->d_flag;
     ha.nt = c.nt;
     ha.tiles_z = (int)gr.x;
@@ -161,6 +165,13 @@ int build_tables(tti_batch *b)
         for (size_t k = g0; k < std::min(mine.size(), g0 + G); ++k) work.push_back(tiled::Work{mine[k], t});
   }
   if ((int)work.size() != b->nwork) return berr(b, TTI_ERR_STATE, "work table size changed");
+  if (all_square != b->square && b->exec) {  // the captured launches select the kernels
+    cudaGraphExecDestroy(b->exec);
+    cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+  }
+  b->square = all_square;
   BCK(b, cudaMemcpyAsync(b->d_vel, vel.data(), sizeof(tiled::HalfArgs) * n, cudaMemcpyHostToDevice, b->stream));
   BCK(b, cudaMemcpyAsync(b->d_str, str.data(), sizeof(tiled::HalfArgs) * n, cudaMemcpyHostToDevice, b->stream));
   BCK(b, cudaMemcpyAsync(b->d_post, post.data(), sizeof(BatchPost) * n, cudaMemcpyHostToDevice, b->stream));
@@ -176,9 +187,9 @@ int build_tables(tti_batch *b)
 int launch_step(tti_batch *b)
 {
   const int n = (int)b->inst.size();
-  BCK(b, tiled::launch_velocity_batch(b->d_vel, b->d_work, b->nwork, b->d_step, b->variant, b->exact, b->stream));
+  BCK(b, tiled::launch_velocity_batch(b->d_vel, b->d_work, b->nwork, b->d_step, b->variant, b->exact, b->square, b->stream));
   if (b->any_vsrc) launch_sources_batch(b->d_src, n, b->d_step, b->stream);
-  BCK(b, tiled::launch_stress_batch(b->d_str, b->d_work, b->nwork, b->d_step, b->variant, b->exact, b->stream));
+  BCK(b, tiled::launch_stress_batch(b->d_str, b->d_work, b->nwork, b->d_step, b->variant, b->exact, b->square, b->stream));
   launch_post_batch(b->d_post, n, b->max_Nx, b->d_step, b->stream);
   launch_advance(b->d_step, b->stream);
   BCK(b, cudaGetLastError());
@@ -190,7 +201,7 @@ int launches_per_step(const tti_batch *b) { return 4 + (b->any_vsrc ? 1 : 0); }
 int ensure_graph(tti_batch *b)
 {
   if (b->exec || b->graph_steps <= 0) return TTI_OK;
-  BCK(b, tiled::prepare_batch(b->variant, b->exact));
+  BCK(b, tiled::prepare_batch(b->variant, b->exact, b->square));
   BCK(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
   int rc = TTI_OK;
   for (int k = 0; k < b->graph_steps && rc == TTI_OK; ++k) rc = launch_step(b);

@@ -31,7 +31,16 @@ struct alignas(64) HalfArgs {
   int *err;    // bit 4: a TMA wait timed out
   int nt;      // batched launches: time steps of this instance (its CTAs idle once the step counter reaches it)
   int tiles_z; // batched launches: tile rows of this instance's grid
+  int square;  // FMA mode with dx == dz: stencil coefficients hc fold in h = 0.5 / dx
+  float hc[5]; // h * C_k
 };
+
+// Sets square / hc for FMA-mode launches on grids with dx == dz.
+inline void set_square(HalfArgs &a, bool exact)
+{
+  a.square = !exact && a.invdx == a.invdz;
+  for (int k = 0; k < 5; ++k) a.hc[k] = 0.5f * a.invdx * rsg(k);
+}
 
 // One CTA of a batched launch: instance `inst`, tile `tile` (row tile % tiles_z, column tile / tiles_z).
 struct Work {
@@ -47,12 +56,13 @@ cudaError_t launch_stress(const HalfArgs &a, int variant, bool exact, cudaStream
 // Batched: one launch over all instances' tiles. `inst` (device) holds each
 // instance's arguments (z_base set), `work` (device) the CTA -> (instance, tile)
 // table; `step` (device) is the shared step counter.
+// `square`: every instance has square (folded) coefficients (set_square).
 cudaError_t launch_velocity_batch(const HalfArgs *inst, const Work *work, int nwork, const int *step, int variant,
-                                  bool exact, cudaStream_t st);
+                                  bool exact, bool square, cudaStream_t st);
 cudaError_t launch_stress_batch(const HalfArgs *inst, const Work *work, int nwork, const int *step, int variant,
-                                bool exact, cudaStream_t st);
+                                bool exact, bool square, cudaStream_t st);
 // Sets the kernels' shared-memory attributes (call before a stream capture).
-cudaError_t prepare_batch(int variant, bool exact);
+cudaError_t prepare_batch(int variant, bool exact, bool square);
 
 // Device side of the TMA halo tiles, shared by the tiled forward and adjoint kernels.
 namespace tma {

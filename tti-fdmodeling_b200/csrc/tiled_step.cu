@@ -48,7 +48,15 @@ __device__ __forceinline__ bool tile_undamped(const HalfArgs &a, const Cells &c)
 }
 
 // Velocity update of tile (tz, tx); `map` holds the tensor maps of sxx, szz, sxz.
-template <int V, bool X>
+// Q (FMA mode, dx == dz): the coefficients carry h = 0.5 / dx, so a derivative
+// is d1 + d2 or d1 - d2 without a product.
+template <bool Q>
+__device__ __forceinline__ float coef(const HalfArgs &a, int k)
+{
+  return Q ? a.hc[k] : rsg(k);
+}
+
+template <int V, bool X, bool Q>
 __device__ __forceinline__ void velocity_tile(const HalfArgs &a, const CUtensorMap *map, float *sm, int tz, int tx)
 {
   using A = Ar<X>;
@@ -83,27 +91,32 @@ __device__ __forceinline__ void velocity_tile(const HalfArgs &a, const CUtensorM
     for (int f = 0; f < 3; ++f) {
       const float *q = s + f * FIELD;
       // d1 = sum C_k (s[x+k][z+k] - s[x-k+1][z-k+1]); d2 = sum C_k (s[x+k][z-k+1] - s[x-k+1][z+k])
-      float s1 = A::mul(rsg(0), A::sub(q[BZ + 1], q[0]));
-      float s2 = A::mul(rsg(0), A::sub(q[BZ], q[1]));
+      float s1 = A::mul(coef<Q>(a, 0), A::sub(q[BZ + 1], q[0]));
+      float s2 = A::mul(coef<Q>(a, 0), A::sub(q[BZ], q[1]));
 #pragma unroll
       for (int k = 2; k <= NH; ++k) {
-        s1 = A::add(s1, A::mul(rsg(k - 1), A::sub(q[k * BZ + k], q[(1 - k) * BZ + 1 - k])));
-        s2 = A::add(s2, A::mul(rsg(k - 1), A::sub(q[k * BZ + 1 - k], q[(1 - k) * BZ + k])));
+        s1 = A::add(s1, A::mul(coef<Q>(a, k - 1), A::sub(q[k * BZ + k], q[(1 - k) * BZ + 1 - k])));
+        s2 = A::add(s2, A::mul(coef<Q>(a, k - 1), A::sub(q[k * BZ + 1 - k], q[(1 - k) * BZ + k])));
       }
       d[f][0] = s1;
       d[f][1] = s2;
     }
-    const float sxx_x = A::mul(A::mul(0.5f, A::add(d[0][0], d[0][1])), invdx);
-    const float szz_z = A::mul(A::mul(0.5f, A::sub(d[1][0], d[1][1])), invdz);
-    const float sxz_x = A::mul(A::mul(0.5f, A::add(d[2][0], d[2][1])), invdx);
-    const float sxz_z = A::mul(A::mul(0.5f, A::sub(d[2][0], d[2][1])), invdz);
+    // x and z derivatives 0.5 (d1 +- d2) / dx, / dz (already scaled when Q)
+    auto dx_ = [&](int f) { return Q ? d[f][0] + d[f][1] : A::mul(A::mul(0.5f, A::add(d[f][0], d[f][1])), invdx); };
+    auto dz_ = [&](int f, float inv) {
+      return Q ? d[f][0] - d[f][1] : A::mul(A::mul(0.5f, A::sub(d[f][0], d[f][1])), inv);
+    };
+    const float sxx_x = dx_(0);
+    const float szz_z = dz_(1, invdz);
+    const float sxz_x = dx_(2);
+    const float sxz_z = dz_(2, invdz);
     const float br = A::mul(c2, ir);
     float fx, fz;
     if (V == TTI_COORDINATE) {
       const float2 sc = __ldg(a.pk.vsc + gi);
       const float sv = sc.x, cv = sc.y;
-      const float sxx_z = A::mul(A::mul(0.5f, A::sub(d[0][0], d[0][1])), invdx);  // invdx as coord:633
-      const float szz_x = A::mul(A::mul(0.5f, A::add(d[1][0], d[1][1])), invdx);
+      const float sxx_z = dz_(0, invdx);  // invdx as coord:633
+      const float szz_x = dx_(1);
       fx = A::add(A::add(A::sub(A::mul(cv, sxx_x), A::mul(sv, sxx_z)), A::mul(sv, sxz_x)), A::mul(cv, sxz_z));
       fz = A::add(A::add(A::sub(A::mul(cv, sxz_x), A::mul(sv, sxz_z)), A::mul(sv, szz_x)), A::mul(cv, szz_z));
     } else {
@@ -193,7 +206,7 @@ __device__ __forceinline__ void stress_store(const HalfArgs &a, size_t gi, float
 }
 
 // Stress update of tile (tz, tx); `map` holds the tensor maps of vx, vz.
-template <int V, bool X>
+template <int V, bool X, bool Q>
 __device__ __forceinline__ void stress_tile(const HalfArgs &a, const CUtensorMap *map, float *sm, int tz, int tx)
 {
   using A = Ar<X>;
@@ -221,20 +234,20 @@ __device__ __forceinline__ void stress_tile(const HalfArgs &a, const CUtensorMap
     for (int f = 0; f < 2; ++f) {
       const float *q = s + f * FIELD;
       // d1 = sum C_k (v[x+k-1][z+k-1] - v[x-k][z-k]); d2 = sum C_k (v[x+k-1][z-k] - v[x-k][z+k-1])
-      float s1 = A::mul(rsg(0), A::sub(q[0], q[-BZ - 1]));
-      float s2 = A::mul(rsg(0), A::sub(q[-1], q[-BZ]));
+      float s1 = A::mul(coef<Q>(a, 0), A::sub(q[0], q[-BZ - 1]));
+      float s2 = A::mul(coef<Q>(a, 0), A::sub(q[-1], q[-BZ]));
 #pragma unroll
       for (int k = 2; k <= NH; ++k) {
-        s1 = A::add(s1, A::mul(rsg(k - 1), A::sub(q[(k - 1) * BZ + k - 1], q[-k * BZ - k])));
-        s2 = A::add(s2, A::mul(rsg(k - 1), A::sub(q[(k - 1) * BZ - k], q[-k * BZ + k - 1])));
+        s1 = A::add(s1, A::mul(coef<Q>(a, k - 1), A::sub(q[(k - 1) * BZ + k - 1], q[-k * BZ - k])));
+        s2 = A::add(s2, A::mul(coef<Q>(a, k - 1), A::sub(q[(k - 1) * BZ - k], q[-k * BZ + k - 1])));
       }
       d[f][0] = s1;
       d[f][1] = s2;
     }
-    const float vxx = A::mul(A::mul(0.5f, A::add(d[0][0], d[0][1])), invdx);
-    const float vxz = A::mul(A::mul(0.5f, A::sub(d[0][0], d[0][1])), invdz);
-    const float vzx = A::mul(A::mul(0.5f, A::add(d[1][0], d[1][1])), invdx);
-    const float vzz = A::mul(A::mul(0.5f, A::sub(d[1][0], d[1][1])), invdz);
+    const float vxx = Q ? d[0][0] + d[0][1] : A::mul(A::mul(0.5f, A::add(d[0][0], d[0][1])), invdx);
+    const float vxz = Q ? d[0][0] - d[0][1] : A::mul(A::mul(0.5f, A::sub(d[0][0], d[0][1])), invdz);
+    const float vzx = Q ? d[1][0] + d[1][1] : A::mul(A::mul(0.5f, A::add(d[1][0], d[1][1])), invdx);
+    const float vzz = Q ? d[1][0] - d[1][1] : A::mul(A::mul(0.5f, A::sub(d[1][0], d[1][1])), invdz);
     stress_store<V, X>(a, gi, vxx, vxz, vzx, vzz, p);
   }
 }
@@ -257,21 +270,21 @@ __device__ __forceinline__ const HalfArgs *stage_args(const HalfArgs *src, float
   return dst;
 }
 
-template <int V, bool X>
+template <int V, bool X, bool Q>
 __global__ void __launch_bounds__(NT, 4) k_velocity_tiled(const __grid_constant__ HalfArgs a)
 {
   extern __shared__ __align__(128) float sm[];
-  velocity_tile<V, X>(a, a.map, sm, blockIdx.x, blockIdx.y);
+  velocity_tile<V, X, Q>(a, a.map, sm, blockIdx.x, blockIdx.y);
 }
 
-template <int V, bool X>
+template <int V, bool X, bool Q>
 __global__ void __launch_bounds__(NT, 4) k_stress_tiled(const __grid_constant__ HalfArgs a)
 {
   extern __shared__ __align__(128) float sm[];
-  stress_tile<V, X>(a, a.map, sm, blockIdx.x, blockIdx.y);
+  stress_tile<V, X, Q>(a, a.map, sm, blockIdx.x, blockIdx.y);
 }
 
-template <int V, bool X>
+template <int V, bool X, bool Q>
 __global__ void __launch_bounds__(NT, 4) k_velocity_batch(const HalfArgs *__restrict__ inst,
                                                           const Work *__restrict__ work, const int *step)
 {
@@ -280,10 +293,10 @@ __global__ void __launch_bounds__(NT, 4) k_velocity_batch(const HalfArgs *__rest
   const HalfArgs *src = inst + w.inst;
   if (*step >= src->nt) return;
   const HalfArgs *a = stage_args(src, sm);
-  velocity_tile<V, X>(*a, src->map, sm, w.tile % a->tiles_z, w.tile / a->tiles_z);
+  velocity_tile<V, X, Q>(*a, src->map, sm, w.tile % a->tiles_z, w.tile / a->tiles_z);
 }
 
-template <int V, bool X>
+template <int V, bool X, bool Q>
 __global__ void __launch_bounds__(NT, 4) k_stress_batch(const HalfArgs *__restrict__ inst,
                                                         const Work *__restrict__ work, const int *step)
 {
@@ -292,7 +305,7 @@ __global__ void __launch_bounds__(NT, 4) k_stress_batch(const HalfArgs *__restri
   const HalfArgs *src = inst + w.inst;
   if (*step >= src->nt) return;
   const HalfArgs *a = stage_args(src, sm);
-  stress_tile<V, X>(*a, src->map, sm, w.tile % a->tiles_z, w.tile / a->tiles_z);
+  stress_tile<V, X, Q>(*a, src->map, sm, w.tile % a->tiles_z, w.tile / a->tiles_z);
 }
 
 template <typename K>
@@ -360,28 +373,32 @@ bool encode_map(CUtensorMap *map, const Grid &g, float *field)
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+template <bool X, bool Q>
+cudaError_t velocity_xq(const HalfArgs &a, int variant, cudaStream_t st)
+{
+  if (variant == TTI_COORDINATE) return launch_k(k_velocity_tiled<TTI_COORDINATE, X, Q>, a, 3, st);
+  if (variant == TTI_TENSOR) return launch_k(k_velocity_tiled<TTI_TENSOR, X, Q>, a, 3, st);
+  return launch_k(k_velocity_tiled<TTI_BOND, X, Q>, a, 3, st);
+}
+
+template <bool X, bool Q>
+cudaError_t stress_xq(const HalfArgs &a, int variant, cudaStream_t st)
+{
+  if (variant == TTI_COORDINATE) return launch_k(k_stress_tiled<TTI_COORDINATE, X, Q>, a, 2, st);
+  if (variant == TTI_TENSOR) return launch_k(k_stress_tiled<TTI_TENSOR, X, Q>, a, 2, st);
+  return launch_k(k_stress_tiled<TTI_BOND, X, Q>, a, 2, st);
+}
+
 cudaError_t launch_velocity(const HalfArgs &a, int variant, bool exact, cudaStream_t st)
 {
-  if (exact) {
-    if (variant == TTI_COORDINATE) return launch_k(k_velocity_tiled<TTI_COORDINATE, true>, a, 3, st);
-    if (variant == TTI_TENSOR) return launch_k(k_velocity_tiled<TTI_TENSOR, true>, a, 3, st);
-    return launch_k(k_velocity_tiled<TTI_BOND, true>, a, 3, st);
-  }
-  if (variant == TTI_COORDINATE) return launch_k(k_velocity_tiled<TTI_COORDINATE, false>, a, 3, st);
-  if (variant == TTI_TENSOR) return launch_k(k_velocity_tiled<TTI_TENSOR, false>, a, 3, st);
-  return launch_k(k_velocity_tiled<TTI_BOND, false>, a, 3, st);
+  if (exact) return velocity_xq<true, false>(a, variant, st);
+  return a.square ? velocity_xq<false, true>(a, variant, st) : velocity_xq<false, false>(a, variant, st);
 }
 
 cudaError_t launch_stress(const HalfArgs &a, int variant, bool exact, cudaStream_t st)
 {
-  if (exact) {
-    if (variant == TTI_COORDINATE) return launch_k(k_stress_tiled<TTI_COORDINATE, true>, a, 2, st);
-    if (variant == TTI_TENSOR) return launch_k(k_stress_tiled<TTI_TENSOR, true>, a, 2, st);
-    return launch_k(k_stress_tiled<TTI_BOND, true>, a, 2, st);
-  }
-  if (variant == TTI_COORDINATE) return launch_k(k_stress_tiled<TTI_COORDINATE, false>, a, 2, st);
-  if (variant == TTI_TENSOR) return launch_k(k_stress_tiled<TTI_TENSOR, false>, a, 2, st);
-  return launch_k(k_stress_tiled<TTI_BOND, false>, a, 2, st);
+  if (exact) return stress_xq<true, false>(a, variant, st);
+  return a.square ? stress_xq<false, true>(a, variant, st) : stress_xq<false, false>(a, variant, st);
 }
 
 constexpr size_t BATCH_SMEM = (size_t)ARGS_OFF * sizeof(float) + ARGS_BYTES;
@@ -396,43 +413,47 @@ cudaError_t launch_batch_k(K kernel, const HalfArgs *inst, const Work *work, int
   return cudaGetLastError();
 }
 
-template <bool X>
+template <bool X, bool Q>
 cudaError_t velocity_batch_x(const HalfArgs *inst, const Work *work, int nwork, const int *step, int variant,
                              cudaStream_t st)
 {
-  if (variant == TTI_COORDINATE) return launch_batch_k(k_velocity_batch<TTI_COORDINATE, X>, inst, work, nwork, step, st);
-  if (variant == TTI_TENSOR) return launch_batch_k(k_velocity_batch<TTI_TENSOR, X>, inst, work, nwork, step, st);
-  return launch_batch_k(k_velocity_batch<TTI_BOND, X>, inst, work, nwork, step, st);
+  if (variant == TTI_COORDINATE)
+    return launch_batch_k(k_velocity_batch<TTI_COORDINATE, X, Q>, inst, work, nwork, step, st);
+  if (variant == TTI_TENSOR) return launch_batch_k(k_velocity_batch<TTI_TENSOR, X, Q>, inst, work, nwork, step, st);
+  return launch_batch_k(k_velocity_batch<TTI_BOND, X, Q>, inst, work, nwork, step, st);
 }
 
-template <bool X>
+template <bool X, bool Q>
 cudaError_t stress_batch_x(const HalfArgs *inst, const Work *work, int nwork, const int *step, int variant,
                            cudaStream_t st)
 {
-  if (variant == TTI_COORDINATE) return launch_batch_k(k_stress_batch<TTI_COORDINATE, X>, inst, work, nwork, step, st);
-  if (variant == TTI_TENSOR) return launch_batch_k(k_stress_batch<TTI_TENSOR, X>, inst, work, nwork, step, st);
-  return launch_batch_k(k_stress_batch<TTI_BOND, X>, inst, work, nwork, step, st);
+  if (variant == TTI_COORDINATE)
+    return launch_batch_k(k_stress_batch<TTI_COORDINATE, X, Q>, inst, work, nwork, step, st);
+  if (variant == TTI_TENSOR) return launch_batch_k(k_stress_batch<TTI_TENSOR, X, Q>, inst, work, nwork, step, st);
+  return launch_batch_k(k_stress_batch<TTI_BOND, X, Q>, inst, work, nwork, step, st);
 }
 
 cudaError_t launch_velocity_batch(const HalfArgs *inst, const Work *work, int nwork, const int *step, int variant,
-                                  bool exact, cudaStream_t st)
+                                  bool exact, bool square, cudaStream_t st)
 {
-  return exact ? velocity_batch_x<true>(inst, work, nwork, step, variant, st)
-               : velocity_batch_x<false>(inst, work, nwork, step, variant, st);
+  if (exact) return velocity_batch_x<true, false>(inst, work, nwork, step, variant, st);
+  return square ? velocity_batch_x<false, true>(inst, work, nwork, step, variant, st)
+                : velocity_batch_x<false, false>(inst, work, nwork, step, variant, st);
 }
 
 cudaError_t launch_stress_batch(const HalfArgs *inst, const Work *work, int nwork, const int *step, int variant,
-                                bool exact, cudaStream_t st)
+                                bool exact, bool square, cudaStream_t st)
 {
-  return exact ? stress_batch_x<true>(inst, work, nwork, step, variant, st)
-               : stress_batch_x<false>(inst, work, nwork, step, variant, st);
+  if (exact) return stress_batch_x<true, false>(inst, work, nwork, step, variant, st);
+  return square ? stress_batch_x<false, true>(inst, work, nwork, step, variant, st)
+                : stress_batch_x<false, false>(inst, work, nwork, step, variant, st);
 }
 
-cudaError_t prepare_batch(int variant, bool exact)
+cudaError_t prepare_batch(int variant, bool exact, bool square)
 {
   // a launch over zero CTAs only sets the attributes
-  cudaError_t e = launch_velocity_batch(nullptr, nullptr, 0, nullptr, variant, exact, nullptr);
-  if (e == cudaSuccess) e = launch_stress_batch(nullptr, nullptr, 0, nullptr, variant, exact, nullptr);
+  cudaError_t e = launch_velocity_batch(nullptr, nullptr, 0, nullptr, variant, exact, square, nullptr);
+  if (e == cudaSuccess) e = launch_stress_batch(nullptr, nullptr, 0, nullptr, variant, exact, square, nullptr);
   return e;
 }
 
