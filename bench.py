@@ -309,6 +309,46 @@ def run_batched(args, local_rank):
             "clocks": clk.summary()}
 
 
+def run_batched_uneven(args, local_rank):
+    """Many independent models of different sizes in one batch (one launch per
+    half-step over all of them): `uneven_models` layered models with seeded
+    nz in [256, 1126], nx in [256, 4096], nt in [1000, 4000] (seed 4), one
+    centred surface shot each, ealThick=40, receivers on every column at z=2.
+    `batch_steps` steps are timed (instances whose nt is reached stay idle)."""
+    import ttifd
+
+    rng = np.random.default_rng(4)
+    M, K, W = args.uneven_models, args.batch_steps, args.warmup
+    sizes = [(int(rng.integers(256, 1127)), int(rng.integers(256, 4097)), int(rng.integers(1000, 4001)))
+             for _ in range(M)]
+    cfgs = [dict(variant=args.variant, nz=nz, nx=nx, nt=nt, dx=10.0, dz=10.0, dt=0.0008, fpeak=15.0, ealThick=40,
+                 freesurface=0, stype=1, seistype=1, mt=1) for nz, nx, nt in sizes]
+    with ttifd.Batch(cfgs, list(range(M)), device=local_rank) as b:
+        cells = []
+        for m, (nz, nx, nt) in enumerate(sizes):
+            mod = synthetic.layered_model(nz, nx, seed=100 + m)
+            b.upload_model(m, *synthetic.padded(mod, 40))
+            inst = b.instances[m]
+            inst.set_source([nx // 2], [2], synthetic.ricker(nt, 0.0008, 15.0)[None, :])
+            for k in (0, 1):
+                inst.set_receivers(k, np.arange(nx, dtype=np.int32), 2)
+            cells.append(inst.Nz * inst.Nx)
+        tuned = b.autotune(10)
+        b.reset()
+        b.step(W)
+        with ClockSampler(local_rank) as clk:
+            b.step(K)
+            ms = b.elapsed_ms
+    total = sum(cells)
+    per = [c * K / (ms / 1e3) / 1e9 for c in cells]
+    return {"workload": f"batched forward, {args.variant}, {M} independent layered models of seeded sizes "
+                        "nz 256-1126, nx 256-4096, nt 1000-4000, one centred shot each, ealThick=40",
+            "models": M, "steps": K, "cells_total": total, "value": total * K / (ms / 1e3) / 1e9, "unit": "Gcell/s",
+            "ms_per_step": ms / K, "per_instance_gcells": {"min": min(per), "median": float(np.median(per)),
+                                                            "max": max(per)},
+            "schedule": tuned, "clocks": clk.summary()}
+
+
 # ---------------------------------------------------------------- gradient arm
 GRAD_WORKLOAD = dict(nz=600, nx=1200, dx=10.0, dz=10.0, dt=0.0008, fpeak=12.0, ealThick=40, freesurface=0, stype=1,
                      seistype=1, mt=1, wsave=0, savew=0, mode=1, scalar=1.0, energy=0)
@@ -457,6 +497,7 @@ def main():
     ap.add_argument("--batch-shots", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=200)
     ap.add_argument("--no-batch", action="store_true", help="skip the batched measurement")
+    ap.add_argument("--uneven-models", type=int, default=48)
     ap.add_argument("--grad-steps", type=int, default=3000)
     ap.add_argument("--grad-ncheck", type=int, default=1,
                     help="gradient segments (1: every state kept, as the 600x1200 case fits in HBM)")
@@ -487,6 +528,7 @@ def main():
     line = run_ours(args, rank, world, local_rank)
     if not args.no_batch and world == 1:
         line["batched"] = run_batched(args, local_rank)
+        line["batched_uneven"] = run_batched_uneven(args, local_rank)
     if not args.no_grad and world == 1:
         line["gradient"] = run_gradient(args, local_rank)
     if rank == 0:
