@@ -425,7 +425,7 @@ cudaError_t launch_adj_tile(K kernel, const AdjTile &at, int nfields, int z_firs
     }
   }
   AdjTile b = at;
-  b.z_base = z_first & ~3;
+  b.z_base = z_first & ~31;  // 32-row aligned: a warp's rows are one 128-byte line
   const int nz = g.Nz - NH - b.z_base, nx = g.Nx - 2 * NH;
   if (nz <= 0 || nx <= 0) return cudaSuccess;
   kernel<<<dim3((nz + tiled::TZ - 1) / tiled::TZ, (nx + tiled::TX - 1) / tiled::TX), tiled::NT, bytes, st>>>(b);

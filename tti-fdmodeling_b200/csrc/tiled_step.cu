@@ -15,6 +15,7 @@
 // from the tiles, so in-place updates are race-free.
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "tiled.cuh"
@@ -39,6 +40,7 @@ __device__ __forceinline__ Cells cells_of(const HalfArgs &a, int tz, int tx)
   return c;
 }
 
+// true when every cell of the tile lies where coef1 = 1 and coef2 = dt
 // true when every cell of the tile lies where coef1 = 1 and coef2 = dt
 __device__ __forceinline__ bool tile_undamped(const HalfArgs &a, const Cells &c)
 {
@@ -347,7 +349,9 @@ cudaError_t launch_k(K kernel, const HalfArgs &a, int nfields, cudaStream_t st)
 
 dim3 grid(const Grid &g, int *z_base)
 {
-  *z_base = g.izStart & ~3;
+  // izStart rounded down to 32 rows, so that a warp's 32 consecutive rows are
+  // one 128-byte line of every per-cell array
+  *z_base = g.izStart & ~31;
   const int nz = g.Nz - NH - *z_base, nx = g.Nx - 2 * NH;
   if (nz <= 0 || nx <= 0) return dim3(0, 0);
   return dim3((nz + TZ - 1) / TZ, (nx + TX - 1) / TX);
