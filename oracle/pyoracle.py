@@ -155,6 +155,7 @@ _ADJ_SIG = {
                                 C.c_int, C.c_int, C.c_double]),
     "adj_destroy": (None, [C.c_void_p]),
     "adj_grid": (None, [C.c_void_p, _IP, _IP, _IP]),
+    "adj_set_formulation": (None, [C.c_void_p, C.c_int]),
     "adj_set_meal": (None, [C.c_void_p, _FP, _FP, _FP]),
     "adj_set_model": (None, [C.c_void_p] + [_DP] * 6),
     "adj_set_source": (None, [C.c_void_p, C.c_int, _IP, _IP, _DP]),
@@ -170,7 +171,8 @@ def _d(a):
 
 class AdjointOracle:
     """Double-precision forward and adjoint-state gradient of the coordinate
-    formulation (oracle/ttifd_adjoint.c), stress source only. MEAL coef1, coef2
+    formulation, or of the Bond formulation without free surface
+    (cfg variant "bond_transformation"; oracle/ttifd_adjoint.c), stress source only. MEAL coef1, coef2
     and Beta are frozen from the float setup of `meal_model` (padded arrays);
     vs and rho stay fixed; the model (vp, eps, delta, theta) can be changed
     with set_model for finite differences."""
@@ -185,6 +187,10 @@ class AdjointOracle:
         c = self.cfg
         self._c = lib.adj_create(c["nz"], c["nx"], c["nt"], c["dx"], c["dz"], c["dt"], c["ealThick"],
                                  c.get("freesurface", 0), c.get("mt", 1), c["seistype"], c.get("scalar", 1.0))
+        bond = c.get("variant") in ("bond_transformation", 2)
+        if bond and c.get("freesurface", 0):
+            raise ValueError("the Bond gradient reference has no free surface")
+        lib.adj_set_formulation(self._c, int(bond))
         nz, nx, nts = C.c_int(), C.c_int(), C.c_int()
         lib.adj_grid(self._c, C.byref(nz), C.byref(nx), C.byref(nts))
         self.Nz, self.Nx, self.nts = nz.value, nx.value, nts.value

@@ -8,7 +8,10 @@
  * (src/main/sufdmod2dTTIelastic/sufdmod2dTTIelastic_coordinate_rotation.c:
  * velocity update :614-672, stress update :804-845, free surface :847-863,
  * stress source :865-886, receivers isoelastic.c:103-144) and of its
- * stiffness build (:497-537), so that
+ * stiffness build (:497-537), and the same for the Bond-transformation
+ * formulation (sufdmod2dTTIelastic_bond_transformation.c: velocity update
+ * :654-703, stress update :836-873, stiffness :492-541; without the free
+ * surface, whose stiffness rewrite :543-568 is not differentiated), so that
  *   J = 1/2 sum over recorded samples (d - dobs)^2
  * has gradients with respect to vp, epsilon, delta and theta (degrees) at
  * every padded cell. Conventions: vs and rho are held fixed; the MEAL arrays
@@ -36,6 +39,8 @@ struct adj_ctx {
   /* model and derived arrays */
   double *vp, *vs, *rho, *eps, *delta, *theta;  /* as given (padded) */
   double *c11, *c13, *c33, *c55, *sn, *cs, *snv, *csv, *ir;
+  int bond;             /* Bond transformation instead of coordinate rotation */
+  double *c15, *c35;    /* Bond only */
   /* geometry */
   int nsrc, *sx, *sz;
   double *src; /* [nsrc][nt] */
@@ -66,8 +71,8 @@ adj_ctx *adj_create(int nz, int nx, int nt, double dx, double dz, double dt, int
   c->dt = dt;
   c->scalar = scalar;
   c->Np = (size_t)c->Nz * c->Nx;
-  double **arrs[] = {&c->coef1, &c->coef2, &c->beta, &c->vp, &c->vs, &c->rho, &c->eps, &c->delta, &c->theta,
-                     &c->c11,   &c->c13,   &c->c33,  &c->c55, &c->sn, &c->cs,  &c->snv, &c->csv,   &c->ir};
+  double **arrs[] = {&c->coef1, &c->coef2, &c->beta, &c->vp,  &c->vs,  &c->rho, &c->eps, &c->delta, &c->theta, &c->c11,
+                     &c->c13,   &c->c33,   &c->c55,  &c->sn,  &c->cs,  &c->snv, &c->csv, &c->ir,    &c->c15,   &c->c35};
   for (size_t k = 0; k < sizeof arrs / sizeof arrs[0]; ++k) *arrs[k] = dalloc(c->Np);
   return c;
 }
@@ -75,8 +80,8 @@ adj_ctx *adj_create(int nz, int nx, int nt, double dx, double dz, double dt, int
 void adj_destroy(adj_ctx *c)
 {
   if (!c) return;
-  double *arrs[] = {c->coef1, c->coef2, c->beta, c->vp, c->vs,  c->rho, c->eps, c->delta, c->theta,
-                    c->c11,   c->c13,   c->c33,  c->c55, c->sn, c->cs,  c->snv, c->csv,   c->ir};
+  double *arrs[] = {c->coef1, c->coef2, c->beta, c->vp,  c->vs,  c->rho, c->eps, c->delta, c->theta, c->c11,
+                    c->c13,   c->c33,   c->c55,  c->sn,  c->cs,  c->snv, c->csv, c->ir,    c->c15,   c->c35};
   for (size_t k = 0; k < sizeof arrs / sizeof arrs[0]; ++k) free(arrs[k]);
   free(c->sx);
   free(c->sz);
@@ -93,6 +98,47 @@ void adj_grid(const adj_ctx *c, int *Nz, int *Nx, int *nts)
   *Nz = c->Nz;
   *Nx = c->Nx;
   *nts = c->nts;
+}
+
+void adj_set_formulation(adj_ctx *c, int bond) { c->bond = bond; }
+
+/* Bond rotation of the VTI moduli (bond:492-541): c11 c13 c15 c33 c35 c55 */
+static void bond_moduli(double C11, double C13, double C33, double C55, double th, double out[6])
+{
+  const double s2 = sin(th) * sin(th), c2 = cos(th) * cos(th), s4 = s2 * s2, c4 = c2 * c2;
+  const double s2t = sin(2.0 * th), c2t = cos(2.0 * th), s22 = s2t * s2t, c22 = c2t * c2t;
+  out[0] = C11 * c4 + C33 * s4 + (0.5 * C13 + C55) * s22;
+  out[1] = (0.25 * (C11 + C33) - C55) * s22 + C13 * (s4 + c4);
+  out[2] = 0.5 * (-C11 * c2 + C33 * s2 + (C13 + 2.0 * C55) * c2t) * s2t;
+  out[3] = C11 * s4 + C33 * c4 + (0.5 * C13 + C55) * s22;
+  out[4] = 0.5 * (-C11 * s2 + C33 * c2 - (C13 + 2.0 * C55) * c2t) * s2t;
+  out[5] = 0.25 * (C11 + C33 - 2.0 * C13) * s22 + C55 * c22;
+}
+
+/* derivatives of bond_moduli: d[m][0..5] = d(c11..c55)/d(C11, C13, C33, theta)[m] */
+static void bond_moduli_grad(double C11, double C13, double C33, double C55, double th, double d[4][6])
+{
+  const double s2 = sin(th) * sin(th), c2 = cos(th) * cos(th), s4 = s2 * s2, c4 = c2 * c2;
+  const double s2t = sin(2.0 * th), c2t = cos(2.0 * th), s22 = s2t * s2t;
+  const double ds2 = s2t, dc2 = -s2t, ds4 = 2.0 * s2 * s2t, dc4 = -2.0 * c2 * s2t;
+  const double ds2t = 2.0 * c2t, dc2t = -2.0 * s2t, ds22 = 4.0 * s2t * c2t, dc22 = -ds22;
+  const double d11[6] = {c4, 0.25 * s22, -0.5 * c2 * s2t, s4, -0.5 * s2 * s2t, 0.25 * s22};
+  const double d13[6] = {0.5 * s22, s4 + c4, 0.5 * c2t * s2t, 0.5 * s22, -0.5 * c2t * s2t, -0.5 * s22};
+  const double d33[6] = {s4, 0.25 * s22, 0.5 * s2 * s2t, c4, 0.5 * c2 * s2t, 0.25 * s22};
+  const double A = C13 + 2.0 * C55;
+  const double dth[6] = {
+      C11 * dc4 + C33 * ds4 + (0.5 * C13 + C55) * ds22,
+      (0.25 * (C11 + C33) - C55) * ds22 + C13 * (ds4 + dc4),
+      0.5 * ((-C11 * dc2 + C33 * ds2 + A * dc2t) * s2t + (-C11 * c2 + C33 * s2 + A * c2t) * ds2t),
+      C11 * ds4 + C33 * dc4 + (0.5 * C13 + C55) * ds22,
+      0.5 * ((-C11 * ds2 + C33 * dc2 - A * dc2t) * s2t + (-C11 * s2 + C33 * c2 - A * c2t) * ds2t),
+      0.25 * (C11 + C33 - 2.0 * C13) * ds22 + C55 * dc22};
+  for (int k = 0; k < 6; ++k) {
+    d[0][k] = d11[k];
+    d[1][k] = d13[k];
+    d[2][k] = d33[k];
+    d[3][k] = dth[k];
+  }
 }
 
 void adj_set_meal(adj_ctx *c, const float *coef1, const float *coef2, const float *beta)
@@ -124,6 +170,16 @@ void adj_set_model(adj_ctx *c, const double *vp, const double *vs, const double 
     c->c33[i] = r * p * p;
     c->c55[i] = r * s * s;
     const double th = c->scalar * theta[i] / 180.0 * M_PI;
+    if (c->bond) {
+      double m[6];
+      bond_moduli(c->c11[i], c->c13[i], c->c33[i], c->c55[i], th, m);
+      c->c11[i] = m[0];
+      c->c13[i] = m[1];
+      c->c15[i] = m[2];
+      c->c33[i] = m[3];
+      c->c35[i] = m[4];
+      c->c55[i] = m[5];
+    }
     c->sn[i] = sin(th);
     c->cs[i] = cos(th);
   }
@@ -221,8 +277,13 @@ static void velocity_half(const adj_ctx *c, state *u)
       const double sxz_x = hx * (e1 + e2), sxz_z = hz * (e1 - e2);
       const size_t i = (size_t)ix * c->Nz + iz;
       const double cv = c->csv[i], sv = c->snv[i], br = c->coef2[i] * c->ir[i];
-      u->vx[i] = c->coef1[i] * u->vx[i] + br * (cv * sxx_x - sv * sxx_z + sv * sxz_x + cv * sxz_z);
-      u->vz[i] = c->coef1[i] * u->vz[i] + br * (cv * sxz_x - sv * sxz_z + sv * szz_x + cv * szz_z);
+      if (c->bond) {
+        u->vx[i] = c->coef1[i] * u->vx[i] + br * (sxx_x + sxz_z);
+        u->vz[i] = c->coef1[i] * u->vz[i] + br * (sxz_x + szz_z);
+      } else {
+        u->vx[i] = c->coef1[i] * u->vx[i] + br * (cv * sxx_x - sv * sxx_z + sv * sxz_x + cv * sxz_z);
+        u->vz[i] = c->coef1[i] * u->vz[i] + br * (cv * sxz_x - sv * sxz_z + sv * szz_x + cv * szz_z);
+      }
     }
 }
 
@@ -236,10 +297,17 @@ static void stress_half(const adj_ctx *c, state *u)
       ds(c, u->vz, ix, iz, &b1, &b2);
       double vxx = hx * (a1 + a2), vxz = hz * (a1 - a2), vzx = hx * (b1 + b2), vzz = hz * (b1 - b2);
       const size_t i = (size_t)ix * c->Nz + iz;
+      const double a = c->coef1[i], b = c->coef2[i];
+      if (c->bond) {
+        const double sh = vzx + vxz;
+        u->sxx[i] = a * u->sxx[i] + b * (c->c11[i] * vxx + c->c13[i] * vzz + c->c15[i] * sh);
+        u->szz[i] = a * u->szz[i] + b * (c->c13[i] * vxx + c->c33[i] * vzz + c->c35[i] * sh);
+        u->sxz[i] = a * u->sxz[i] + b * (c->c15[i] * vxx + c->c35[i] * vzz + c->c55[i] * sh);
+        continue;
+      }
       const double s = c->sn[i], co = c->cs[i];
       const double rxx = co * vxx - s * vxz, rxz = s * vxx + co * vxz;
       const double rzx = co * vzx - s * vzz, rzz = s * vzx + co * vzz;
-      const double a = c->coef1[i], b = c->coef2[i];
       u->sxx[i] = a * u->sxx[i] + b * (c->c11[i] * rxx + c->c13[i] * rzz);
       u->szz[i] = a * u->szz[i] + b * (c->c13[i] * rxx + c->c33[i] * rzz);
       u->sxz[i] = a * u->sxz[i] + b * c->c55[i] * (rzx + rxz);
@@ -370,7 +438,7 @@ double adj_gradient(adj_ctx *c, const double *dobs[3], double *g_vp, double *g_e
   double *T[6];
   for (int k = 0; k < 6; ++k) T[k] = dalloc(Np);
   double *gc11 = dalloc(Np), *gc13 = dalloc(Np), *gc33 = dalloc(Np), *gc55 = dalloc(Np), *gth = dalloc(Np);
-  double *gsv = dalloc(Np), *gcv = dalloc(Np);
+  double *gsv = dalloc(Np), *gcv = dalloc(Np), *gc15 = dalloc(Np), *gc35 = dalloc(Np);
   if (g_src) memset(g_src, 0, sizeof(double) * (size_t)c->nsrc * c->nt);
   for (int it = c->nt - 1; it >= 0; --it) {
     const state *f = &keep[it];
@@ -428,10 +496,30 @@ double adj_gradient(adj_ctx *c, const double *dobs[3], double *g_vp, double *g_e
         ds(c, f->vx, ix, iz, &a1, &a2);
         ds(c, f->vz, ix, iz, &b1, &b2);
         const double vxx = hx * (a1 + a2), vxz = hz * (a1 - a2), vzx = hx * (b1 + b2), vzz = hz * (b1 - b2);
+        const double la = L.sxx[i], lb = L.szz[i], le = L.sxz[i], b = c->coef2[i];
+        if (c->bond) {  /* sigma = H (vxx, vzz, vzx + vxz), H symmetric with c15, c35 */
+          const double sh = vzx + vxz;
+          gc11[i] += b * la * vxx;
+          gc13[i] += b * (la * vzz + lb * vxx);
+          gc15[i] += b * (la * sh + le * vxx);
+          gc33[i] += b * lb * vzz;
+          gc35[i] += b * (lb * sh + le * vzz);
+          gc55[i] += b * le * sh;
+          const double Lxx = b * (c->c11[i] * la + c->c13[i] * lb + c->c15[i] * le);
+          const double Lzz = b * (c->c13[i] * la + c->c33[i] * lb + c->c35[i] * le);
+          const double Lsh = b * (c->c15[i] * la + c->c35[i] * lb + c->c55[i] * le);
+          T[0][i] = Lxx;
+          T[1][i] = Lsh;
+          T[2][i] = Lsh;
+          T[3][i] = Lzz;
+          L.sxx[i] *= c->coef1[i];
+          L.szz[i] *= c->coef1[i];
+          L.sxz[i] *= c->coef1[i];
+          continue;
+        }
         const double s = c->sn[i], co = c->cs[i];
         const double rxx = co * vxx - s * vxz, rxz = s * vxx + co * vxz;
         const double rzx = co * vzx - s * vzz, rzz = s * vzx + co * vzz;
-        const double la = L.sxx[i], lb = L.szz[i], le = L.sxz[i], b = c->coef2[i];
         const double c11 = c->c11[i], c13 = c->c13[i], c33 = c->c33[i], c55 = c->c55[i];
         gc11[i] += b * la * rxx;
         gc13[i] += b * (la * rzz + lb * rxx);
@@ -473,9 +561,12 @@ double adj_gradient(adj_ctx *c, const double *dobs[3], double *g_vp, double *g_e
         const double sxz_x = hx * (e1 + e2), sxz_z = hz * (e1 - e2);
         const double br = c->coef2[i] * c->ir[i];
         const double Fx = br * L.vx[i], Fz = br * L.vz[i];
-        const double cv = c->csv[i], sv = c->snv[i];
-        gsv[i] += Fx * (-sxx_z + sxz_x) + Fz * (-sxz_z + szz_x);
-        gcv[i] += Fx * (sxx_x + sxz_z) + Fz * (sxz_x + szz_z);
+        /* coordinate: rotation by theta_v; Bond: fx = sxx_x + sxz_z, fz = sxz_x + szz_z */
+        const double cv = c->bond ? 1.0 : c->csv[i], sv = c->bond ? 0.0 : c->snv[i];
+        if (!c->bond) {
+          gsv[i] += Fx * (-sxx_z + sxz_x) + Fz * (-sxz_z + szz_x);
+          gcv[i] += Fx * (sxx_x + sxz_z) + Fz * (sxz_x + szz_z);
+        }
         const double Axx_x = cv * Fx, Axx_z = -sv * Fx;
         const double Axz_x = sv * Fx + cv * Fz, Axz_z = cv * Fx - sv * Fz;
         const double Azz_x = sv * Fz, Azz_z = cv * Fz;
@@ -518,9 +609,28 @@ double adj_gradient(adj_ctx *c, const double *dobs[3], double *g_vp, double *g_e
       const double q = sqrt(f * (f + 2.0 * d));
       const double dc11_dp = 2.0 * r * p * (1.0 + 2.0 * e), dc33_dp = 2.0 * r * p;
       const double dc13_dp = r * (2.0 * p * q + p * p * (f + d) / q * 2.0 * s * s / (p * p * p));
-      g_vp[i] = (gc11[i] * dc11_dp + gc13[i] * dc13_dp + gc33[i] * dc33_dp) / B;
-      g_eps[i] = gc11[i] * 2.0 * r * p * p;
-      g_delta[i] = gc13[i] * r * p * p * f / q;
+      double G11 = gc11[i], G13 = gc13[i], G33 = gc33[i];  /* gradients of the VTI moduli */
+      if (c->bond) {
+        const double th = c->scalar * c->theta[i] / 180.0 * M_PI;
+        const double C11 = r * p * p * (1.0 + 2.0 * e), C13 = r * (p * p * q - s * s), C33 = r * p * p,
+                     C55 = r * s * s;
+        double dm[4][6];
+        bond_moduli_grad(C11, C13, C33, C55, th, dm);
+        const double gm[6] = {gc11[i], gc13[i], gc15[i], gc33[i], gc35[i], gc55[i]};
+        G11 = G13 = G33 = 0.0;
+        double gt = 0.0;
+        for (int k = 0; k < 6; ++k) {
+          G11 += gm[k] * dm[0][k];
+          G13 += gm[k] * dm[1][k];
+          G33 += gm[k] * dm[2][k];
+          gt += gm[k] * dm[3][k];
+        }
+        g_theta[i] = gt * rad;
+      }
+      g_vp[i] = (G11 * dc11_dp + G13 * dc13_dp + G33 * dc33_dp) / B;
+      g_eps[i] = G11 * 2.0 * r * p * p;
+      g_delta[i] = G13 * r * p * p * f / q;
+      if (c->bond) continue;
       /* theta at the stress node, plus the velocity-node averages that read it */
       double gt = gth[i];
       const double sn = c->sn[i], cs = c->cs[i];
@@ -546,6 +656,8 @@ double adj_gradient(adj_ctx *c, const double *dobs[3], double *g_vp, double *g_e
   free(gc55);
   free(gth);
   free(gsv);
+  free(gc15);
+  free(gc35);
   free(gcv);
   for (int k = 0; k < 3; ++k) free(rec[k]);
   return J;

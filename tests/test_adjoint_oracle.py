@@ -13,8 +13,8 @@ from pyoracle import AdjointOracle
 CFG = dict(nz=36, nx=48, nt=220, dx=10.0, dz=10.0, dt=0.001, fpeak=15.0, ealThick=8, seistype=3, mt=1)
 
 
-def _setup(fs, seed=5):
-    cfg = dict(CFG, freesurface=fs)
+def _setup(fs, seed=5, variant="coordinate_rotation"):
+    cfg = dict(CFG, freesurface=fs, variant=variant)
     m = synthetic.layered_model(cfg["nz"], cfg["nx"], seed=seed, nlayers=4)
     pads = synthetic.padded(m, cfg["ealThick"])
     adj = AdjointOracle(cfg, pads)
@@ -27,9 +27,12 @@ def _setup(fs, seed=5):
     return cfg, adj, pads, w
 
 
-@pytest.mark.parametrize("fs", [0, 1])
-def test_dot_product(fs):
-    cfg, adj, pads, w = _setup(fs)
+CASES = [(0, "coordinate_rotation"), (1, "coordinate_rotation"), (0, "bond_transformation")]
+
+
+@pytest.mark.parametrize("fs,variant", CASES)
+def test_dot_product(fs, variant):
+    cfg, adj, pads, w = _setup(fs, variant=variant)
     with adj:
         d = adj.forward()
         rng = np.random.default_rng(1)
@@ -47,9 +50,9 @@ def _misfit(adj, model, dobs):
     return 0.5 * sum(float(np.sum((a - b) ** 2)) for a, b in zip(d, dobs))
 
 
-@pytest.mark.parametrize("fs", [0, 1])
-def test_gradient_matches_central_differences(fs):
-    cfg, adj, pads, w = _setup(fs)
+@pytest.mark.parametrize("fs,variant", CASES)
+def test_gradient_matches_central_differences(fs, variant):
+    cfg, adj, pads, w = _setup(fs, variant=variant)
     E = cfg["ealThick"] + 5
     with adj:
         # observed data from a model with a perturbed patch; gradient at the start model

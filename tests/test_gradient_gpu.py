@@ -15,8 +15,8 @@ CFG = dict(nz=36, nx=48, nt=220, dx=10.0, dz=10.0, dt=0.001, fpeak=15.0, ealThic
 NAMES = ("vp", "eps", "delta", "theta")
 
 
-def _case(fs, sx=24):
-    cfg = dict(CFG, freesurface=fs)
+def _case(fs, sx=24, variant="coordinate_rotation"):
+    cfg = dict(CFG, freesurface=fs, variant=variant)
     m = synthetic.layered_model(cfg["nz"], cfg["nx"], seed=5, nlayers=4)
     pads = synthetic.padded(m, cfg["ealThick"])
     E = cfg["ealThick"] + 5
@@ -33,7 +33,7 @@ def _device(cfg, pads, w, gx, dobs, ncheck, sx=24, h=None):
 
     own = h is None
     if own:
-        h = ttifd.Modeling(variant="coordinate_rotation", stype=1, **cfg)
+        h = ttifd.Modeling(stype=1, **dict({"variant": "coordinate_rotation"}, **cfg))
         h.upload_model(*pads)
         h.grad_zero()
     h.set_source([sx], [3], w[None, :])
@@ -49,14 +49,15 @@ def _rel(a, b):
 
 
 @pytest.mark.parametrize("kernel", ["tiled", "naive"])
-@pytest.mark.parametrize("fs", [0, 1])
-def test_gradient_matches_cpu_reference(fs, kernel, monkeypatch, gpu_lib):
+@pytest.mark.parametrize("fs,variant", [(0, "coordinate_rotation"), (1, "coordinate_rotation"),
+                                        (0, "bond_transformation")])
+def test_gradient_matches_cpu_reference(fs, variant, kernel, monkeypatch, gpu_lib):
     """Both adjoint paths: TMA-tiled (default) and one thread per cell (TTIFD_KERNEL=naive)."""
     if kernel == "naive":
         monkeypatch.setenv("TTIFD_KERNEL", "naive")
     else:
         monkeypatch.delenv("TTIFD_KERNEL", raising=False)
-    cfg, pads, true, w, gx = _case(fs)
+    cfg, pads, true, w, gx = _case(fs, variant=variant)
     with AdjointOracle(cfg, pads) as adj:
         adj.set_model(*true)
         adj.set_source([24], [3], w[None, :])
@@ -109,7 +110,7 @@ def test_device_dot_product(gpu_lib):
     import ttifd
 
     cfg, pads, true, w, gx = _case(1)
-    with ttifd.Modeling(variant="coordinate_rotation", stype=1, **cfg) as h:
+    with ttifd.Modeling(stype=1, **cfg) as h:
         h.upload_model(*pads)
         h.set_source([24], [3], w[None, :])
         for k in (0, 1, 2):
@@ -127,10 +128,12 @@ def test_device_dot_product(gpu_lib):
     assert abs(lhs - rhs) <= 2e-4 * abs(lhs), (lhs, rhs)
 
 
-def test_gradient_rejects_other_formulations(gpu_lib):
+@pytest.mark.parametrize("variant,fs", [("tensor_rotation", 0), ("bond_transformation", 1)])
+def test_gradient_rejects_unsupported_cases(variant, fs, gpu_lib):
+    """No tensor-rotation gradient; no Bond gradient with the free-surface stiffness rewrite."""
     import ttifd
 
-    with ttifd.Modeling(variant="tensor_rotation", stype=1, **CFG) as h:
+    with ttifd.Modeling(stype=1, **dict(CFG, variant=variant, freesurface=fs)) as h:
         with pytest.raises(ttifd.TTIError) as e:
             h.grad_zero()
         assert e.value.code == ttifd.ERR_ARG

@@ -37,7 +37,8 @@ struct GradState {
   float *lam[5] = {};       // adjoint vx vz sxx szz sxz
   float *T[4] = {};         // stress-half adjoint strain terms (read by the transposed stress stencils)
   float *TV[6] = {};        // velocity-half adjoint derivative terms (read by the transposed velocity stencils)
-  float *acc[7] = {};       // sums: c11 c13 c33 (c55: kept zero, vs and rho are fixed) theta(stress node) sin_v cos_v
+  float *acc[7] = {};       // sums. coordinate: c11 c13 c33 (c55 kept zero) theta(stress node) sin_v cos_v;
+                            // Bond: c11 c13 c33 c55 c15 c35 (the rotated moduli)
   float *out[4] = {};       // vp eps delta theta
   float *ckpt = nullptr;    // ncheck x 5 fields
   float *keep = nullptr;    // seg x 5 fields
@@ -163,6 +164,7 @@ __global__ void k_adj_free_surface(Grid g, AdjArgs a)
 }
 
 // stress-half adjoint, local part: gradient sums, T0..T3, lambda_sigma *= coef1
+template <int V>
 __global__ void __launch_bounds__(BZ *BX) k_adj_stress_local(AdjArgs a)
 {
   const Grid &g = a.g;
@@ -173,6 +175,27 @@ __global__ void __launch_bounds__(BZ *BX) k_adj_stress_local(AdjArgs a)
   pair_s(a.keep[0], L, ix, iz, a1, a2);
   pair_s(a.keep[1], L, ix, iz, b1, b2);
   const float vxx = a.hx * (a1 + a2), vxz = a.hz * (a1 - a2), vzx = a.hx * (b1 + b2), vzz = a.hz * (b1 - b2);
+  if (V == TTI_BOND) {  // sigma += coef2 H (vxx, vzz, vzx + vxz), H symmetric with c15, c35 (bond:836-873)
+    const float la = a.lam[2][i], lb = a.lam[3][i], le = a.lam[4][i], b = a.p.coef2[i], sh = vzx + vxz;
+    const float c11 = a.p.c11[i], c13 = a.p.c13[i], c15 = a.p.c15[i], c33 = a.p.c33[i], c35 = a.p.c35[i],
+                c55 = a.p.c55[i];
+    a.acc[0][i] += b * la * vxx;
+    a.acc[1][i] += b * (la * vzz + lb * vxx);
+    a.acc[2][i] += b * lb * vzz;
+    a.acc[3][i] += b * le * sh;
+    a.acc[4][i] += b * (la * sh + le * vxx);
+    a.acc[5][i] += b * (lb * sh + le * vzz);
+    const float Lsh = b * (c15 * la + c35 * lb + c55 * le);
+    a.T[0][i] = b * (c11 * la + c13 * lb + c15 * le);
+    a.T[1][i] = Lsh;
+    a.T[2][i] = Lsh;
+    a.T[3][i] = b * (c13 * la + c33 * lb + c35 * le);
+    const float c1 = a.p.coef1[i];
+    a.lam[2][i] = c1 * la;
+    a.lam[3][i] = c1 * lb;
+    a.lam[4][i] = c1 * le;
+    return;
+  }
   const float s = a.p.sn[i], co = a.p.cs[i];
   const float rxx = co * vxx - s * vxz, rxz = s * vxx + co * vxz;
   const float rzx = co * vzx - s * vzz, rzz = s * vzx + co * vzz;
@@ -196,6 +219,7 @@ __global__ void __launch_bounds__(BZ *BX) k_adj_stress_local(AdjArgs a)
 // Transposed stress stencils into lambda_v (minus the velocity-node pairs),
 // then the velocity-half adjoint at the same cell: sin/cos theta_v sums,
 // TV0..TV5, lambda_v *= coef1. Both act on one cell's lambda_v, so one pass.
+template <int V>
 __global__ void __launch_bounds__(BZ *BX) k_adj_velocity(AdjArgs a)
 {
   const Grid &g = a.g;
@@ -222,9 +246,12 @@ __global__ void __launch_bounds__(BZ *BX) k_adj_velocity(AdjArgs a)
   const float sxz_x = hx * (e1 + e2), sxz_z = hz * (e1 - e2);
   const float br = a.p.coef2[i] * a.p.invrho[i];
   const float Fx = br * lx, Fz = br * lz;
-  const float cv = a.p.csv[i], sv = a.p.snv[i];
-  a.acc[5][i] += Fx * (sxz_x - sxx_z) + Fz * (szz_x - sxz_z);
-  a.acc[6][i] += Fx * (sxx_x + sxz_z) + Fz * (sxz_x + szz_z);
+  // coordinate: rotation by theta_v; Bond: fx = sxx_x + sxz_z, fz = sxz_x + szz_z
+  const float cv = V == TTI_BOND ? 1.0f : a.p.csv[i], sv = V == TTI_BOND ? 0.0f : a.p.snv[i];
+  if (V != TTI_BOND) {
+    a.acc[5][i] += Fx * (sxz_x - sxx_z) + Fz * (szz_x - sxz_z);
+    a.acc[6][i] += Fx * (sxx_x + sxz_z) + Fz * (sxz_x + szz_z);
+  }
   const float Axx_x = cv * Fx, Axx_z = -sv * Fx;
   const float Axz_x = sv * Fx + cv * Fz, Axz_z = cv * Fx - sv * Fz;
   const float Azz_x = sv * Fz, Azz_z = cv * Fz;
@@ -315,6 +342,7 @@ __device__ __forceinline__ void vpair(const float *q, float &d1, float &d2)
 
 // transposed stress stencils into lambda_v, then the velocity-half adjoint
 // (maps: T0..T3, kept sxx, szz, sxz)
+template <int V>
 __global__ void __launch_bounds__(tiled::NT, 2) k_adj_velocity_tiled(const __grid_constant__ AdjTile at)
 {
   constexpr int F = tiled::FIELD, B = tiled::BZ;
@@ -352,12 +380,17 @@ __global__ void __launch_bounds__(tiled::NT, 2) k_adj_velocity_tiled(const __gri
     const float sxx_x = hx * (a1 + a2), sxx_z = hx * (a1 - a2);  // 1/dx for both, as coord:633
     const float szz_x = hx * (b1 + b2), szz_z = hz * (b1 - b2);
     const float sxz_x = hx * (e1 + e2), sxz_z = hz * (e1 - e2);
-    const float2 cf = __ldg(at.pk.cf + i), vsc = __ldg(at.pk.vsc + i);
+    const float2 cf = __ldg(at.pk.cf + i);
     const float br = cf.y * __ldg(a.p.invrho + i);
     const float Fx = br * lx, Fz = br * lz;
-    const float sv = vsc.x, cv = vsc.y;
-    a.acc[5][i] += Fx * (sxz_x - sxx_z) + Fz * (szz_x - sxz_z);
-    a.acc[6][i] += Fx * (sxx_x + sxz_z) + Fz * (sxz_x + szz_z);
+    float sv = 0.0f, cv = 1.0f;  // Bond: fx = sxx_x + sxz_z, fz = sxz_x + szz_z
+    if (V != TTI_BOND) {
+      const float2 vsc = __ldg(at.pk.vsc + i);
+      sv = vsc.x;
+      cv = vsc.y;
+      a.acc[5][i] += Fx * (sxz_x - sxx_z) + Fz * (szz_x - sxz_z);
+      a.acc[6][i] += Fx * (sxx_x + sxz_z) + Fz * (sxz_x + szz_z);
+    }
     const float Axx_x = cv * Fx, Axx_z = -sv * Fx;
     const float Axz_x = sv * Fx + cv * Fz, Axz_z = cv * Fx - sv * Fz;
     const float Azz_x = sv * Fz, Azz_z = cv * Fz;
@@ -446,10 +479,35 @@ __global__ void k_residual(const float *rec, const float *obs, float *res, size_
   if ((threadIdx.x & 31) == 0) atomicAdd(J, acc);
 }
 
-// chain rule to vp, epsilon, delta, theta (degrees), every cell
-__global__ void k_chain(Grid g, Params p, const float *vp, const float *vs, const float *rho, const float *beta,
-                        const float *eps, const float *delta, GradState gs, float rad)
+// Bond rotation of the VTI moduli (bond:492-541): derivatives of c11 c13 c15
+// c33 c35 c55 with respect to C11, C13, C33 and theta (d[0..3][0..5])
+__device__ void bond_moduli_grad(double C11, double C13, double C33, double C55, double th, double d[4][6])
 {
+  const double sn = sin(th), cs = cos(th);
+  const double s2 = sn * sn, c2 = cs * cs, s4 = s2 * s2, c4 = c2 * c2;
+  const double s2t = sin(2.0 * th), c2t = cos(2.0 * th), s22 = s2t * s2t;
+  const double ds2 = s2t, dc2 = -s2t, ds4 = 2.0 * s2 * s2t, dc4 = -2.0 * c2 * s2t;
+  const double ds2t = 2.0 * c2t, dc2t = -2.0 * s2t, ds22 = 4.0 * s2t * c2t, dc22 = -ds22;
+  const double A = C13 + 2.0 * C55;
+  const double rows[4][6] = {
+      {c4, 0.25 * s22, -0.5 * c2 * s2t, s4, -0.5 * s2 * s2t, 0.25 * s22},
+      {0.5 * s22, s4 + c4, 0.5 * c2t * s2t, 0.5 * s22, -0.5 * c2t * s2t, -0.5 * s22},
+      {s4, 0.25 * s22, 0.5 * s2 * s2t, c4, 0.5 * c2 * s2t, 0.25 * s22},
+      {C11 * dc4 + C33 * ds4 + (0.5 * C13 + C55) * ds22, (0.25 * (C11 + C33) - C55) * ds22 + C13 * (ds4 + dc4),
+       0.5 * ((-C11 * dc2 + C33 * ds2 + A * dc2t) * s2t + (-C11 * c2 + C33 * s2 + A * c2t) * ds2t),
+       C11 * ds4 + C33 * dc4 + (0.5 * C13 + C55) * ds22,
+       0.5 * ((-C11 * ds2 + C33 * dc2 - A * dc2t) * s2t + (-C11 * s2 + C33 * c2 - A * c2t) * ds2t),
+       0.25 * (C11 + C33 - 2.0 * C13) * ds22 + C55 * dc22}};
+  for (int m = 0; m < 4; ++m)
+    for (int k = 0; k < 6; ++k) d[m][k] = rows[m][k];
+}
+
+// chain rule to vp, epsilon, delta, theta (degrees), every cell
+template <int V>
+__global__ void k_chain(Grid g, Params p, const float *vp, const float *vs, const float *rho, const float *beta,
+                        const float *eps, const float *delta, const float *theta, GradState gs, float scalar)
+{
+  const float rad = (float)(scalar * M_PI / 180.0);
   const int iz = blockIdx.x * BZ + threadIdx.x, ix = blockIdx.y * BX + threadIdx.y;
   if (iz >= g.Nz || ix >= g.Nx) return;
   const size_t L = g.ldz, i = (size_t)ix * L + iz;
@@ -458,10 +516,27 @@ __global__ void k_chain(Grid g, Params p, const float *vp, const float *vs, cons
   const double q = sqrt(f * (f + 2.0 * d));
   const double dc11 = 2.0 * R * P * (1.0 + 2.0 * e), dc33 = 2.0 * R * P;
   const double dc13 = q > 0.0 ? R * (2.0 * P * q + (f + d) / q * 2.0 * S * S / P) : 0.0;
-  const double g11 = gs.acc[0][i], g13 = gs.acc[1][i], g33 = gs.acc[2][i];
+  double g11 = gs.acc[0][i], g13 = gs.acc[1][i], g33 = gs.acc[2][i];  // VTI moduli (coordinate)
+  if (V == TTI_BOND) {  // through the Bond rotation: sums of c11 c13 c33 c55 c15 c35
+    const double C11 = R * P * P * (1.0 + 2.0 * e), C13 = R * (P * P * q - S * S), C33 = R * P * P, C55 = R * S * S;
+    double dm[4][6];
+    const double th = scalar * (double)theta[i] / 180.0 * M_PI;
+    bond_moduli_grad(C11, C13, C33, C55, th, dm);
+    const double gm[6] = {gs.acc[0][i], gs.acc[1][i], gs.acc[4][i], gs.acc[2][i], gs.acc[5][i], gs.acc[3][i]};
+    g11 = g13 = g33 = 0.0;
+    double gt = 0.0;
+    for (int k = 0; k < 6; ++k) {
+      g11 += gm[k] * dm[0][k];
+      g13 += gm[k] * dm[1][k];
+      g33 += gm[k] * dm[2][k];
+      gt += gm[k] * dm[3][k];
+    }
+    gs.out[3][i] = (float)(gt * rad);
+  }
   gs.out[0][i] = (float)((g11 * dc11 + g13 * dc13 + g33 * dc33) / B);
   gs.out[1][i] = (float)(g11 * 2.0 * R * P * P);
   gs.out[2][i] = (float)(q > 0.0 ? g13 * R * P * P * f / q : 0.0);
+  if (V == TTI_BOND) return;
   double gt = gs.acc[4][i];
   const double sn = p.sn[i], cs = p.cs[i];
   for (int a = 0; a <= 1; ++a)
@@ -488,8 +563,11 @@ int gerr(tti_handle *h, int code, const char *msg) { return handle_error(h, code
 
 int grad_check(tti_handle *h)
 {
-  if (h->cfg.variant != TTI_COORDINATE)
-    return gerr(h, TTI_ERR_ARG, "the adjoint-state gradient is implemented for the coordinate formulation");
+  if (h->cfg.variant == TTI_TENSOR)
+    return gerr(h, TTI_ERR_ARG,
+                "the adjoint-state gradient is implemented for the coordinate and Bond formulations");
+  if (h->cfg.variant == TTI_BOND && h->cfg.freesurface)
+    return gerr(h, TTI_ERR_ARG, "the Bond gradient does not differentiate the free-surface stiffness rewrite");
   if (h->use_fused) return gerr(h, TTI_ERR_STATE, "the gradient runs on the tiled or per-cell kernels");
   if (!h->have_model || !h->m_eps) return gerr(h, TTI_ERR_STATE, "model not uploaded");
   if (h->cfg.stype != 1) return gerr(h, TTI_ERR_ARG, "the gradient models the stress source (stype = 1)");
@@ -580,7 +658,8 @@ int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
     // the stress-half adjoint stays one thread per cell: it is bound by its
     // per-cell reads and writes, not by its two stencil fields
     const dim3 blk(BZ, BX), grd((g.Nz + BZ - 1) / BZ, (g.Nx + BX - 1) / BX);
-    k_adj_stress_local<<<grd, blk, 0, h->stream>>>(a);
+    if (c.variant == TTI_BOND) k_adj_stress_local<TTI_BOND><<<grd, blk, 0, h->stream>>>(a);
+    else k_adj_stress_local<TTI_COORDINATE><<<grd, blk, 0, h->stream>>>(a);
     AdjTile at;
     memset(&at, 0, sizeof at);
     at.a = a;
@@ -588,14 +667,20 @@ int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
     at.err = h->d_flag;
     for (int k = 0; k < 4; ++k) at.map[k] = s->maps[k];
     for (int f = 0; f < 3; ++f) at.map[4 + f] = s->slot_maps[(size_t)slot * 3 + f];  // kept sxx, szz, sxz
-    GCK(h, launch_adj_tile(k_adj_velocity_tiled, at, 7, g.izStart, g, h->stream));
+    if (c.variant == TTI_BOND) GCK(h, launch_adj_tile(k_adj_velocity_tiled<TTI_BOND>, at, 7, g.izStart, g, h->stream));
+    else GCK(h, launch_adj_tile(k_adj_velocity_tiled<TTI_COORDINATE>, at, 7, g.izStart, g, h->stream));
     for (int k = 0; k < 6; ++k) at.map[k] = s->maps[4 + k];
     GCK(h, launch_adj_tile(k_adj_vstencil_tiled, at, 6, a.z_lo, g, h->stream));
     return TTI_OK;
   }
   const dim3 blk(BZ, BX), grd((g.Nz + BZ - 1) / BZ, (g.Nx + BX - 1) / BX);
-  k_adj_stress_local<<<grd, blk, 0, h->stream>>>(a);
-  k_adj_velocity<<<grd, blk, 0, h->stream>>>(a);
+  if (c.variant == TTI_BOND) {
+    k_adj_stress_local<TTI_BOND><<<grd, blk, 0, h->stream>>>(a);
+    k_adj_velocity<TTI_BOND><<<grd, blk, 0, h->stream>>>(a);
+  } else {
+    k_adj_stress_local<TTI_COORDINATE><<<grd, blk, 0, h->stream>>>(a);
+    k_adj_velocity<TTI_COORDINATE><<<grd, blk, 0, h->stream>>>(a);
+  }
   k_adj_velocity_stencil<<<grd, blk, 0, h->stream>>>(a);
   GCK(h, cudaGetLastError());
   return TTI_OK;
@@ -780,9 +865,15 @@ int tti_grad_fetch(tti_handle *h, int which, float *out)
   GradState *s = h->grad;
   const Grid &g = h->g;
   const dim3 blk(BZ, BX), grd((g.Nz + BZ - 1) / BZ, (g.Nx + BX - 1) / BX);
-  const float rad = (float)(h->cfg.scalar * M_PI / 180.0);
-  k_chain<<<grd, blk, 0, h->stream>>>(g, handle_step_args(h).p, h->par[TTI_P_VP], h->par[TTI_P_VS],
-                                      h->par[TTI_P_RHO], h->par[TTI_P_BETA], h->m_eps, h->m_delta, *s, rad);
+  const float *th = h->m_theta;
+  if (h->cfg.variant == TTI_BOND)
+    k_chain<TTI_BOND><<<grd, blk, 0, h->stream>>>(g, handle_step_args(h).p, h->par[TTI_P_VP], h->par[TTI_P_VS],
+                                                  h->par[TTI_P_RHO], h->par[TTI_P_BETA], h->m_eps, h->m_delta, th,
+                                                  *s, h->cfg.scalar);
+  else
+    k_chain<TTI_COORDINATE><<<grd, blk, 0, h->stream>>>(g, handle_step_args(h).p, h->par[TTI_P_VP],
+                                                        h->par[TTI_P_VS], h->par[TTI_P_RHO], h->par[TTI_P_BETA],
+                                                        h->m_eps, h->m_delta, th, *s, h->cfg.scalar);
   h->launches++;
   GCK(h, cudaGetLastError());
   GCK(h, cudaMemcpy2DAsync(out, (size_t)g.Nz * sizeof(float), s->out[which], (size_t)g.ldz * sizeof(float),

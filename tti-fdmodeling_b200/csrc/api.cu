@@ -503,6 +503,7 @@ int tti_destroy(tti_handle *h)
   cudaFree(h->d_energy);
   cudaFree(h->m_eps);
   cudaFree(h->m_delta);
+  cudaFree(h->m_theta);
   grad_release(h);
   cudaFree(h->d_flag);
   cudaFree(h->d_snap);
@@ -601,10 +602,10 @@ int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const floa
     }
   }
   cudaStreamSynchronize(h->stream);
-  // the gradient's chain rule needs epsilon and delta as given
-  if (rc == TTI_OK && c.variant == TTI_COORDINATE) {
-    for (int k = 0; k < 2; ++k) {
-      float *&dst = k == 0 ? h->m_eps : h->m_delta;
+  // the gradient's chain rule needs epsilon and delta as given (and theta for Bond)
+  if (rc == TTI_OK && c.variant != TTI_TENSOR) {
+    for (int k = 0; k < (c.variant == TTI_BOND ? 3 : 2); ++k) {
+      float *&dst = k == 0 ? h->m_eps : k == 1 ? h->m_delta : h->m_theta;
       if (!dst && cudaMalloc(&dst, g.n * sizeof(float)) != cudaSuccess) {
         rc = set_err(h, TTI_ERR_NOMEM, "device allocation failed");
         break;

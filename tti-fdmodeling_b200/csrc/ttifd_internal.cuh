@@ -88,6 +88,7 @@ struct tti_handle {
   bool use_tiled = false;  // tiled half-step kernels with TMA halo tiles (in place)
   const tti_handle *owner = nullptr;  // set when the parameter arrays belong to another handle (batched shots)
   float *m_eps = nullptr, *m_delta = nullptr;  // epsilon, delta as uploaded (gradient chain rule)
+  float *m_theta = nullptr;                    // theta (degrees) as uploaded (Bond gradient chain rule)
   struct GradState *grad = nullptr;            // adjoint-state gradient buffers (adjoint.cu)
   void *tmaps = nullptr;   // host copy of the 5 tensor maps (vx vz sxx szz sxz), 64-byte aligned
   int seg = 0;          // columns per CTA of the fused step
