@@ -8,7 +8,9 @@
  * (src/main/sufdmod2dTTIelastic/sufdmod2dTTIelastic_coordinate_rotation.c:
  * velocity update :614-672, stress update :804-845, free surface :847-863,
  * stress source :865-886, receivers isoelastic.c:103-144) and of its
- * stiffness build (:497-537), and the same for the Bond-transformation
+ * stiffness build (:497-537), the same for the tensor-rotation formulation
+ * (sufdmod2dTTIelastic_tensor_rotation.c: tau update and sigma = R tau
+ * :799-851, stiffness :498-519), and for the Bond-transformation
  * formulation (sufdmod2dTTIelastic_bond_transformation.c: velocity update
  * :654-703, stress update :836-873, stiffness :492-541; without the free
  * surface, whose stiffness rewrite :543-568 is not differentiated), so that
@@ -39,7 +41,7 @@ struct adj_ctx {
   /* model and derived arrays */
   double *vp, *vs, *rho, *eps, *delta, *theta;  /* as given (padded) */
   double *c11, *c13, *c33, *c55, *sn, *cs, *snv, *csv, *ir;
-  int bond;             /* Bond transformation instead of coordinate rotation */
+  int bond, tensor;     /* Bond transformation / tensor rotation instead of coordinate rotation */
   double *c15, *c35;    /* Bond only */
   /* geometry */
   int nsrc, *sx, *sz;
@@ -100,7 +102,11 @@ void adj_grid(const adj_ctx *c, int *Nz, int *Nx, int *nts)
   *nts = c->nts;
 }
 
-void adj_set_formulation(adj_ctx *c, int bond) { c->bond = bond; }
+void adj_set_formulation(adj_ctx *c, int variant)
+{
+  c->tensor = variant == 1;
+  c->bond = variant == 2;
+}
 
 /* Bond rotation of the VTI moduli (bond:492-541): c11 c13 c15 c33 c35 c55 */
 static void bond_moduli(double C11, double C13, double C33, double C55, double th, double out[6])
@@ -260,7 +266,7 @@ static double src_weight(const adj_ctx *c, int a, int b)
 
 /* ---------------------------------------------------------------- forward */
 typedef struct {
-  double *vx, *vz, *sxx, *szz, *sxz;
+  double *vx, *vz, *sxx, *szz, *sxz, *txx, *tzz, *txz;  /* tau: tensor rotation only */
 } state;
 
 static void velocity_half(const adj_ctx *c, state *u)
@@ -277,7 +283,7 @@ static void velocity_half(const adj_ctx *c, state *u)
       const double sxz_x = hx * (e1 + e2), sxz_z = hz * (e1 - e2);
       const size_t i = (size_t)ix * c->Nz + iz;
       const double cv = c->csv[i], sv = c->snv[i], br = c->coef2[i] * c->ir[i];
-      if (c->bond) {
+      if (c->bond || c->tensor) {
         u->vx[i] = c->coef1[i] * u->vx[i] + br * (sxx_x + sxz_z);
         u->vz[i] = c->coef1[i] * u->vz[i] + br * (sxz_x + szz_z);
       } else {
@@ -306,6 +312,21 @@ static void stress_half(const adj_ctx *c, state *u)
         continue;
       }
       const double s = c->sn[i], co = c->cs[i];
+      if (c->tensor) {  /* rotated strain rates, Hooke on tau, sigma = R tau (tensor:826-851) */
+        const double s2 = s * s, c2 = co * co, st = 2.0 * s * co, sh = vxz + vzx;
+        const double exx = c2 * vxx + s2 * vzz - 0.5 * st * sh, ezz = s2 * vxx + c2 * vzz + 0.5 * st * sh;
+        const double exz = st * (vxx - vzz) + (c2 - s2) * sh;
+        const double nxx = a * u->txx[i] + b * (c->c11[i] * exx + c->c13[i] * ezz);
+        const double nzz = a * u->tzz[i] + b * (c->c13[i] * exx + c->c33[i] * ezz);
+        const double nxz = a * u->txz[i] + b * c->c55[i] * exz;
+        u->txx[i] = nxx;
+        u->tzz[i] = nzz;
+        u->txz[i] = nxz;
+        u->sxx[i] = c2 * nxx + s2 * nzz + st * nxz;
+        u->szz[i] = s2 * nxx + c2 * nzz - st * nxz;
+        u->sxz[i] = -0.5 * st * (nxx - nzz) + (c2 - s2) * nxz;
+        continue;
+      }
       const double rxx = co * vxx - s * vxz, rxz = s * vxx + co * vxz;
       const double rzx = co * vzx - s * vzz, rzz = s * vzx + co * vzz;
       u->sxx[i] = a * u->sxx[i] + b * (c->c11[i] * rxx + c->c13[i] * rzz);
@@ -340,6 +361,10 @@ static void stress_source(const adj_ctx *c, state *u, int it)
         const double k = 0.5 * src_weight(c, a, b) * w;
         A2(u->sxx, ix, iz) += k;
         A2(u->szz, ix, iz) += k;
+        if (c->tensor) {
+          A2(u->txx, ix, iz) += k;
+          A2(u->tzz, ix, iz) += k;
+        }
       }
   }
 }
@@ -368,7 +393,7 @@ static void record(const adj_ctx *c, const state *u, int it, double *rec[3])
 
 static state state_alloc(size_t n)
 {
-  state s = {dalloc(n), dalloc(n), dalloc(n), dalloc(n), dalloc(n)};
+  state s = {dalloc(n), dalloc(n), dalloc(n), dalloc(n), dalloc(n), dalloc(n), dalloc(n), dalloc(n)};
   return s;
 }
 
@@ -379,10 +404,13 @@ static void state_free(state *s)
   free(s->sxx);
   free(s->szz);
   free(s->sxz);
+  free(s->txx);
+  free(s->tzz);
+  free(s->txz);
 }
 
 /* one step; `keep` (may be NULL) receives (v after the velocity half, sigma
- * before the stress half), the two states the adjoint step reads */
+ * and tau before the stress half), the states the adjoint step reads */
 static void step(const adj_ctx *c, state *u, int it, double *rec[3], state *keep)
 {
   velocity_half(c, u);
@@ -392,6 +420,9 @@ static void step(const adj_ctx *c, state *u, int it, double *rec[3], state *keep
     memcpy(keep->sxx, u->sxx, c->Np * sizeof(double));
     memcpy(keep->szz, u->szz, c->Np * sizeof(double));
     memcpy(keep->sxz, u->sxz, c->Np * sizeof(double));
+    memcpy(keep->txx, u->txx, c->Np * sizeof(double));
+    memcpy(keep->tzz, u->tzz, c->Np * sizeof(double));
+    memcpy(keep->txz, u->txz, c->Np * sizeof(double));
   }
   stress_half(c, u);
   if (c->fs) free_surface(c, u);
@@ -469,6 +500,7 @@ double adj_gradient(adj_ctx *c, const double *dobs[3], double *g_vp, double *g_e
             const int ix = x0 + a, iz = z0 + b;
             if (ix < 0 || ix >= Nx || iz < 0 || iz >= Nz) continue;
             acc += 0.5 * src_weight(c, a, b) * (A2(L.sxx, ix, iz) + A2(L.szz, ix, iz));
+            if (c->tensor) acc += 0.5 * src_weight(c, a, b) * (A2(L.txx, ix, iz) + A2(L.tzz, ix, iz));
           }
         g_src[(size_t)n * c->nt + it] = acc;
       }
@@ -518,6 +550,43 @@ double adj_gradient(adj_ctx *c, const double *dobs[3], double *g_vp, double *g_e
           continue;
         }
         const double s = c->sn[i], co = c->cs[i];
+        if (c->tensor) {
+          /* forward: n = coef1 tau + coef2 H e(theta, v); tau' = n; sigma' = R(theta) n */
+          const double s2 = s * s, c2 = co * co, st = 2.0 * s * co, cd = c2 - s2, sh = vxz + vzx;
+          const double exx = c2 * vxx + s2 * vzz - 0.5 * st * sh, ezz = s2 * vxx + c2 * vzz + 0.5 * st * sh;
+          const double exz = st * (vxx - vzz) + cd * sh;
+          const double c11 = c->c11[i], c13 = c->c13[i], c33 = c->c33[i], c55 = c->c55[i], a = c->coef1[i];
+          const double nxx = a * f->txx[i] + b * (c11 * exx + c13 * ezz);
+          const double nzz = a * f->tzz[i] + b * (c13 * exx + c33 * ezz);
+          const double nxz = a * f->txz[i] + b * c55 * exz;
+          /* lambda_n = lambda_tau' + R^T lambda_sigma' */
+          const double lxx = L.txx[i] + c2 * la + s2 * lb - 0.5 * st * le;
+          const double lzz = L.tzz[i] + s2 * la + c2 * lb + 0.5 * st * le;
+          const double lxz = L.txz[i] + st * la - st * lb + cd * le;
+          gc11[i] += b * lxx * exx;
+          gc13[i] += b * (lxx * ezz + lzz * exx);
+          gc33[i] += b * lzz * ezz;
+          gc55[i] += b * lxz * exz;
+          /* theta: through the strain rotation and through R */
+          const double dexx = st * (vzz - vxx) - cd * sh, dexz = 2.0 * cd * (vxx - vzz) - 2.0 * st * sh;
+          const double dnxx = b * (c11 * dexx - c13 * dexx), dnzz = b * (c13 * dexx - c33 * dexx);
+          const double dnxz = b * c55 * dexz;
+          const double rxx_ = -st * nxx + st * nzz + 2.0 * cd * nxz, rzz_ = -rxx_;
+          const double rxz_ = -cd * (nxx - nzz) - 2.0 * st * nxz;
+          gth[i] += lxx * dnxx + lzz * dnzz + lxz * dnxz + la * rxx_ + lb * rzz_ + le * rxz_;
+          /* lambda of the strain rates, then of the velocity derivatives */
+          const double Lexx = b * (c11 * lxx + c13 * lzz), Lezz = b * (c13 * lxx + c33 * lzz), Lexz = b * c55 * lxz;
+          const double Lsh = -0.5 * st * Lexx + 0.5 * st * Lezz + cd * Lexz;
+          T[0][i] = c2 * Lexx + s2 * Lezz + st * Lexz;
+          T[1][i] = Lsh;
+          T[2][i] = Lsh;
+          T[3][i] = s2 * Lexx + c2 * Lezz - st * Lexz;
+          L.txx[i] = a * lxx;
+          L.tzz[i] = a * lzz;
+          L.txz[i] = a * lxz;
+          L.sxx[i] = L.szz[i] = L.sxz[i] = 0.0;  /* sigma is overwritten by R tau */
+          continue;
+        }
         const double rxx = co * vxx - s * vxz, rxz = s * vxx + co * vxz;
         const double rzx = co * vzx - s * vzz, rzz = s * vzx + co * vzz;
         const double c11 = c->c11[i], c13 = c->c13[i], c33 = c->c33[i], c55 = c->c55[i];
@@ -562,8 +631,9 @@ double adj_gradient(adj_ctx *c, const double *dobs[3], double *g_vp, double *g_e
         const double br = c->coef2[i] * c->ir[i];
         const double Fx = br * L.vx[i], Fz = br * L.vz[i];
         /* coordinate: rotation by theta_v; Bond: fx = sxx_x + sxz_z, fz = sxz_x + szz_z */
-        const double cv = c->bond ? 1.0 : c->csv[i], sv = c->bond ? 0.0 : c->snv[i];
-        if (!c->bond) {
+        const int norot = c->bond || c->tensor;
+        const double cv = norot ? 1.0 : c->csv[i], sv = norot ? 0.0 : c->snv[i];
+        if (!norot) {
           gsv[i] += Fx * (-sxx_z + sxz_x) + Fz * (-sxz_z + szz_x);
           gcv[i] += Fx * (sxx_x + sxz_z) + Fz * (sxz_x + szz_z);
         }
@@ -630,7 +700,8 @@ double adj_gradient(adj_ctx *c, const double *dobs[3], double *g_vp, double *g_e
       g_vp[i] = (G11 * dc11_dp + G13 * dc13_dp + G33 * dc33_dp) / B;
       g_eps[i] = G11 * 2.0 * r * p * p;
       g_delta[i] = G13 * r * p * p * f / q;
-      if (c->bond) continue;
+      if (c->tensor) g_theta[i] = gth[i] * rad;  /* no rotation at the velocity node */
+      if (c->bond || c->tensor) continue;
       /* theta at the stress node, plus the velocity-node averages that read it */
       double gt = gth[i];
       const double sn = c->sn[i], cs = c->cs[i];

@@ -15,8 +15,9 @@ adj_ctx *adj_create(int nz, int nx, int nt, double dx, double dz, double dt, int
                     int seistype, double scalar);
 void adj_destroy(adj_ctx *c);
 void adj_grid(const adj_ctx *c, int *Nz, int *Nx, int *nts);
-/* 1: Bond transformation (without free surface); 0: coordinate rotation (default). Before adj_set_model. */
-void adj_set_formulation(adj_ctx *c, int bond);
+/* 0: coordinate rotation (default), 1: tensor rotation, 2: Bond transformation
+ * (without free surface). Before adj_set_model. */
+void adj_set_formulation(adj_ctx *c, int variant);
 /* frozen MEAL arrays, padded [Nx][Nz] */
 void adj_set_meal(adj_ctx *c, const float *coef1, const float *coef2, const float *beta);
 /* padded [Nx][Nz] model (theta in degrees); builds the coordinate-rotation stiffness */

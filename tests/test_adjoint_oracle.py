@@ -27,7 +27,8 @@ def _setup(fs, seed=5, variant="coordinate_rotation"):
     return cfg, adj, pads, w
 
 
-CASES = [(0, "coordinate_rotation"), (1, "coordinate_rotation"), (0, "bond_transformation")]
+CASES = [(0, "coordinate_rotation"), (1, "coordinate_rotation"), (0, "bond_transformation"),
+         (0, "tensor_rotation"), (1, "tensor_rotation")]
 
 
 @pytest.mark.parametrize("fs,variant", CASES)

@@ -34,14 +34,14 @@ using namespace ttifd;
 
 struct GradState {
   int ncheck = 0, seg = 0;  // checkpoints, steps per segment
-  float *lam[5] = {};       // adjoint vx vz sxx szz sxz
+  float *lam[8] = {};       // adjoint vx vz sxx szz sxz (+ txx tzz txz: tensor rotation)
   float *T[4] = {};         // stress-half adjoint strain terms (read by the transposed stress stencils)
   float *TV[6] = {};        // velocity-half adjoint derivative terms (read by the transposed velocity stencils)
   float *acc[7] = {};       // sums. coordinate: c11 c13 c33 (c55 kept zero) theta(stress node) sin_v cos_v;
                             // Bond: c11 c13 c33 c55 c15 c35 (the rotated moduli)
   float *out[4] = {};       // vp eps delta theta
-  float *ckpt = nullptr;    // ncheck x 5 fields
-  float *keep = nullptr;    // seg x 5 fields
+  float *ckpt = nullptr;    // (ncheck - 1) x the formulation's fields (5, tensor 8)
+  float *keep = nullptr;    // seg x 5 fields: vx vz and sxx szz sxz (tensor: txx tzz txz)
   float *obs[3] = {};       // observed traces, time-major [nts][ntrace]
   float *res[3] = {};       // residuals, time-major
   float *gsrc = nullptr;    // [nsrc][nt]
@@ -60,7 +60,7 @@ constexpr int BZ = 32, BX = 8;
 struct AdjArgs {
   Grid g;
   Params p;
-  float *lam[5];
+  float *lam[8];
   float *T[4];
   float *TV[6];
   float *acc[7];
@@ -132,6 +132,7 @@ __global__ void k_source_grad(Grid g, AdjArgs a, SourceSet s, K1 tab, float *gsr
     if (ix >= 0 && ix < g.Nx && iz >= 0 && iz < g.Nz) {
       const size_t c = (size_t)ix * g.ldz + iz;
       v = tab.k1[t] * (a.lam[2][c] + a.lam[3][c]);
+      if (a.lam[5]) v += tab.k1[t] * (a.lam[5][c] + a.lam[6][c]);  // tensor: the source also adds to tau
     }
   }
   part[t] = v;
@@ -196,6 +197,42 @@ __global__ void __launch_bounds__(BZ *BX) k_adj_stress_local(AdjArgs a)
     a.lam[4][i] = c1 * le;
     return;
   }
+  if (V == TTI_TENSOR) {
+    // forward (tensor:826-851): n = coef1 tau + coef2 H e(theta, v); tau' = n; sigma' = R(theta) n.
+    // keep[2..4] hold tau before the stress half.
+    const float la = a.lam[2][i], lb = a.lam[3][i], le = a.lam[4][i], b = a.p.coef2[i], c1 = a.p.coef1[i];
+    const float s2 = a.p.s2[i], c2 = a.p.c2[i], st = a.p.s2t[i], cd = c2 - s2, sh = vxz + vzx;
+    const float c11 = a.p.c11[i], c13 = a.p.c13[i], c33 = a.p.c33[i], c55 = a.p.c55[i];
+    const float exx = c2 * vxx + s2 * vzz - 0.5f * st * sh, ezz = s2 * vxx + c2 * vzz + 0.5f * st * sh;
+    const float exz = st * (vxx - vzz) + cd * sh;
+    const float nxx = c1 * a.keep[2][i] + b * (c11 * exx + c13 * ezz);
+    const float nzz = c1 * a.keep[3][i] + b * (c13 * exx + c33 * ezz);
+    const float nxz = c1 * a.keep[4][i] + b * c55 * exz;
+    // lambda_n = lambda_tau' + R^T lambda_sigma'
+    const float lxx = a.lam[5][i] + c2 * la + s2 * lb - 0.5f * st * le;
+    const float lzz = a.lam[6][i] + s2 * la + c2 * lb + 0.5f * st * le;
+    const float lxz = a.lam[7][i] + st * la - st * lb + cd * le;
+    a.acc[0][i] += b * lxx * exx;
+    a.acc[1][i] += b * (lxx * ezz + lzz * exx);
+    a.acc[2][i] += b * lzz * ezz;
+    a.acc[3][i] += b * lxz * exz;
+    // theta: through the strain rotation (d s2 = st, d c2 = -st, d st = 2 cd) and through R
+    const float dexx = st * (vzz - vxx) - cd * sh, dexz = 2.0f * cd * (vxx - vzz) - 2.0f * st * sh;
+    const float rxx_ = -st * nxx + st * nzz + 2.0f * cd * nxz, rxz_ = -cd * (nxx - nzz) - 2.0f * st * nxz;
+    a.acc[4][i] += lxx * b * (c11 - c13) * dexx + lzz * b * (c13 - c33) * dexx + lxz * b * c55 * dexz +
+                   (la - lb) * rxx_ + le * rxz_;
+    const float Lexx = b * (c11 * lxx + c13 * lzz), Lezz = b * (c13 * lxx + c33 * lzz), Lexz = b * c55 * lxz;
+    const float Lsh = 0.5f * st * (Lezz - Lexx) + cd * Lexz;
+    a.T[0][i] = c2 * Lexx + s2 * Lezz + st * Lexz;
+    a.T[1][i] = Lsh;
+    a.T[2][i] = Lsh;
+    a.T[3][i] = s2 * Lexx + c2 * Lezz - st * Lexz;
+    a.lam[5][i] = c1 * lxx;
+    a.lam[6][i] = c1 * lzz;
+    a.lam[7][i] = c1 * lxz;
+    a.lam[2][i] = a.lam[3][i] = a.lam[4][i] = 0.0f;  // sigma is overwritten by R tau
+    return;
+  }
   const float s = a.p.sn[i], co = a.p.cs[i];
   const float rxx = co * vxx - s * vxz, rxz = s * vxx + co * vxz;
   const float rzx = co * vzx - s * vzz, rzz = s * vzx + co * vzz;
@@ -247,8 +284,8 @@ __global__ void __launch_bounds__(BZ *BX) k_adj_velocity(AdjArgs a)
   const float br = a.p.coef2[i] * a.p.invrho[i];
   const float Fx = br * lx, Fz = br * lz;
   // coordinate: rotation by theta_v; Bond: fx = sxx_x + sxz_z, fz = sxz_x + szz_z
-  const float cv = V == TTI_BOND ? 1.0f : a.p.csv[i], sv = V == TTI_BOND ? 0.0f : a.p.snv[i];
-  if (V != TTI_BOND) {
+  const float cv = V != TTI_COORDINATE ? 1.0f : a.p.csv[i], sv = V != TTI_COORDINATE ? 0.0f : a.p.snv[i];
+  if (V == TTI_COORDINATE) {
     a.acc[5][i] += Fx * (sxz_x - sxx_z) + Fz * (szz_x - sxz_z);
     a.acc[6][i] += Fx * (sxx_x + sxz_z) + Fz * (sxz_x + szz_z);
   }
@@ -383,8 +420,8 @@ __global__ void __launch_bounds__(tiled::NT, 2) k_adj_velocity_tiled(const __gri
     const float2 cf = __ldg(at.pk.cf + i);
     const float br = cf.y * __ldg(a.p.invrho + i);
     const float Fx = br * lx, Fz = br * lz;
-    float sv = 0.0f, cv = 1.0f;  // Bond: fx = sxx_x + sxz_z, fz = sxz_x + szz_z
-    if (V != TTI_BOND) {
+    float sv = 0.0f, cv = 1.0f;  // tensor and Bond: fx = sxx_x + sxz_z, fz = sxz_x + szz_z
+    if (V == TTI_COORDINATE) {
       const float2 vsc = __ldg(at.pk.vsc + i);
       sv = vsc.x;
       cv = vsc.y;
@@ -536,7 +573,8 @@ __global__ void k_chain(Grid g, Params p, const float *vp, const float *vs, cons
   gs.out[0][i] = (float)((g11 * dc11 + g13 * dc13 + g33 * dc33) / B);
   gs.out[1][i] = (float)(g11 * 2.0 * R * P * P);
   gs.out[2][i] = (float)(q > 0.0 ? g13 * R * P * P * f / q : 0.0);
-  if (V == TTI_BOND) return;
+  if (V == TTI_TENSOR) gs.out[3][i] = (float)(gs.acc[4][i] * rad);  // no rotation at the velocity node
+  if (V != TTI_COORDINATE) return;
   double gt = gs.acc[4][i];
   const double sn = p.sn[i], cs = p.cs[i];
   for (int a = 0; a <= 1; ++a)
@@ -563,9 +601,6 @@ int gerr(tti_handle *h, int code, const char *msg) { return handle_error(h, code
 
 int grad_check(tti_handle *h)
 {
-  if (h->cfg.variant == TTI_TENSOR)
-    return gerr(h, TTI_ERR_ARG,
-                "the adjoint-state gradient is implemented for the coordinate and Bond formulations");
   if (h->cfg.variant == TTI_BOND && h->cfg.freesurface)
     return gerr(h, TTI_ERR_ARG, "the Bond gradient does not differentiate the free-surface stiffness rewrite");
   if (h->use_fused) return gerr(h, TTI_ERR_STATE, "the gradient runs on the tiled or per-cell kernels");
@@ -585,7 +620,7 @@ int grad_alloc(tti_handle *h)
     return cudaMemsetAsync(*p, 0, n * sizeof(float), h->stream) == cudaSuccess;
   };
   bool ok = true;
-  for (auto &p : s->lam) ok = ok && al(&p);
+  for (int k = 0; k < (h->cfg.variant == TTI_TENSOR ? 8 : 5); ++k) ok = ok && al(&s->lam[k]);
   for (auto &p : s->T) ok = ok && al(&p);
   for (auto &p : s->TV) ok = ok && al(&p);
   for (auto &p : s->acc) ok = ok && al(&p);
@@ -611,7 +646,7 @@ AdjArgs adj_args(tti_handle *h, int slot)
   AdjArgs a;
   a.g = h->g;
   a.p = handle_step_args(h).p;
-  for (int k = 0; k < 5; ++k) a.lam[k] = s->lam[k];
+  for (int k = 0; k < 8; ++k) a.lam[k] = s->lam[k];
   for (int k = 0; k < 4; ++k) a.T[k] = s->T[k];
   for (int k = 0; k < 6; ++k) a.TV[k] = s->TV[k];
   for (int k = 0; k < 7; ++k) a.acc[k] = s->acc[k];
@@ -659,6 +694,7 @@ int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
     // per-cell reads and writes, not by its two stencil fields
     const dim3 blk(BZ, BX), grd((g.Nz + BZ - 1) / BZ, (g.Nx + BX - 1) / BX);
     if (c.variant == TTI_BOND) k_adj_stress_local<TTI_BOND><<<grd, blk, 0, h->stream>>>(a);
+    else if (c.variant == TTI_TENSOR) k_adj_stress_local<TTI_TENSOR><<<grd, blk, 0, h->stream>>>(a);
     else k_adj_stress_local<TTI_COORDINATE><<<grd, blk, 0, h->stream>>>(a);
     AdjTile at;
     memset(&at, 0, sizeof at);
@@ -667,8 +703,10 @@ int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
     at.err = h->d_flag;
     for (int k = 0; k < 4; ++k) at.map[k] = s->maps[k];
     for (int f = 0; f < 3; ++f) at.map[4 + f] = s->slot_maps[(size_t)slot * 3 + f];  // kept sxx, szz, sxz
-    if (c.variant == TTI_BOND) GCK(h, launch_adj_tile(k_adj_velocity_tiled<TTI_BOND>, at, 7, g.izStart, g, h->stream));
-    else GCK(h, launch_adj_tile(k_adj_velocity_tiled<TTI_COORDINATE>, at, 7, g.izStart, g, h->stream));
+    if (c.variant == TTI_COORDINATE)
+      GCK(h, launch_adj_tile(k_adj_velocity_tiled<TTI_COORDINATE>, at, 7, g.izStart, g, h->stream));
+    else  // tensor and Bond: no rotation at the velocity node
+      GCK(h, launch_adj_tile(k_adj_velocity_tiled<TTI_BOND>, at, 7, g.izStart, g, h->stream));
     for (int k = 0; k < 6; ++k) at.map[k] = s->maps[4 + k];
     GCK(h, launch_adj_tile(k_adj_vstencil_tiled, at, 6, a.z_lo, g, h->stream));
     return TTI_OK;
@@ -677,6 +715,9 @@ int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
   if (c.variant == TTI_BOND) {
     k_adj_stress_local<TTI_BOND><<<grd, blk, 0, h->stream>>>(a);
     k_adj_velocity<TTI_BOND><<<grd, blk, 0, h->stream>>>(a);
+  } else if (c.variant == TTI_TENSOR) {
+    k_adj_stress_local<TTI_TENSOR><<<grd, blk, 0, h->stream>>>(a);
+    k_adj_velocity<TTI_BOND><<<grd, blk, 0, h->stream>>>(a);  // no rotation at the velocity node
   } else {
     k_adj_stress_local<TTI_COORDINATE><<<grd, blk, 0, h->stream>>>(a);
     k_adj_velocity<TTI_COORDINATE><<<grd, blk, 0, h->stream>>>(a);
@@ -765,13 +806,14 @@ int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
   const int nt = c.nt;
   ncheck = std::min(ncheck, nt);
   const int seg = (nt + ncheck - 1) / ncheck, nseg = (nt + seg - 1) / seg;
+  const int nf = h->cfg.variant == TTI_TENSOR ? 8 : 5;  // fields of a full state (checkpoints)
   const size_t n = h->g.n, state = 5 * n;
   if (s->ncheck != nseg || s->seg != seg) {
     cudaFree(s->ckpt);
     cudaFree(s->keep);
     s->ckpt = s->keep = nullptr;
     s->slot_maps_n = 0;  // the kept-state tensor maps point into the old buffer
-    if (cudaMalloc(&s->ckpt, sizeof(float) * state * std::max(1, nseg - 1)) != cudaSuccess ||
+    if (cudaMalloc(&s->ckpt, sizeof(float) * nf * n * std::max(1, nseg - 1)) != cudaSuccess ||
         cudaMalloc(&s->keep, sizeof(float) * state * seg) != cudaSuccess) {
       s->ncheck = s->seg = 0;
       return gerr(h, TTI_ERR_NOMEM, "device allocation of the checkpoints failed (use fewer steps per segment)");
@@ -809,8 +851,8 @@ int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
   for (int q = 0; q < nseg; ++q) {
     const bool last = q == nseg - 1;
     if (!last)
-      for (int f = 0; f < 5; ++f)
-        GCK(h, cudaMemcpyAsync(s->ckpt + ((size_t)q * 5 + f) * n, h->fld[f], n * sizeof(float),
+      for (int f = 0; f < nf; ++f)
+        GCK(h, cudaMemcpyAsync(s->ckpt + ((size_t)q * nf + f) * n, h->fld[f], n * sizeof(float),
                                cudaMemcpyDeviceToDevice, h->stream));
     for (int k = q * seg; k < std::min(nt, (q + 1) * seg); ++k) {
       float *keep[5];
@@ -830,14 +872,15 @@ int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
   double J = 0.0;
   GCK(h, cudaMemcpyAsync(&J, s->d_J, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   // adjoint, segment by segment from the last
-  for (auto p : s->lam) GCK(h, cudaMemsetAsync(p, 0, n * sizeof(float), h->stream));
+  for (auto p : s->lam)
+    if (p) GCK(h, cudaMemsetAsync(p, 0, n * sizeof(float), h->stream));
   for (auto p : s->T) GCK(h, cudaMemsetAsync(p, 0, n * sizeof(float), h->stream));
   for (auto p : s->TV) GCK(h, cudaMemsetAsync(p, 0, n * sizeof(float), h->stream));
   for (int q = nseg - 1; q >= 0; --q) {
     const int k0 = q * seg, k1 = std::min(nt, (q + 1) * seg);
     if (q < nseg - 1) {  // recompute the segment from its checkpoint
-      for (int f = 0; f < 5; ++f)
-        GCK(h, cudaMemcpyAsync(h->fld[f], s->ckpt + ((size_t)q * 5 + f) * n, n * sizeof(float),
+      for (int f = 0; f < nf; ++f)
+        GCK(h, cudaMemcpyAsync(h->fld[f], s->ckpt + ((size_t)q * nf + f) * n, n * sizeof(float),
                                cudaMemcpyDeviceToDevice, h->stream));
       h->step_index = k0;
       for (int k = k0; k < k1; ++k) {
@@ -866,7 +909,11 @@ int tti_grad_fetch(tti_handle *h, int which, float *out)
   const Grid &g = h->g;
   const dim3 blk(BZ, BX), grd((g.Nz + BZ - 1) / BZ, (g.Nx + BX - 1) / BX);
   const float *th = h->m_theta;
-  if (h->cfg.variant == TTI_BOND)
+  if (h->cfg.variant == TTI_TENSOR)
+    k_chain<TTI_TENSOR><<<grd, blk, 0, h->stream>>>(g, handle_step_args(h).p, h->par[TTI_P_VP], h->par[TTI_P_VS],
+                                                    h->par[TTI_P_RHO], h->par[TTI_P_BETA], h->m_eps, h->m_delta, th,
+                                                    *s, h->cfg.scalar);
+  else if (h->cfg.variant == TTI_BOND)
     k_chain<TTI_BOND><<<grd, blk, 0, h->stream>>>(g, handle_step_args(h).p, h->par[TTI_P_VP], h->par[TTI_P_VS],
                                                   h->par[TTI_P_RHO], h->par[TTI_P_BETA], h->m_eps, h->m_delta, th,
                                                   *s, h->cfg.scalar);

@@ -202,8 +202,10 @@ int launch_one_step(tti_handle *h, const SourceTables &tab, cudaEvent_t *ev = nu
   else launch_velocity(a, h->stream);
   if (ev) CK(h, cudaEventRecord(ev[1], h->stream));
   if (vsrc) launch_sources(a, s, &tab, c.stype, 0, it, h->stream);
-  if (keep) {
-    launch_copy5(h->fld, keep, h->g.n, h->stream);
+  if (keep) {  // vx vz, and sxx szz sxz (tensor: txx tzz txz, which the tensor adjoint reads)
+    const bool t = c.variant == TTI_TENSOR;
+    float *const src[5] = {h->fld[0], h->fld[1], h->fld[t ? 5 : 2], h->fld[t ? 6 : 3], h->fld[t ? 7 : 4]};
+    launch_copy5(src, keep, h->g.n, h->stream);
     h->launches++;
   }
   if (ev) CK(h, cudaEventRecord(ev[2], h->stream));
@@ -603,7 +605,7 @@ int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const floa
   }
   cudaStreamSynchronize(h->stream);
   // the gradient's chain rule needs epsilon and delta as given (and theta for Bond)
-  if (rc == TTI_OK && c.variant != TTI_TENSOR) {
+  if (rc == TTI_OK) {
     for (int k = 0; k < (c.variant == TTI_BOND ? 3 : 2); ++k) {
       float *&dst = k == 0 ? h->m_eps : k == 1 ? h->m_delta : h->m_theta;
       if (!dst && cudaMalloc(&dst, g.n * sizeof(float)) != cudaSuccess) {
