@@ -184,10 +184,9 @@ int tti_fetch_field(tti_handle *h, int which, float *out);
 int tti_fetch_energy(tti_handle *h, float *ek, float *ep);
 
 /* ---- Adjoint-state gradient ---------------------------------------------------
- * The reference has no adjoint; these entry points add one for the coordinate
- * and tensor-rotation formulations, and for the Bond formulation without free
- * surface (its free-surface stiffness rewrite, bond:543-568, is not
- * differentiated), with the stress source (stype 1). Misfit
+ * The reference has no adjoint; these entry points add one for all three
+ * formulations (for Bond through its free-surface stiffness rewrite,
+ * bond:543-568, too), with the stress source (stype 1). Misfit
  *   J = 1/2 sum over the recorded samples of (d - dobs)^2
  * (the components seistype records). tti_grad_run cuts the loop into
  * `ncheck` segments: a forward pass saves the state at each segment start

@@ -170,9 +170,8 @@ def _d(a):
 
 
 class AdjointOracle:
-    """Double-precision forward and adjoint-state gradient of the coordinate and
-    tensor-rotation formulations, or of the Bond formulation without free
-    surface (cfg variant; oracle/ttifd_adjoint.c), stress source only. MEAL coef1, coef2
+    """Double-precision forward and adjoint-state gradient of the three
+    formulations (cfg variant; oracle/ttifd_adjoint.c), stress source only. MEAL coef1, coef2
     and Beta are frozen from the float setup of `meal_model` (padded arrays);
     vs and rho stay fixed; the model (vp, eps, delta, theta) can be changed
     with set_model for finite differences."""
@@ -189,8 +188,6 @@ class AdjointOracle:
                                  c.get("freesurface", 0), c.get("mt", 1), c["seistype"], c.get("scalar", 1.0))
         variant = c.get("variant", 0)
         variant = ttifd.VARIANTS[variant] if isinstance(variant, str) else int(variant)
-        if variant == ttifd.BOND and c.get("freesurface", 0):
-            raise ValueError("the Bond gradient reference has no free surface")
         lib.adj_set_formulation(self._c, variant)
         nz, nx, nts = C.c_int(), C.c_int(), C.c_int()
         lib.adj_grid(self._c, C.byref(nz), C.byref(nx), C.byref(nts))

@@ -12,8 +12,8 @@
  * (sufdmod2dTTIelastic_tensor_rotation.c: tau update and sigma = R tau
  * :799-851, stiffness :498-519), and for the Bond-transformation
  * formulation (sufdmod2dTTIelastic_bond_transformation.c: velocity update
- * :654-703, stress update :836-873, stiffness :492-541; without the free
- * surface, whose stiffness rewrite :543-568 is not differentiated), so that
+ * :654-703, stress update :836-873, stiffness :492-541 and its free-surface
+ * rewrite :543-568), so that
  *   J = 1/2 sum over recorded samples (d - dobs)^2
  * has gradients with respect to vp, epsilon, delta and theta (degrees) at
  * every padded cell. Conventions: vs and rho are held fixed; the MEAL arrays
@@ -121,6 +121,34 @@ static void bond_moduli(double C11, double C13, double C33, double C55, double t
   out[5] = 0.25 * (C11 + C33 - 2.0 * C13) * s22 + C55 * c22;
 }
 
+/* Bond free-surface row (bond:543-568): the moduli a = (c11 c13 c15 c33 c35 c55)
+ * are replaced by an effective c11 (returned) and zeros; dc[k] = d c11'/d a[k]. */
+static double bond_fs_c11(const double a[6], double dc[6])
+{
+  const double a11 = a[0], a13 = a[1], a15 = a[2], a33 = a[3], a35 = a[4], a55 = a[5];
+  const double N = a13 * a55 - a15 * a35, D = a33 * a55 - a35 * a35;
+  double n35 = -N / D;
+  int fallback = !isfinite(n35);
+  if (fallback) n35 = -a13 / a33;
+  if (!isfinite(n35)) n35 = 0.0;
+  const double M = a13 * n35 - a15 * a33, Q = a33 * a55 - n35 * n35, n55 = M / Q;
+  for (int v = 0; v < 6; ++v) {  /* one-hot forward derivatives */
+    const double d11 = v == 0, d13 = v == 1, d15 = v == 2, d33 = v == 3, d35 = v == 4, d55 = v == 5;
+    double dn35;
+    if (!fallback) {
+      const double dN = d13 * a55 + a13 * d55 - d15 * a35 - a15 * d35, dD = d33 * a55 + a33 * d55 - 2.0 * a35 * d35;
+      dn35 = -(dN * D - N * dD) / (D * D);
+    } else {
+      dn35 = isfinite(-a13 / a33) ? -(d13 * a33 - a13 * d33) / (a33 * a33) : 0.0;
+    }
+    const double dM = d13 * n35 + a13 * dn35 - d15 * a33 - a15 * d33;
+    const double dQ = d33 * a55 + a33 * d55 - 2.0 * n35 * dn35;
+    const double dn55 = (dM * Q - M * dQ) / (Q * Q);
+    dc[v] = d11 - d13 * n35 - a13 * dn35 + d15 * n55 + a15 * dn55;
+  }
+  return a11 - a13 * n35 + a15 * n55;
+}
+
 /* derivatives of bond_moduli: d[m][0..5] = d(c11..c55)/d(C11, C13, C33, theta)[m] */
 static void bond_moduli_grad(double C11, double C13, double C33, double C55, double th, double d[4][6])
 {
@@ -185,6 +213,11 @@ void adj_set_model(adj_ctx *c, const double *vp, const double *vs, const double 
       c->c33[i] = m[3];
       c->c35[i] = m[4];
       c->c55[i] = m[5];
+      if (c->fs && (int)(i % (size_t)c->Nz) == c->E) {  /* the free-surface row */
+        double dc[6];
+        c->c11[i] = bond_fs_c11(m, dc);
+        c->c13[i] = c->c15[i] = c->c33[i] = c->c35[i] = c->c55[i] = 0.0;
+      }
     }
     c->sn[i] = sin(th);
     c->cs[i] = cos(th);
@@ -686,7 +719,14 @@ double adj_gradient(adj_ctx *c, const double *dobs[3], double *g_vp, double *g_e
                      C55 = r * s * s;
         double dm[4][6];
         bond_moduli_grad(C11, C13, C33, C55, th, dm);
-        const double gm[6] = {gc11[i], gc13[i], gc15[i], gc33[i], gc35[i], gc55[i]};
+        double gm[6] = {gc11[i], gc13[i], gc15[i], gc33[i], gc35[i], gc55[i]};
+        if (c->fs && iz == c->E) {  /* only the effective c11 acts on the free-surface row */
+          double m[6], dc[6];
+          bond_moduli(C11, C13, C33, C55, th, m);
+          bond_fs_c11(m, dc);
+          const double g = gc11[i];
+          for (int k = 0; k < 6; ++k) gm[k] = g * dc[k];
+        }
         G11 = G13 = G33 = 0.0;
         double gt = 0.0;
         for (int k = 0; k < 6; ++k) {

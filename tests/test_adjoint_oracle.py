@@ -28,7 +28,7 @@ def _setup(fs, seed=5, variant="coordinate_rotation"):
 
 
 CASES = [(0, "coordinate_rotation"), (1, "coordinate_rotation"), (0, "bond_transformation"),
-         (0, "tensor_rotation"), (1, "tensor_rotation")]
+         (1, "bond_transformation"), (0, "tensor_rotation"), (1, "tensor_rotation")]
 
 
 @pytest.mark.parametrize("fs,variant", CASES)
@@ -82,3 +82,29 @@ def test_gradient_matches_central_differences(fs, variant):
         scale = {n: max(abs(c[4]) for c in checks if c[0] == n) for n in ("vp", "eps", "delta", "theta")}
         for name, ix, iz, fd, an in checks:
             assert abs(fd - an) <= 1e-3 * max(abs(an), 1e-2 * scale[name]), (name, ix, iz, fd, an)
+
+
+def test_bond_free_surface_row_gradient():
+    """On the free-surface row the Bond moduli are replaced by an effective c11
+    (bond:543-568); the gradient there goes through that rewrite."""
+    cfg, adj, pads, w = _setup(1, variant="bond_transformation")
+    E = cfg["ealThick"] + 5
+    with adj:
+        true = [np.array(a, dtype=np.float64) for a in pads]
+        true[0][E + 10:E + 30, E:E + 6] *= 1.05
+        true[5][E + 10:E + 30, E:E + 6] += 8.0
+        adj.set_model(*true)
+        dobs = adj.forward()
+        start = [np.array(a, dtype=np.float64) for a in pads]
+        adj.set_model(*start)
+        _, g, _ = adj.gradient(dobs)
+        for name, idx, h in (("vp", 0, 1e-3), ("eps", 3, 1e-3), ("theta", 5, 1e-2)):
+            for ix in (E + 18, E + 27):
+                step = h * (start[0][ix, E] if name == "vp" else 1.0)
+                mp = [a.copy() for a in start]
+                mm = [a.copy() for a in start]
+                mp[idx][ix, E] += step
+                mm[idx][ix, E] -= step
+                fd = (_misfit(adj, mp, dobs) - _misfit(adj, mm, dobs)) / (2 * step)
+                an = g[name][ix, E]
+                assert abs(fd - an) <= 1e-3 * abs(an) and abs(an) > 0, (name, ix, fd, an)

@@ -50,8 +50,8 @@ def _rel(a, b):
 
 @pytest.mark.parametrize("kernel", ["tiled", "naive"])
 @pytest.mark.parametrize("fs,variant", [(0, "coordinate_rotation"), (1, "coordinate_rotation"),
-                                        (0, "bond_transformation"), (0, "tensor_rotation"),
-                                        (1, "tensor_rotation")])
+                                        (0, "bond_transformation"), (1, "bond_transformation"),
+                                        (0, "tensor_rotation"), (1, "tensor_rotation")])
 def test_gradient_matches_cpu_reference(fs, variant, kernel, monkeypatch, gpu_lib):
     """Both adjoint paths: TMA-tiled (default) and one thread per cell (TTIFD_KERNEL=naive)."""
     if kernel == "naive":
@@ -129,12 +129,11 @@ def test_device_dot_product(gpu_lib):
     assert abs(lhs - rhs) <= 2e-4 * abs(lhs), (lhs, rhs)
 
 
-@pytest.mark.parametrize("variant,fs", [("bond_transformation", 1)])
-def test_gradient_rejects_unsupported_cases(variant, fs, gpu_lib):
-    """No Bond gradient with the free-surface stiffness rewrite."""
+def test_gradient_rejects_velocity_sources(gpu_lib):
+    """The gradient models the stress source only (stype 1)."""
     import ttifd
 
-    with ttifd.Modeling(stype=1, **dict(CFG, variant=variant, freesurface=fs)) as h:
+    with ttifd.Modeling(stype=2, **dict(CFG, variant="coordinate_rotation")) as h:
         with pytest.raises(ttifd.TTIError) as e:
             h.grad_zero()
         assert e.value.code == ttifd.ERR_ARG

@@ -539,10 +539,37 @@ __device__ void bond_moduli_grad(double C11, double C13, double C33, double C55,
     for (int k = 0; k < 6; ++k) d[m][k] = rows[m][k];
 }
 
+// Bond free-surface row (bond:543-568): the moduli a = (c11 c13 c15 c33 c35 c55)
+// act only through the effective c11' = a11 - a13 n35 + a15 n55; dc[k] = dc11'/da[k].
+__device__ void bond_fs_c11_grad(const double a[6], double dc[6])
+{
+  const double a13 = a[1], a15 = a[2], a33 = a[3], a35 = a[4], a55 = a[5];
+  const double N = a13 * a55 - a15 * a35, D = a33 * a55 - a35 * a35;
+  double n35 = -N / D;
+  const bool fallback = !isfinite(n35);
+  if (fallback) n35 = -a13 / a33;
+  if (!isfinite(n35)) n35 = 0.0;
+  const double M = a13 * n35 - a15 * a33, Q = a33 * a55 - n35 * n35, n55 = M / Q;
+  for (int v = 0; v < 6; ++v) {  // one-hot forward derivatives
+    const double d11 = v == 0, d13 = v == 1, d15 = v == 2, d33 = v == 3, d35 = v == 4, d55 = v == 5;
+    double dn35;
+    if (!fallback) {
+      const double dN = d13 * a55 + a13 * d55 - d15 * a35 - a15 * d35, dD = d33 * a55 + a33 * d55 - 2.0 * a35 * d35;
+      dn35 = -(dN * D - N * dD) / (D * D);
+    } else {
+      dn35 = isfinite(-a13 / a33) ? -(d13 * a33 - a13 * d33) / (a33 * a33) : 0.0;
+    }
+    const double dM = d13 * n35 + a13 * dn35 - d15 * a33 - a15 * d33;
+    const double dQ = d33 * a55 + a33 * d55 - 2.0 * n35 * dn35;
+    dc[v] = d11 - d13 * n35 - a13 * dn35 + d15 * n55 + a15 * (dM * Q - M * dQ) / (Q * Q);
+  }
+}
+
 // chain rule to vp, epsilon, delta, theta (degrees), every cell
 template <int V>
 __global__ void k_chain(Grid g, Params p, const float *vp, const float *vs, const float *rho, const float *beta,
-                        const float *eps, const float *delta, const float *theta, GradState gs, float scalar)
+                        const float *eps, const float *delta, const float *theta, GradState gs, float scalar,
+                        int freesurface)
 {
   const float rad = (float)(scalar * M_PI / 180.0);
   const int iz = blockIdx.x * BZ + threadIdx.x, ix = blockIdx.y * BX + threadIdx.y;
@@ -559,7 +586,21 @@ __global__ void k_chain(Grid g, Params p, const float *vp, const float *vs, cons
     double dm[4][6];
     const double th = scalar * (double)theta[i] / 180.0 * M_PI;
     bond_moduli_grad(C11, C13, C33, C55, th, dm);
-    const double gm[6] = {gs.acc[0][i], gs.acc[1][i], gs.acc[4][i], gs.acc[2][i], gs.acc[5][i], gs.acc[3][i]};
+    double gm[6] = {gs.acc[0][i], gs.acc[1][i], gs.acc[4][i], gs.acc[2][i], gs.acc[5][i], gs.acc[3][i]};
+    if (freesurface && iz == g.E) {  // only the effective c11 acts on the free-surface row
+      const double s2 = sin(th) * sin(th), c2 = cos(th) * cos(th), s4 = s2 * s2, c4 = c2 * c2;
+      const double s2t = sin(2.0 * th), c2t = cos(2.0 * th), s22 = s2t * s2t, c22 = c2t * c2t;
+      const double m[6] = {C11 * c4 + C33 * s4 + (0.5 * C13 + C55) * s22,
+                           (0.25 * (C11 + C33) - C55) * s22 + C13 * (s4 + c4),
+                           0.5 * (-C11 * c2 + C33 * s2 + (C13 + 2.0 * C55) * c2t) * s2t,
+                           C11 * s4 + C33 * c4 + (0.5 * C13 + C55) * s22,
+                           0.5 * (-C11 * s2 + C33 * c2 - (C13 + 2.0 * C55) * c2t) * s2t,
+                           0.25 * (C11 + C33 - 2.0 * C13) * s22 + C55 * c22};
+      double dc[6];
+      bond_fs_c11_grad(m, dc);
+      const double g11_ = gm[0];
+      for (int k = 0; k < 6; ++k) gm[k] = g11_ * dc[k];
+    }
     g11 = g13 = g33 = 0.0;
     double gt = 0.0;
     for (int k = 0; k < 6; ++k) {
@@ -601,11 +642,9 @@ int gerr(tti_handle *h, int code, const char *msg) { return handle_error(h, code
 
 int grad_check(tti_handle *h)
 {
-  if (h->cfg.variant == TTI_BOND && h->cfg.freesurface)
-    return gerr(h, TTI_ERR_ARG, "the Bond gradient does not differentiate the free-surface stiffness rewrite");
   if (h->use_fused) return gerr(h, TTI_ERR_STATE, "the gradient runs on the tiled or per-cell kernels");
-  if (!h->have_model || !h->m_eps) return gerr(h, TTI_ERR_STATE, "model not uploaded");
   if (h->cfg.stype != 1) return gerr(h, TTI_ERR_ARG, "the gradient models the stress source (stype = 1)");
+  if (!h->have_model || !h->m_eps) return gerr(h, TTI_ERR_STATE, "model not uploaded");
   return TTI_OK;
 }
 
@@ -912,15 +951,15 @@ int tti_grad_fetch(tti_handle *h, int which, float *out)
   if (h->cfg.variant == TTI_TENSOR)
     k_chain<TTI_TENSOR><<<grd, blk, 0, h->stream>>>(g, handle_step_args(h).p, h->par[TTI_P_VP], h->par[TTI_P_VS],
                                                     h->par[TTI_P_RHO], h->par[TTI_P_BETA], h->m_eps, h->m_delta, th,
-                                                    *s, h->cfg.scalar);
+                                                    *s, h->cfg.scalar, h->cfg.freesurface);
   else if (h->cfg.variant == TTI_BOND)
     k_chain<TTI_BOND><<<grd, blk, 0, h->stream>>>(g, handle_step_args(h).p, h->par[TTI_P_VP], h->par[TTI_P_VS],
                                                   h->par[TTI_P_RHO], h->par[TTI_P_BETA], h->m_eps, h->m_delta, th,
-                                                  *s, h->cfg.scalar);
+                                                  *s, h->cfg.scalar, h->cfg.freesurface);
   else
     k_chain<TTI_COORDINATE><<<grd, blk, 0, h->stream>>>(g, handle_step_args(h).p, h->par[TTI_P_VP],
                                                         h->par[TTI_P_VS], h->par[TTI_P_RHO], h->par[TTI_P_BETA],
-                                                        h->m_eps, h->m_delta, th, *s, h->cfg.scalar);
+                                                        h->m_eps, h->m_delta, th, *s, h->cfg.scalar, h->cfg.freesurface);
   h->launches++;
   GCK(h, cudaGetLastError());
   GCK(h, cudaMemcpy2DAsync(out, (size_t)g.Nz * sizeof(float), s->out[which], (size_t)g.ldz * sizeof(float),
