@@ -98,70 +98,79 @@ __device__ __forceinline__ bool interior(const Grid &g, int ix, int iz)
   return ix >= NH && ix < g.Nx - NH && iz >= g.izStart && iz < g.Nz - NH;
 }
 
-// residual injection (adjoint of the receiver sampling), blockIdx.y = component
-struct Inject {
-  const int *rx[3], *rz[3];
-  const float *res[3];  // this step's residual row of each component (null: not recorded)
-  int n[3];
-};
-__global__ void k_inject(Grid g, AdjArgs a, Inject in)
-{
-  const int k = blockIdx.y, t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (!in.res[k] || t >= in.n[k]) return;
-  const size_t c = (size_t)in.rx[k][t] * g.ldz + in.rz[k][t];
-  const float r = in.res[k][t];
-  if (k == TTI_REC_VX) atomicAdd(a.lam[0] + c, r);
-  else if (k == TTI_REC_VZ) atomicAdd(a.lam[1] + c, r);
-  else {
-    atomicAdd(a.lam[2] + c, 0.5f * r);
-    atomicAdd(a.lam[3] + c, 0.5f * r);
-  }
-}
-
-// dJ/d(source sample): adjoint of the stress source, one block per source
+// the stress-source weights 0.5 w over the 11 x 11 window
 struct K1 {
   float k1[121];
 };
-__global__ void k_source_grad(Grid g, AdjArgs a, SourceSet s, K1 tab, float *gsrc, int it)
+// The column work of a reverse step, one warp per padded-grid column, in the
+// order the step needs it: residual injection at the column's receivers (the
+// adjoint of isoelastic.c:103-144), this column's part of dJ/d(source sample)
+// (the adjoint of the stress source, read before the free surface as the
+// source is added after it), then the adjoint of the free-surface image.
+struct SurfaceArgs {
+  Grid g;
+  float *lam[8];
+  const int *colptr[3], *rzs[3], *rid[3];  // receivers by column
+  const float *res[3];                     // this step's residual rows (null: nothing to inject)
+  int nrec[3];
+  SourceSet src;
+  K1 k1;
+  float *gsrc;  // [nsrc][nt], summed over columns
+  int it, fs, tensor;
+};
+
+__global__ void k_adj_surface(SurfaceArgs a)
 {
-  __shared__ float part[128];
-  const int n = blockIdx.x, t = threadIdx.x;
-  float v = 0.0f;
-  if (t < 121) {
-    const int ix = s.x[n] + t / 11 - NH, iz = s.z[n] + t % 11 - NH;
-    if (ix >= 0 && ix < g.Nx && iz >= 0 && iz < g.Nz) {
-      const size_t c = (size_t)ix * g.ldz + iz;
-      v = tab.k1[t] * (a.lam[2][c] + a.lam[3][c]);
-      if (a.lam[5]) v += tab.k1[t] * (a.lam[5][c] + a.lam[6][c]);  // tensor: the source also adds to tau
+  const Grid &g = a.g;
+  const int lane = threadIdx.x & 31;
+  const int ix = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (ix >= g.Nx) return;
+  const size_t col = (size_t)ix * g.ldz;
+  for (int k = 0; k < 3; ++k) {
+    if (!a.res[k]) continue;
+    for (int j = a.colptr[k][ix] + lane; j < a.colptr[k][ix + 1]; j += 32) {
+      const size_t c = col + a.rzs[k][j];
+      const float r = a.res[k][a.rid[k][j]];
+      if (k == TTI_REC_VX) atomicAdd(a.lam[0] + c, r);
+      else if (k == TTI_REC_VZ) atomicAdd(a.lam[1] + c, r);
+      else {
+        atomicAdd(a.lam[2] + c, 0.5f * r);
+        atomicAdd(a.lam[3] + c, 0.5f * r);
+      }
     }
   }
-  part[t] = v;
-  __syncthreads();
-  for (int o = 64; o > 0; o >>= 1) {
-    if (t < o) part[t] += part[t + o];
-    __syncthreads();
+  __syncwarp();
+  for (int n = 0; n < a.src.n; ++n) {
+    const int dx = ix - a.src.x[n];
+    if (dx < -NH || dx > NH) continue;
+    const int iz = a.src.z[n] + lane - NH;
+    float v = 0.0f;
+    if (lane <= 2 * NH && iz >= 0 && iz < g.Nz) {
+      const size_t c = col + iz;
+      float l = a.lam[2][c] + a.lam[3][c];
+      if (a.tensor) l += a.lam[5][c] + a.lam[6][c];  // the source also adds to tau
+      v = a.k1.k1[(dx + NH) * 11 + lane] * l;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) atomicAdd(a.gsrc + (size_t)n * a.src.nt + a.it, v);
   }
-  if (t == 0) gsrc[(size_t)n * s.nt + it] = part[0];
-}
-
-// adjoint of the free-surface image (one thread per column)
-__global__ void k_adj_free_surface(Grid g, AdjArgs a)
-{
-  const int ix = NH + blockIdx.x * blockDim.x + threadIdx.x;
-  if (ix >= g.Nx - NH) return;
-  const size_t c = (size_t)ix * g.ldz + g.izStart;
-  float *xx = a.lam[2], *zz = a.lam[3], *xz = a.lam[4];
-  for (int k = 1; k <= NH; ++k) {
-    xx[c] += 2.0f * xx[c - k];
-    xx[c + k] -= xx[c - k];
-    xx[c - k] = 0.0f;
-    zz[c + k] -= zz[c - k];
-    zz[c - k] = 0.0f;
-    xz[c + k] -= xz[c - k];
-    xz[c - k] = 0.0f;
+  __syncwarp();
+  if (a.fs && lane == 0 && ix >= NH && ix < g.Nx - NH) {
+    const size_t c = col + g.izStart;
+    float *xx = a.lam[2], *zz = a.lam[3], *xz = a.lam[4];
+    for (int k = 1; k <= NH; ++k) {
+      xx[c] += 2.0f * xx[c - k];
+      xx[c + k] -= xx[c - k];
+      xx[c - k] = 0.0f;
+      zz[c + k] -= zz[c - k];
+      zz[c - k] = 0.0f;
+      xz[c + k] -= xz[c - k];
+      xz[c - k] = 0.0f;
+    }
+    xz[c] = 0.0f;
+    zz[c] = 0.0f;
   }
-  xz[c] = 0.0f;
-  zz[c] = 0.0f;
 }
 
 // stress-half adjoint, local part: gradient sums, T0..T3, lambda_sigma *= coef1
@@ -704,30 +713,33 @@ int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
   const int it = c.mode == 2 ? c.nt - 1 - n : n;
   const AdjArgs a = adj_args(h, slot);
   const Grid &g = h->g;
-  if (c.seistype > 0 && it % c.mt == 0) {
-    Inject in;
-    int nmax = 0;
+  {  // injection, source gradient and free-surface adjoint: one column-parallel launch
+    SurfaceArgs sa;
+    memset(&sa, 0, sizeof sa);
+    sa.g = g;
+    for (int k = 0; k < 8; ++k) sa.lam[k] = a.lam[k];
+    const bool inject = c.seistype > 0 && it % c.mt == 0;
+    bool any = false;
     for (int k = 0; k < 3; ++k) {
-      const bool on = s->res[k] && h->nrec[k] > 0;
-      in.rx[k] = h->d_rx[k];
-      in.rz[k] = h->d_rz[k];
-      in.res[k] = on ? s->res[k] + (size_t)(it / c.mt) * h->nrec[k] : nullptr;
-      in.n[k] = on ? h->nrec[k] : 0;
-      nmax = std::max(nmax, in.n[k]);
+      const bool on = inject && s->res[k] && h->nrec[k] > 0;
+      sa.colptr[k] = h->d_rcol[k];
+      sa.rzs[k] = h->d_rzs[k];
+      sa.rid[k] = h->d_rid[k];
+      sa.res[k] = on ? s->res[k] + (size_t)(it / c.mt) * h->nrec[k] : nullptr;
+      any = any || on;
     }
-    if (nmax > 0) {
-      k_inject<<<dim3((nmax + 127) / 128, 3), 128, 0, h->stream>>>(g, a, in);
+    sa.src = SourceSet{h->nsrc, h->d_sx, h->d_sz, h->d_src, c.nt};
+    memcpy(sa.k1.k1, tab.k1, sizeof sa.k1.k1);
+    sa.gsrc = s->gsrc;
+    sa.it = it;
+    sa.fs = c.freesurface == 1;
+    sa.tensor = c.variant == TTI_TENSOR;
+    if (any || h->nsrc > 0 || sa.fs) {
+      k_adj_surface<<<(g.Nx + 3) / 4, 128, 0, h->stream>>>(sa);
       h->launches++;
     }
   }
-  if (h->nsrc > 0) {
-    K1 k1;
-    memcpy(k1.k1, tab.k1, sizeof k1.k1);
-    k_source_grad<<<h->nsrc, 128, 0, h->stream>>>(g, a, SourceSet{h->nsrc, h->d_sx, h->d_sz, h->d_src, c.nt}, k1,
-                                                   s->gsrc, it);
-  }
-  if (c.freesurface == 1) k_adj_free_surface<<<(g.Nx + 127) / 128, 128, 0, h->stream>>>(g, a);
-  h->launches += 3 + (c.freesurface == 1) + (h->nsrc > 0);
+  h->launches += 3;
   if (h->use_tiled) {  // TMA halo tiles (the per-cell kernels below serve TTIFD_KERNEL=naive)
     // the stress-half adjoint stays one thread per cell: it is bound by its
     // per-cell reads and writes, not by its two stencil fields
@@ -914,6 +926,7 @@ int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
   for (auto p : s->lam)
     if (p) GCK(h, cudaMemsetAsync(p, 0, n * sizeof(float), h->stream));
   for (auto p : s->T) GCK(h, cudaMemsetAsync(p, 0, n * sizeof(float), h->stream));
+  if (s->gsrc) GCK(h, cudaMemsetAsync(s->gsrc, 0, sizeof(float) * (size_t)s->gsrc_n, h->stream));
   for (auto p : s->TV) GCK(h, cudaMemsetAsync(p, 0, n * sizeof(float), h->stream));
   for (int q = nseg - 1; q >= 0; --q) {
     const int k0 = q * seg, k1 = std::min(nt, (q + 1) * seg);
