@@ -121,6 +121,7 @@ struct SurfaceArgs {
 
 __global__ void k_adj_surface(SurfaceArgs a)
 {
+  pdl_sync();
   const Grid &g = a.g;
   const int lane = threadIdx.x & 31;
   const int ix = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -177,6 +178,7 @@ __global__ void k_adj_surface(SurfaceArgs a)
 template <int V>
 __global__ void __launch_bounds__(BZ *BX) k_adj_stress_local(AdjArgs a)
 {
+  pdl_sync();
   const Grid &g = a.g;
   const int iz = blockIdx.x * BZ + threadIdx.x, ix = blockIdx.y * BX + threadIdx.y;
   if (!interior(g, ix, iz)) return;
@@ -391,6 +393,7 @@ __device__ __forceinline__ void vpair(const float *q, float &d1, float &d2)
 template <int V>
 __global__ void __launch_bounds__(tiled::NT, 2) k_adj_velocity_tiled(const __grid_constant__ AdjTile at)
 {
+  pdl_sync();
   constexpr int F = tiled::FIELD, B = tiled::BZ;
   extern __shared__ __align__(128) float sm[];
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm + 7 * F);
@@ -454,6 +457,7 @@ __global__ void __launch_bounds__(tiled::NT, 2) k_adj_velocity_tiled(const __gri
 // transposed velocity stencils into lambda_sigma (maps: TV0..TV5), rows from z_lo
 __global__ void __launch_bounds__(tiled::NT, 2) k_adj_vstencil_tiled(const __grid_constant__ AdjTile at)
 {
+  pdl_sync();
   constexpr int F = tiled::FIELD, B = tiled::BZ;
   extern __shared__ __align__(128) float sm[];
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm + 6 * F);
@@ -507,8 +511,8 @@ cudaError_t launch_adj_tile(K kernel, const AdjTile &at, int nfields, int z_firs
   b.z_base = z_first & ~31;  // 32-row aligned: a warp's rows are one 128-byte line
   const int nz = g.Nz - NH - b.z_base, nx = g.Nx - 2 * NH;
   if (nz <= 0 || nx <= 0) return cudaSuccess;
-  kernel<<<dim3((nz + tiled::TZ - 1) / tiled::TZ, (nx + tiled::TX - 1) / tiled::TX), tiled::NT, bytes, st>>>(b);
-  return cudaGetLastError();
+  return launch_pdl(kernel, dim3((nz + tiled::TZ - 1) / tiled::TZ, (nx + tiled::TX - 1) / tiled::TX), dim3(tiled::NT),
+                    bytes, st, b);
 }
 
 // residuals d - dobs (time-major) and J
@@ -735,7 +739,7 @@ int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
     sa.fs = c.freesurface == 1;
     sa.tensor = c.variant == TTI_TENSOR;
     if (any || h->nsrc > 0 || sa.fs) {
-      k_adj_surface<<<(g.Nx + 3) / 4, 128, 0, h->stream>>>(sa);
+      GCK(h, launch_pdl(k_adj_surface, dim3((g.Nx + 3) / 4), dim3(128), 0, h->stream, sa));
       h->launches++;
     }
   }
@@ -744,9 +748,9 @@ int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
     // the stress-half adjoint stays one thread per cell: it is bound by its
     // per-cell reads and writes, not by its two stencil fields
     const dim3 blk(BZ, BX), grd((g.Nz + BZ - 1) / BZ, (g.Nx + BX - 1) / BX);
-    if (c.variant == TTI_BOND) k_adj_stress_local<TTI_BOND><<<grd, blk, 0, h->stream>>>(a);
-    else if (c.variant == TTI_TENSOR) k_adj_stress_local<TTI_TENSOR><<<grd, blk, 0, h->stream>>>(a);
-    else k_adj_stress_local<TTI_COORDINATE><<<grd, blk, 0, h->stream>>>(a);
+    if (c.variant == TTI_BOND) GCK(h, launch_pdl(k_adj_stress_local<TTI_BOND>, grd, blk, 0, h->stream, a));
+    else if (c.variant == TTI_TENSOR) GCK(h, launch_pdl(k_adj_stress_local<TTI_TENSOR>, grd, blk, 0, h->stream, a));
+    else GCK(h, launch_pdl(k_adj_stress_local<TTI_COORDINATE>, grd, blk, 0, h->stream, a));
     AdjTile at;
     memset(&at, 0, sizeof at);
     at.a = a;

@@ -364,6 +364,7 @@ __device__ void post_column(const Grid &g, const Fields &f, const PostArgs &p, i
 
 __global__ void k_post(Grid g, Fields f, PostArgs p)
 {
+  pdl_sync();
   const int ix = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (ix >= g.Nx) return;
   post_column(g, f, p, ix, p.it, p.irec);
@@ -454,7 +455,7 @@ void launch_energy(const StepArgs &a, int nz, int nx, double *out2, cudaStream_t
 
 void launch_post(const StepArgs &a, const PostArgs &p, cudaStream_t st)
 {
-  k_post<<<(a.g.Nx + 3) / 4, 128, 0, st>>>(a.g, a.f, p);  // 4 columns (warps) per block
+  launch_pdl(k_post, dim3((a.g.Nx + 3) / 4), dim3(128), 0, st, a.g, a.f, p);  // 4 columns (warps) per block
 }
 
 void launch_post_batch(const BatchPost *d, int n, int maxNx, const int *step, cudaStream_t st)
@@ -474,6 +475,7 @@ struct Copy5 {
 };
 __global__ void k_copy5(Copy5 c, size_t n4)
 {
+  pdl_sync();
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n4; q += (size_t)gridDim.x * blockDim.x) {
 #pragma unroll
     for (int f = 0; f < 5; ++f) c.dst[f][q] = c.src[f][q];
@@ -488,7 +490,7 @@ void launch_copy5(float *const *src, float *const *dst, size_t n, cudaStream_t s
     c.dst[f] = reinterpret_cast<float4 *>(dst[f]);
   }
   const size_t n4 = n / 4;
-  k_copy5<<<(unsigned)std::min<size_t>((n4 + 255) / 256, 148 * 16), 256, 0, st>>>(c, n4);
+  launch_pdl(k_copy5, dim3((unsigned)std::min<size_t>((n4 + 255) / 256, 148 * 16)), dim3(256), 0, st, c, n4);
 }
 
 // Receivers r0 .. r0 + nr - 1 of the time-major [nts][n] block, transposed to

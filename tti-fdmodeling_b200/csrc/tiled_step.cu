@@ -276,6 +276,7 @@ template <int V, bool X, bool Q>
 __global__ void __launch_bounds__(NT, 4) k_velocity_tiled(const __grid_constant__ HalfArgs a)
 {
   extern __shared__ __align__(128) float sm[];
+  pdl_sync();
   velocity_tile<V, X, Q>(a, a.map, sm, blockIdx.x, blockIdx.y);
 }
 
@@ -283,6 +284,7 @@ template <int V, bool X, bool Q>
 __global__ void __launch_bounds__(NT, 4) k_stress_tiled(const __grid_constant__ HalfArgs a)
 {
   extern __shared__ __align__(128) float sm[];
+  pdl_sync();
   stress_tile<V, X, Q>(a, a.map, sm, blockIdx.x, blockIdx.y);
 }
 
@@ -341,8 +343,7 @@ cudaError_t launch_k(K kernel, const HalfArgs &a, int nfields, cudaStream_t st)
   HalfArgs b = a;
   const dim3 gr = grid(a.g, &b.z_base);
   if (gr.x == 0 || gr.y == 0) return cudaSuccess;
-  kernel<<<gr, NT, bytes, st>>>(b);
-  return cudaGetLastError();
+  return launch_pdl(kernel, gr, dim3(NT), bytes, st, b);
 }
 
 }  // namespace

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdlib.h>
 
 #include <string>
 
@@ -20,6 +21,43 @@ __host__ __device__ __forceinline__ constexpr float rsg(int k)
          : k == 2 ? 0.0272965993810630f
          : k == 3 ? -0.00699199493927320f
                   : 0.00132022981661381f;
+}
+
+// Programmatic dependent launch. A kernel launched with launch_pdl may be
+// scheduled while the kernel before it in the stream is still draining; it
+// calls pdl_sync() before touching any memory, which signals that its own
+// dependents may be scheduled and then waits until the previous kernel has
+// completed and its writes are visible. Without the launch attribute both
+// instructions do nothing. TTIFD_PDL=0 launches normally.
+__device__ __forceinline__ void pdl_sync()
+{
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+inline bool pdl_enabled()
+{
+  static const bool on = [] {
+    const char *e = getenv("TTIFD_PDL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args... args)
+{
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
 // Device grid description. Arrays are column-major in x: element (ix, iz) at
