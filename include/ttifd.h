@@ -186,7 +186,9 @@ int tti_fetch_energy(tti_handle *h, float *ek, float *ep);
 /* ---- Adjoint-state gradient ---------------------------------------------------
  * The reference has no adjoint; these entry points add one for all three
  * formulations (for Bond through its free-surface stiffness rewrite,
- * bond:543-568, too), with the stress source (stype 1). Misfit
+ * bond:543-568, too) and every source type: the source tables do not depend
+ * on the model, so stype only changes the forward replay and the source
+ * gradient. Misfit
  *   J = 1/2 sum over the recorded samples of (d - dobs)^2
  * (the components seistype records). tti_grad_run cuts the loop into
  * `ncheck` segments: a forward pass saves the state at each segment start
@@ -208,7 +210,11 @@ int tti_grad_zero(tti_handle *h);
 /* tti_elapsed_ms afterwards gives the device time of the whole run. */
 int tti_grad_run(tti_handle *h, int ncheck, double *misfit);
 int tti_grad_fetch(tti_handle *h, int which, float *out);
-/* dJ/d(source samples) of the last run, [nsrc][nt]. */
+/* dJ/d(source samples) of the last run, [nsrc][nt]: the stress source
+ * (stype 1) reads the adjoint stresses after the residual injection; the
+ * velocity sources (stype 2-8, coord:674-802) read the adjoint velocities
+ * between the stress-half and velocity-half adjoints, with the window cells
+ * outside the velocity update accumulating their own adjoint. */
 int tti_grad_fetch_source(tti_handle *h, float *out);
 /* Device pointers of the 7 gradient sums (c11, c13, c33, c55, theta at the
  * stress node, sin/cos theta at the velocity node), each `count` floats of

@@ -156,6 +156,7 @@ _ADJ_SIG = {
     "adj_destroy": (None, [C.c_void_p]),
     "adj_grid": (None, [C.c_void_p, _IP, _IP, _IP]),
     "adj_set_formulation": (None, [C.c_void_p, C.c_int]),
+    "adj_set_stype": (None, [C.c_void_p, C.c_int]),
     "adj_set_meal": (None, [C.c_void_p, _FP, _FP, _FP]),
     "adj_set_model": (None, [C.c_void_p] + [_DP] * 6),
     "adj_set_source": (None, [C.c_void_p, C.c_int, _IP, _IP, _DP]),
@@ -171,7 +172,8 @@ def _d(a):
 
 class AdjointOracle:
     """Double-precision forward and adjoint-state gradient of the three
-    formulations (cfg variant; oracle/ttifd_adjoint.c), stress source only. MEAL coef1, coef2
+    formulations (cfg variant; oracle/ttifd_adjoint.c) with the stress source
+    or a velocity source (cfg stype, default 1). MEAL coef1, coef2
     and Beta are frozen from the float setup of `meal_model` (padded arrays);
     vs and rho stay fixed; the model (vp, eps, delta, theta) can be changed
     with set_model for finite differences."""
@@ -189,6 +191,7 @@ class AdjointOracle:
         variant = c.get("variant", 0)
         variant = ttifd.VARIANTS[variant] if isinstance(variant, str) else int(variant)
         lib.adj_set_formulation(self._c, variant)
+        lib.adj_set_stype(self._c, int(c.get("stype", 1)))
         nz, nx, nts = C.c_int(), C.c_int(), C.c_int()
         lib.adj_grid(self._c, C.byref(nz), C.byref(nx), C.byref(nts))
         self.Nz, self.Nx, self.nts = nz.value, nx.value, nts.value

@@ -19,8 +19,15 @@
  * every padded cell. Conventions: vs and rho are held fixed; the MEAL arrays
  * coef1, coef2 and Beta are frozen (given, from the float setup of a
  * reference model); stiffness uses vp/Beta, vs/Beta, rho*Beta (meal.c:450-490).
- * Only the stress source (stype 1) is modelled. The forward states are all
- * kept in memory (small test grids).
+ * Sources: the stress source (stype 1, :865-886) and the velocity sources
+ * (stype 2-8, :674-802), which add to v after the velocity update. The
+ * source tables do not depend on the model, so the model gradient has the same
+ * adjoint for every stype; the source-wavelet gradient reads lambda_v between
+ * the stress-half and velocity-half adjoints. A velocity source window can
+ * reach cells the velocity update never writes (the image rows above a free
+ * surface, the outer rim); v there only accumulates source samples, so its
+ * adjoint only accumulates the transposed stress stencils. The forward
+ * states are all kept in memory (small test grids).
  */
 #include <math.h>
 #include <stdlib.h>
@@ -33,7 +40,7 @@ static const double RSGC[5] = {1.24362739770907f, -0.114021164233934f, 0.0272965
                                0.00132022981661381f};
 
 struct adj_ctx {
-  int nz, nx, nt, E, Nz, Nx, izs, fs, mt, seistype, nts;
+  int nz, nx, nt, E, Nz, Nx, izs, fs, mt, seistype, nts, stype;
   double dx, dz, dt, scalar;
   size_t Np;
   /* frozen MEAL */
@@ -72,6 +79,7 @@ adj_ctx *adj_create(int nz, int nx, int nt, double dx, double dz, double dt, int
   c->dz = dz;
   c->dt = dt;
   c->scalar = scalar;
+  c->stype = 1;
   c->Np = (size_t)c->Nz * c->Nx;
   double **arrs[] = {&c->coef1, &c->coef2, &c->beta, &c->vp,  &c->vs,  &c->rho, &c->eps, &c->delta, &c->theta, &c->c11,
                      &c->c13,   &c->c33,   &c->c55,  &c->sn,  &c->cs,  &c->snv, &c->csv, &c->ir,    &c->c15,   &c->c35};
@@ -107,6 +115,8 @@ void adj_set_formulation(adj_ctx *c, int variant)
   c->tensor = variant == 1;
   c->bond = variant == 2;
 }
+
+void adj_set_stype(adj_ctx *c, int stype) { c->stype = stype; }
 
 /* Bond rotation of the VTI moduli (bond:492-541): c11 c13 c15 c33 c35 c55 */
 static void bond_moduli(double C11, double C13, double C33, double C55, double th, double out[6])
@@ -290,11 +300,75 @@ static void ds(const adj_ctx *c, const double *a, int ix, int iz, double *d1, do
   *d2 = s2;
 }
 
+/* the velocity-node pair with cells outside the grid read as zero */
+static double at0(const adj_ctx *c, const double *a, int ix, int iz)
+{
+  return ix < 0 || ix >= c->Nx || iz < 0 || iz >= c->Nz ? 0.0 : A2(a, ix, iz);
+}
+
+static void dv_rim(const adj_ctx *c, const double *a, int ix, int iz, double *d1, double *d2)
+{
+  double s1 = 0.0, s2 = 0.0;
+  for (int k = 1; k <= NH; ++k) {
+    s1 += RSGC[k - 1] * (at0(c, a, ix + k, iz + k) - at0(c, a, ix - k + 1, iz - k + 1));
+    s2 += RSGC[k - 1] * (at0(c, a, ix + k, iz - k + 1) - at0(c, a, ix - k + 1, iz + k));
+  }
+  *d1 = s1;
+  *d2 = s2;
+}
+
 static double src_weight(const adj_ctx *c, int a, int b)
 {
   const double alpha = log(0.8) / (c->dx * c->dx + c->dz * c->dz);
   const double rx = a * c->dx, rz = b * c->dz;
   return exp(alpha * (rx * rx + rz * rz)) / (c->dx * c->dz) * c->dt;
+}
+
+/* cells and weights of velocity source n (stype 2-8, coord:674-802):
+ * vx[cell] += wx src(t), vz[cell] += wz src(t). stype 4 is stype 2 followed by
+ * stype 3 on the same window; stype 8 touches four cells without a window.
+ * Returns the number of cells (at most 121). */
+static int vsrc_cells(const adj_ctx *c, int n, int *cx, int *cz, double *wx, double *wz)
+{
+  const int x0 = c->sx[n] + c->E, z0 = c->sz[n] + c->E;
+  int m = 0;
+  if (c->stype == 8) {
+    static const int ox[4] = {0, -1, -1, 0}, oz[4] = {0, 0, -1, -1};
+    static const double sgx[4] = {-1.0, -1.0, 1.0, 1.0}, sgz[4] = {1.0, -1.0, -1.0, 1.0};
+    const double q = 0.125 * sqrt(2.0);
+    for (int k = 0; k < 4; ++k, ++m) {
+      cx[m] = x0 + ox[k];
+      cz[m] = z0 + oz[k];
+      wx[m] = sgx[k] * q;
+      wz[m] = sgz[k] * q;
+    }
+    return m;
+  }
+  const double alpha = log(0.8) / (c->dx * c->dx + c->dz * c->dz);
+  for (int a = -NH; a <= NH; ++a)
+    for (int b = -NH; b <= NH; ++b) {
+      const int ix = x0 + a, iz = z0 + b;
+      if (ix < 0 || ix >= c->Nx || iz < 0 || iz >= c->Nz) continue;
+      const double w = src_weight(c, a, b), kx = 2.0 * alpha * a * c->dx * w, kz = 2.0 * alpha * b * c->dz * w;
+      double x = 0.0, z = 0.0;
+      if (c->stype == 2 || c->stype == 4) {  /* divergence force */
+        x += kx;
+        z += kz;
+      }
+      if (c->stype == 3 || c->stype == 4) {  /* curl force */
+        x -= kz;
+        z += kx;
+      }
+      if (c->stype == 5) x = w;  /* horizontal point force */
+      if (c->stype == 6) z = w;  /* vertical point force */
+      if (c->stype == 7) x = z = 0.5 * sqrt(2.0) * w;  /* tilted point force */
+      cx[m] = ix;
+      cz[m] = iz;
+      wx[m] = x;
+      wz[m] = z;
+      ++m;
+    }
+  return m;
 }
 
 /* ---------------------------------------------------------------- forward */
@@ -382,8 +456,23 @@ static void free_surface(const adj_ctx *c, state *u)
   }
 }
 
+static void velocity_source(const adj_ctx *c, state *u, int it)
+{
+  int cx[121], cz[121];
+  double wx[121], wz[121];
+  for (int n = 0; n < c->nsrc; ++n) {
+    const double w = c->src[(size_t)n * c->nt + it];
+    const int m = vsrc_cells(c, n, cx, cz, wx, wz);
+    for (int q = 0; q < m; ++q) {
+      A2(u->vx, cx[q], cz[q]) += wx[q] * w;
+      A2(u->vz, cx[q], cz[q]) += wz[q] * w;
+    }
+  }
+}
+
 static void stress_source(const adj_ctx *c, state *u, int it)
 {
+  if (c->stype != 1) return;
   for (int n = 0; n < c->nsrc; ++n) {
     const int x0 = c->sx[n] + c->E, z0 = c->sz[n] + c->E;
     const double w = c->src[(size_t)n * c->nt + it];
@@ -447,6 +536,7 @@ static void state_free(state *s)
 static void step(const adj_ctx *c, state *u, int it, double *rec[3], state *keep)
 {
   velocity_half(c, u);
+  if (c->stype >= 2) velocity_source(c, u, it);
   if (keep) {
     memcpy(keep->vx, u->vx, c->Np * sizeof(double));
     memcpy(keep->vz, u->vz, c->Np * sizeof(double));
@@ -524,7 +614,7 @@ double adj_gradient(adj_ctx *c, const double *dobs[3], double *g_vp, double *g_e
       }
     }
     /* source-wavelet gradient (adjoint of the stress source) */
-    if (g_src)
+    if (g_src && c->stype == 1)
       for (int n = 0; n < c->nsrc; ++n) {
         const int x0 = c->sx[n] + c->E, z0 = c->sz[n] + c->E;
         double acc = 0.0;
@@ -649,6 +739,32 @@ double adj_gradient(adj_ctx *c, const double *dobs[3], double *g_vp, double *g_e
         L.vx[i] -= hx * (p1 + p2) + hz * (q1 - q2);
         L.vz[i] -= hx * (r1 + r2) + hz * (s1 - s2);
       }
+    if (c->stype >= 2) {
+      /* velocity cells outside the update (image rows, rim): v there holds the
+       * injected samples, so lambda_v only accumulates the transposed stencils */
+      for (int ix = 0; ix < Nx; ++ix)
+        for (int iz = 0; iz < Nz; ++iz) {
+          if (ix >= NH && ix < Nx - NH && iz >= izs && iz < Nz - NH) continue;
+          double p1, p2, q1, q2, r1, r2, s1, s2;
+          dv_rim(c, T[0], ix, iz, &p1, &p2);
+          dv_rim(c, T[1], ix, iz, &q1, &q2);
+          dv_rim(c, T[2], ix, iz, &r1, &r2);
+          dv_rim(c, T[3], ix, iz, &s1, &s2);
+          A2(L.vx, ix, iz) -= hx * (p1 + p2) + hz * (q1 - q2);
+          A2(L.vz, ix, iz) -= hx * (r1 + r2) + hz * (s1 - s2);
+        }
+      /* source-wavelet gradient (adjoint of the velocity sources) */
+      if (g_src) {
+        int cx[121], cz[121];
+        double wx[121], wz[121];
+        for (int n = 0; n < c->nsrc; ++n) {
+          const int m = vsrc_cells(c, n, cx, cz, wx, wz);
+          double acc = 0.0;
+          for (int q = 0; q < m; ++q) acc += wx[q] * A2(L.vx, cx[q], cz[q]) + wz[q] * A2(L.vz, cx[q], cz[q]);
+          g_src[(size_t)n * c->nt + it] = acc;
+        }
+      }
+    }
     /* adjoint of the velocity half */
     for (int k = 0; k < 6; ++k) memset(T[k], 0, Np * sizeof(double));
     for (int ix = NH; ix < Nx - NH; ++ix)

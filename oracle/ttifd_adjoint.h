@@ -23,7 +23,9 @@ void adj_set_meal(adj_ctx *c, const float *coef1, const float *coef2, const floa
 /* padded [Nx][Nz] model (theta in degrees); builds the coordinate-rotation stiffness */
 void adj_set_model(adj_ctx *c, const double *vp, const double *vs, const double *rho, const double *eps,
                    const double *delta, const double *theta);
-/* stress sources (stype 1); positions in physical cells, w is [n][nt] */
+/* source type: 1 stress source (default), 2-8 velocity sources */
+void adj_set_stype(adj_ctx *c, int stype);
+/* sources of the set stype; positions in physical cells, w is [n][nt] */
 void adj_set_source(adj_ctx *c, int n, const int *sx, const int *sz, const double *w);
 void adj_set_receivers(adj_ctx *c, int kind, int n, const int *gx, const int *gz);
 /* traces [ntrace][nts] per recorded component (NULL entries skipped) */

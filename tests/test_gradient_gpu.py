@@ -1,8 +1,9 @@
 """Device adjoint-state gradient (tti_grad_*) against the double-precision CPU
 reference (oracle/ttifd_adjoint.c, itself pinned by the dot-product test and
 central finite differences): misfit, the four model gradients and the source
-gradient; independence of the checkpoint count; shot accumulation; the
-dot-product test of the device adjoint."""
+gradient, for the stress source and the velocity sources; independence of the
+checkpoint count; shot accumulation; the dot-product test of the device
+adjoint."""
 import numpy as np
 import pytest
 
@@ -28,15 +29,15 @@ def _case(fs, sx=24, variant="coordinate_rotation"):
     return cfg, pads, true, w, gx
 
 
-def _device(cfg, pads, w, gx, dobs, ncheck, sx=24, h=None):
+def _device(cfg, pads, w, gx, dobs, ncheck, sx=24, h=None, sz=3):
     import ttifd
 
     own = h is None
     if own:
-        h = ttifd.Modeling(stype=1, **dict({"variant": "coordinate_rotation"}, **cfg))
+        h = ttifd.Modeling(**dict({"variant": "coordinate_rotation", "stype": 1}, **cfg))
         h.upload_model(*pads)
         h.grad_zero()
-    h.set_source([sx], [3], w[None, :])
+    h.set_source([sx], [sz], w[None, :])
     for k in (0, 1, 2):
         h.set_receivers(k, gx, 2)
         h.grad_set_observed(k, dobs[k])
@@ -129,14 +130,71 @@ def test_device_dot_product(gpu_lib):
     assert abs(lhs - rhs) <= 2e-4 * abs(lhs), (lhs, rhs)
 
 
-def test_gradient_rejects_velocity_sources(gpu_lib):
-    """The gradient models the stress source only (stype 1)."""
+VSRC = [(s, 1, "coordinate_rotation", "tiled") for s in range(2, 9)] + \
+    [(4, 0, "coordinate_rotation", "tiled"), (2, 1, "coordinate_rotation", "naive"),
+     (8, 1, "coordinate_rotation", "naive"), (5, 1, "tensor_rotation", "tiled"), (7, 0, "bond_transformation", "tiled")]
+
+
+@pytest.mark.parametrize("stype,fs,variant,kernel", VSRC)
+def test_velocity_source_gradient_matches_cpu_reference(stype, fs, variant, kernel, monkeypatch, gpu_lib):
+    """Velocity sources (stype 2-8): the model gradient (same adjoint kernels,
+    forward replay with the velocity source) and the source gradient (read from
+    lambda_v between the adjoint halves; one row below the free surface the
+    window reaches the image rows, stype 8 sits on the surface row). The
+    observed traces are the true model's at half amplitude, so the residual is
+    of the size of the data: with the true model's own traces the residual is
+    a small difference of two close wavefields, and the float forward's
+    rounding (1e-5 of the traces) grows to 4e-4 of J for stype 8, which would
+    measure the residual's conditioning rather than the adjoint."""
+    if kernel == "naive":
+        monkeypatch.setenv("TTIFD_KERNEL", "naive")
+    else:
+        monkeypatch.delenv("TTIFD_KERNEL", raising=False)
+    cfg, pads, true, w, gx = _case(fs, variant=variant)
+    cfg = dict(cfg, stype=stype)
+    sz = 0 if stype == 8 else 1
+    with AdjointOracle(cfg, pads) as adj:
+        adj.set_model(*true)
+        adj.set_source([24], [sz], w[None, :])
+        for k in (0, 1, 2):
+            adj.set_receivers(k, gx, 2)
+        dobs = [0.5 * d for d in adj.forward()]
+        adj.set_model(*pads)
+        J_ref, g_ref, gs_ref = adj.gradient(dobs)
+    h, J = _device(cfg, pads, w, gx, [d.astype(np.float32) for d in dobs], ncheck=9, sz=sz)
+    with h:  # measured on B200: J 1e-7..1e-6, gradients 4e-7..1.4e-6, source gradient 5e-7..5e-6
+        assert J == pytest.approx(J_ref, rel=1e-5)
+        for name in NAMES:
+            err = _rel(h.grad_fetch(name), g_ref[name])
+            assert err <= 2e-5, (name, err)
+        assert _rel(h.grad_fetch_source(1), gs_ref) <= 5e-5
+
+
+@pytest.mark.parametrize("stype", [3, 8])
+def test_device_dot_product_velocity_sources(stype, gpu_lib):
+    """<L w, r> = <w, L^T r> for a velocity source whose cells reach the image
+    rows above the free surface."""
     import ttifd
 
-    with ttifd.Modeling(stype=2, **dict(CFG, variant="coordinate_rotation")) as h:
-        with pytest.raises(ttifd.TTIError) as e:
-            h.grad_zero()
-        assert e.value.code == ttifd.ERR_ARG
+    cfg, pads, true, w, gx = _case(1)
+    cfg = dict(cfg, stype=stype)
+    sz = 0 if stype == 8 else 1
+    with ttifd.Modeling(**cfg) as h:
+        h.upload_model(*pads)
+        h.set_source([24], [sz], w[None, :])
+        for k in (0, 1, 2):
+            h.set_receivers(k, gx, 2)
+        h.run()
+        d = [h.fetch_traces(k).astype(np.float64) for k in (0, 1, 2)]
+    rng = np.random.default_rng(4)
+    scale = max(np.abs(x).max() for x in d)
+    r = [scale * rng.standard_normal(x.shape) for x in d]
+    h, _ = _device(cfg, pads, w, gx, [(a - b).astype(np.float32) for a, b in zip(d, r)], ncheck=4, sz=sz)
+    with h:
+        gsrc = h.grad_fetch_source(1).astype(np.float64)
+    lhs = sum(float(np.sum(a * b)) for a, b in zip(d, r))
+    rhs = float(np.sum(gsrc[0] * w))
+    assert abs(lhs - rhs) <= 2e-4 * abs(lhs), (lhs, rhs)
 
 
 def test_gradient_sums_are_device_views(gpu_lib):

@@ -1,8 +1,11 @@
-// Adjoint-state gradient (tti_grad_*), coordinate-rotation formulation.
+// Adjoint-state gradient (tti_grad_*) of the three formulations, stated
+// here for the coordinate rotation (the tensor and Bond branches differ in
+// the stress-half adjoint and the chain rule only).
 //
 // Misfit J = 1/2 sum over the recorded samples of (d - dobs)^2. The forward
 // step (coord:611-926) is, per time step n:
-//   v'  = coef1 v + coef2 invrho R(theta_v) D_sigma sigma      velocity half (:614-672) + sources
+//   v'  = coef1 v + coef2 invrho R(theta_v) D_sigma sigma      velocity half (:614-672)
+//         + velocity sources, stype 2-8 (:674-802)
 //   s'  = coef1 s + coef2 H(c11, c13, c33, c55, theta) D_v v'   stress half (:804-845)
 //   s'' = P_fs s' (free surface, :847-863), + stress source, record (isoelastic.c:103-144)
 // Its discrete adjoint, run backwards from n = nt-1, is per step:
@@ -51,6 +54,15 @@ struct GradState {
   CUtensorMap *maps = nullptr;  // host copies, 64-byte aligned: T0..T3, TV0..TV5
   CUtensorMap *slot_maps = nullptr;  // kept sxx, szz, sxz of every segment slot (seg x 3)
   int slot_maps_n = 0;
+  // velocity sources (stype 2-8): per source vm cells (ix, iz, index in the
+  // rim list or -1; ix < 0: off the grid) with weights (wx, wz),
+  // v[cell] += w src(t); the cells of all windows outside the velocity update,
+  // each once, with their accumulated transposed stencils (x, z) in double
+  int4 *vcell = nullptr;
+  float2 *vw = nullptr;
+  int2 *vrim = nullptr;
+  double *vrim_acc = nullptr;
+  int vm = 0, vrim_n = 0;
 };
 
 namespace {
@@ -171,6 +183,100 @@ __global__ void k_adj_surface(SurfaceArgs a)
     }
     xz[c] = 0.0f;
     zz[c] = 0.0f;
+  }
+}
+
+// Adjoint of the velocity sources (coord:674-802), between the stress-half
+// adjoint (T0..T3 written) and the velocity-half adjoint (lambda_v not yet
+// updated). The source adds w src(t) to v after the velocity update, so
+// dJ/d src(t) = sum over its cells of w . lambda_v with lambda_v already
+// holding the transposed stress stencils of T. Cells outside the velocity
+// update (image rows above a free surface, the rim) are never written by the
+// forward step except by the source; their lambda_v only accumulates those
+// stencils (a running sum over the whole reverse pass, kept in double beside
+// lambda_v, which there holds only the injected residuals), which this kernel
+// applies first, once per cell. One block: the rim update must finish before
+// any source reads it.
+struct VSrcArgs {
+  Grid g;
+  const float *lam0, *lam1;
+  const float *T[4];
+  const int4 *cell;
+  const float2 *w;
+  const int2 *rim;
+  double *rim_acc;  // [nrim][2]
+  int m, nsrc, nrim;
+  float hx, hz;
+  float *gsrc;  // [nsrc][nt]
+  int nt, it;
+};
+
+__device__ __forceinline__ float t_at(const float *a, const Grid &g, int ix, int iz)
+{
+  return ix < 0 || ix >= g.Nx || iz < 0 || iz >= g.Nz ? 0.0f : a[(size_t)ix * g.ldz + iz];
+}
+
+// the transposed stress stencils at one velocity cell, T read as zero off the grid
+__device__ float2 vsrc_dT(const VSrcArgs &a, int ix, int iz)
+{
+  float d[4][2];
+#pragma unroll
+  for (int f = 0; f < 4; ++f) {
+    float s1 = 0.0f, s2 = 0.0f;
+#pragma unroll
+    for (int k = 1; k <= NH; ++k) {
+      s1 += rsg(k - 1) * (t_at(a.T[f], a.g, ix + k, iz + k) - t_at(a.T[f], a.g, ix - k + 1, iz - k + 1));
+      s2 += rsg(k - 1) * (t_at(a.T[f], a.g, ix + k, iz - k + 1) - t_at(a.T[f], a.g, ix - k + 1, iz + k));
+    }
+    d[f][0] = s1;
+    d[f][1] = s2;
+  }
+  return make_float2(a.hx * (d[0][0] + d[0][1]) + a.hz * (d[1][0] - d[1][1]),
+                     a.hx * (d[2][0] + d[2][1]) + a.hz * (d[3][0] - d[3][1]));
+}
+
+constexpr int VSRC_THREADS = 256;
+
+__global__ void __launch_bounds__(VSRC_THREADS) k_adj_vsource(VSrcArgs a)
+{
+  pdl_sync();
+  const Grid &g = a.g;
+  for (int q = threadIdx.x; q < a.nrim; q += blockDim.x) {
+    const int2 c = a.rim[q];
+    const float2 d = vsrc_dT(a, c.x, c.y);
+    a.rim_acc[2 * q] -= d.x;
+    a.rim_acc[2 * q + 1] -= d.y;
+  }
+  __syncthreads();
+  __shared__ double part[VSRC_THREADS / 32];
+  for (int n = 0; n < a.nsrc; ++n) {
+    double v = 0.0;
+    for (int q = threadIdx.x; q < a.m; q += blockDim.x) {
+      const int4 c = a.cell[(size_t)n * a.m + q];
+      if (c.x < 0) continue;
+      const size_t i = (size_t)c.x * g.ldz + c.y;
+      double lx = a.lam0[i], lz = a.lam1[i];
+      if (c.z >= 0) {  // outside the velocity update: plus the accumulated stencils
+        lx += a.rim_acc[2 * c.z];
+        lz += a.rim_acc[2 * c.z + 1];
+      } else {  // the velocity-half adjoint has not yet applied T here
+        const float2 d = vsrc_dT(a, c.x, c.y);
+        lx -= d.x;
+        lz -= d.y;
+      }
+      const float2 w = a.w[(size_t)n * a.m + q];
+      v += w.x * lx + w.y * lz;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += part[k];
+      a.gsrc[(size_t)n * a.nt + a.it] = (float)t;
+    }
+    __syncthreads();
   }
 }
 
@@ -656,7 +762,6 @@ int gerr(tti_handle *h, int code, const char *msg) { return handle_error(h, code
 int grad_check(tti_handle *h)
 {
   if (h->use_fused) return gerr(h, TTI_ERR_STATE, "the gradient runs on the tiled or per-cell kernels");
-  if (h->cfg.stype != 1) return gerr(h, TTI_ERR_ARG, "the gradient models the stress source (stype = 1)");
   if (!h->have_model || !h->m_eps) return gerr(h, TTI_ERR_STATE, "model not uploaded");
   return TTI_OK;
 }
@@ -709,6 +814,115 @@ AdjArgs adj_args(tti_handle *h, int slot)
   return a;
 }
 
+// Cells and weights of the velocity sources from the forward step's own
+// tables (the same float weights sources_block adds with), and the cells of
+// all windows outside the velocity update.
+int vsource_tables(tti_handle *h, const SourceTables &tab)
+{
+  GradState *s = h->grad;
+  cudaFree(s->vcell);
+  cudaFree(s->vw);
+  cudaFree(s->vrim);
+  cudaFree(s->vrim_acc);
+  s->vcell = nullptr;
+  s->vw = nullptr;
+  s->vrim = nullptr;
+  s->vrim_acc = nullptr;
+  s->vm = s->vrim_n = 0;
+  const int stype = h->cfg.stype, ns = h->nsrc;
+  if (stype < 2 || ns <= 0) return TTI_OK;
+  const Grid &g = h->g;
+  std::vector<int> sx(ns), sz(ns);
+  GCK(h, cudaMemcpyAsync(sx.data(), h->d_sx, sizeof(int) * ns, cudaMemcpyDeviceToHost, h->stream));
+  GCK(h, cudaMemcpyAsync(sz.data(), h->d_sz, sizeof(int) * ns, cudaMemcpyDeviceToHost, h->stream));
+  GCK(h, cudaStreamSynchronize(h->stream));
+  const int m = stype == 8 ? 4 : 121;
+  std::vector<int4> cell((size_t)ns * m);
+  std::vector<float2> w((size_t)ns * m);
+  std::vector<int2> rim;
+  for (int n = 0; n < ns; ++n)
+    for (int q = 0; q < m; ++q) {
+      int ix, iz;
+      float wx = 0.0f, wz = 0.0f;
+      if (stype == 8) {  // coord:782-801: four cells, +-sqrt(2)/8
+        static const int ox[4] = {0, -1, -1, 0}, oz[4] = {0, 0, -1, -1};
+        static const float gx[4] = {-1.0f, -1.0f, 1.0f, 1.0f}, gz[4] = {1.0f, -1.0f, -1.0f, 1.0f};
+        ix = sx[n] + ox[q];
+        iz = sz[n] + oz[q];
+        wx = gx[q] * tab.q8;
+        wz = gz[q] * tab.q8;
+      } else {  // the 11 x 11 window, cell q = (x offset + 5) * 11 + (z offset + 5)
+        ix = sx[n] + q / 11 - NH;
+        iz = sz[n] + q % 11 - NH;
+        if (stype == 2 || stype == 4) {
+          wx += tab.kx[q];
+          wz += tab.kz[q];
+        }
+        if (stype == 3 || stype == 4) {
+          wx -= tab.kz[q];
+          wz += tab.kx[q];
+        }
+        if (stype == 5) wx = tab.k5[q];
+        if (stype == 6) wz = tab.k5[q];
+        if (stype == 7) wx = wz = tab.k7[q];
+      }
+      const bool on = ix >= 0 && ix < g.Nx && iz >= 0 && iz < g.Nz;
+      cell[(size_t)n * m + q] = on ? make_int4(ix, iz, -1, 0) : make_int4(-1, -1, -1, 0);
+      w[(size_t)n * m + q] = make_float2(wx, wz);
+      const bool upd = ix >= NH && ix < g.Nx - NH && iz >= g.izStart && iz < g.Nz - NH;
+      if (on && !upd) rim.push_back(make_int2(ix, iz));
+    }
+  const auto less = [](int2 a, int2 b) { return a.x != b.x ? a.x < b.x : a.y < b.y; };
+  std::sort(rim.begin(), rim.end(), less);
+  rim.erase(std::unique(rim.begin(), rim.end(), [](int2 a, int2 b) { return a.x == b.x && a.y == b.y; }),
+            rim.end());
+  for (auto &c : cell)
+    if (c.x >= 0) {
+      const auto it = std::lower_bound(rim.begin(), rim.end(), make_int2(c.x, c.y), less);
+      if (it != rim.end() && it->x == c.x && it->y == c.y) c.z = (int)(it - rim.begin());
+    }
+  GCK(h, cudaMalloc(&s->vcell, sizeof(int4) * cell.size()));
+  GCK(h, cudaMalloc(&s->vw, sizeof(float2) * w.size()));
+  GCK(h, cudaMemcpyAsync(s->vcell, cell.data(), sizeof(int4) * cell.size(), cudaMemcpyHostToDevice, h->stream));
+  GCK(h, cudaMemcpyAsync(s->vw, w.data(), sizeof(float2) * w.size(), cudaMemcpyHostToDevice, h->stream));
+  if (!rim.empty()) {
+    GCK(h, cudaMalloc(&s->vrim, sizeof(int2) * rim.size()));
+    GCK(h, cudaMalloc(&s->vrim_acc, sizeof(double) * 2 * rim.size()));
+    GCK(h, cudaMemcpyAsync(s->vrim, rim.data(), sizeof(int2) * rim.size(), cudaMemcpyHostToDevice, h->stream));
+    GCK(h, cudaMemsetAsync(s->vrim_acc, 0, sizeof(double) * 2 * rim.size(), h->stream));
+  }
+  GCK(h, cudaStreamSynchronize(h->stream));  // the host vectors go out of scope
+  s->vm = m;
+  s->vrim_n = (int)rim.size();
+  return TTI_OK;
+}
+
+int launch_vsource(tti_handle *h, const AdjArgs &a, int it)
+{
+  GradState *s = h->grad;
+  if (s->vm == 0) return TTI_OK;
+  VSrcArgs v;
+  v.g = h->g;
+  v.lam0 = a.lam[0];
+  v.lam1 = a.lam[1];
+  for (int k = 0; k < 4; ++k) v.T[k] = a.T[k];
+  v.cell = s->vcell;
+  v.w = s->vw;
+  v.rim = s->vrim;
+  v.rim_acc = s->vrim_acc;
+  v.m = s->vm;
+  v.nsrc = h->nsrc;
+  v.nrim = s->vrim_n;
+  v.hx = a.hx;
+  v.hz = a.hz;
+  v.gsrc = s->gsrc;
+  v.nt = h->cfg.nt;
+  v.it = it;
+  GCK(h, launch_pdl(k_adj_vsource, dim3(1), dim3(VSRC_THREADS), 0, h->stream, v));
+  h->launches++;
+  return TTI_OK;
+}
+
 // adjoint of forward step index n (time index it), segment slot `slot`
 int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
 {
@@ -732,13 +946,14 @@ int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
       sa.res[k] = on ? s->res[k] + (size_t)(it / c.mt) * h->nrec[k] : nullptr;
       any = any || on;
     }
-    sa.src = SourceSet{h->nsrc, h->d_sx, h->d_sz, h->d_src, c.nt};
+    const bool ssrc = h->nsrc > 0 && c.stype == 1;
+    sa.src = SourceSet{ssrc ? h->nsrc : 0, h->d_sx, h->d_sz, h->d_src, c.nt};
     memcpy(sa.k1.k1, tab.k1, sizeof sa.k1.k1);
     sa.gsrc = s->gsrc;
     sa.it = it;
     sa.fs = c.freesurface == 1;
     sa.tensor = c.variant == TTI_TENSOR;
-    if (any || h->nsrc > 0 || sa.fs) {
+    if (any || ssrc || sa.fs) {
       GCK(h, launch_pdl(k_adj_surface, dim3((g.Nx + 3) / 4), dim3(128), 0, h->stream, sa));
       h->launches++;
     }
@@ -751,6 +966,7 @@ int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
     if (c.variant == TTI_BOND) GCK(h, launch_pdl(k_adj_stress_local<TTI_BOND>, grd, blk, 0, h->stream, a));
     else if (c.variant == TTI_TENSOR) GCK(h, launch_pdl(k_adj_stress_local<TTI_TENSOR>, grd, blk, 0, h->stream, a));
     else GCK(h, launch_pdl(k_adj_stress_local<TTI_COORDINATE>, grd, blk, 0, h->stream, a));
+    if (int rc = launch_vsource(h, a, it)) return rc;
     AdjTile at;
     memset(&at, 0, sizeof at);
     at.a = a;
@@ -767,16 +983,12 @@ int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
     return TTI_OK;
   }
   const dim3 blk(BZ, BX), grd((g.Nz + BZ - 1) / BZ, (g.Nx + BX - 1) / BX);
-  if (c.variant == TTI_BOND) {
-    k_adj_stress_local<TTI_BOND><<<grd, blk, 0, h->stream>>>(a);
-    k_adj_velocity<TTI_BOND><<<grd, blk, 0, h->stream>>>(a);
-  } else if (c.variant == TTI_TENSOR) {
-    k_adj_stress_local<TTI_TENSOR><<<grd, blk, 0, h->stream>>>(a);
-    k_adj_velocity<TTI_BOND><<<grd, blk, 0, h->stream>>>(a);  // no rotation at the velocity node
-  } else {
-    k_adj_stress_local<TTI_COORDINATE><<<grd, blk, 0, h->stream>>>(a);
-    k_adj_velocity<TTI_COORDINATE><<<grd, blk, 0, h->stream>>>(a);
-  }
+  if (c.variant == TTI_BOND) k_adj_stress_local<TTI_BOND><<<grd, blk, 0, h->stream>>>(a);
+  else if (c.variant == TTI_TENSOR) k_adj_stress_local<TTI_TENSOR><<<grd, blk, 0, h->stream>>>(a);
+  else k_adj_stress_local<TTI_COORDINATE><<<grd, blk, 0, h->stream>>>(a);
+  if (int rc = launch_vsource(h, a, it)) return rc;
+  if (c.variant == TTI_COORDINATE) k_adj_velocity<TTI_COORDINATE><<<grd, blk, 0, h->stream>>>(a);
+  else k_adj_velocity<TTI_BOND><<<grd, blk, 0, h->stream>>>(a);  // tensor and Bond: no rotation at the velocity node
   k_adj_velocity_stencil<<<grd, blk, 0, h->stream>>>(a);
   GCK(h, cudaGetLastError());
   return TTI_OK;
@@ -799,6 +1011,10 @@ void grad_release(tti_handle *h)
   cudaFree(s->ckpt);
   cudaFree(s->keep);
   cudaFree(s->gsrc);
+  cudaFree(s->vcell);
+  cudaFree(s->vw);
+  cudaFree(s->vrim);
+  cudaFree(s->vrim_acc);
   cudaFree(s->d_J);
   free(s->maps);
   free(s->slot_maps);
@@ -899,6 +1115,7 @@ int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
   }
   SourceTables tab;
   handle_source_tables(h, &tab);
+  if ((rc = vsource_tables(h, tab))) return rc;
   // pass 1: forward with a checkpoint at every segment start but the last,
   // whose states are kept directly (ncheck = 1: all states, no recomputation)
   if ((rc = tti_reset(h))) return rc;

@@ -259,7 +259,7 @@ class Modeling:
         self._call("fetch_field", self._h, which, _f(out))
         return out
 
-    # -- adjoint-state gradient (coordinate formulation, stype 1)
+    # -- adjoint-state gradient (three formulations, every source type)
     def grad_set_observed(self, kind, dobs):
         d = np.ascontiguousarray(dobs, dtype=np.float32)
         if d.shape != (self._nrec.get(kind, 0), self.nts):
