@@ -273,12 +273,14 @@ int do_snapshot(tti_handle *h, tti_snapshot_fn fn, void *user, int it)
   const size_t n = (size_t)nzo * nxo;
   if (h->snap_cap < n) {
     cudaFree(h->d_snap);
-    cudaFreeHost(h->h_snap);
+    free(h->h_snap);
     h->d_snap = nullptr;
     h->h_snap = nullptr;
     h->snap_cap = 0;
     CK(h, cudaMalloc(&h->d_snap, n * sizeof(float)));
-    CK(h, cudaMallocHost(&h->h_snap, n * sizeof(float)));
+    h->h_snap = static_cast<float *>(malloc(n * sizeof(float)));
+    if (!h->h_snap) return set_err(h, TTI_ERR_NOMEM, "host allocation of the snapshot buffer failed");
+    prefault(h->h_snap, n * sizeof(float));
     h->snap_cap = n;
   }
   int kinds[3];
@@ -287,6 +289,7 @@ int do_snapshot(tti_handle *h, tti_snapshot_fn fn, void *user, int it)
   for (int q = 0; q < nk; ++q) {
     launch_snapshot(a, kinds[q], h->cfg.savew, h->d_snap, h->stream);
     h->launches++;
+    // pageable destination whose pages are resident: the driver's staged copy
     CK(h, cudaMemcpyAsync(h->h_snap, h->d_snap, n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
     if (fn(user, it, kinds[q], h->h_snap, nzo, nxo) != 0)
@@ -509,11 +512,8 @@ int tti_destroy(tti_handle *h)
   grad_release(h);
   cudaFree(h->d_flag);
   cudaFree(h->d_snap);
-  if (h->h_snap) cudaFreeHost(h->h_snap);
-  for (int b = 0; b < 2; ++b) {
-    cudaFree(h->d_stage[b]);
-    if (h->h_stage[b]) cudaFreeHost(h->h_stage[b]);
-  }
+  free(h->h_snap);
+  cudaFree(h->d_stage);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   free(h->tmaps);
@@ -544,26 +544,27 @@ int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const floa
   const size_t np = (size_t)g.Nz * g.Nx;
   // stability check on the unscaled padded vp (stable.c:217-246)
   {
-    double vmax = FLT_MIN;
-    for (size_t i = 0; i < np; ++i) vmax = fmaxf(vp[i], (float)vmax);
+    const double vmax = host_max(vp, np, FLT_MIN);
     const double csum = (double)rsg(0) + (double)rsg(2) + (double)rsg(4);
     const double dtmax = 1.0f / (vmax * sqrt((1.0 / (c.dx * c.dx) + 1.0 / (c.dz * c.dz)) * csum));
     if (c.dt > dtmax)
       return set_err(h, TTI_ERR_UNSTABLE,
                      "the finite differenct scheme is unstable! the time step size must smaller than %5.5f!", dtmax);
   }
-  // raw model on the device (pitched), freed after the precompute
+  // raw model on the device (pitched, one block of six arrays), freed after the precompute
   float *raw[6] = {};
   const float *src[6] = {vp, vs, rho, epsilon, delta, theta};
-  float *d_w = nullptr;
+  float *d_w = nullptr, *raw_block = nullptr;
   int rc = TTI_OK;
-  for (int k = 0; k < 6 && rc == TTI_OK; ++k) {
-    cudaError_t e = cudaMalloc(&raw[k], g.n * sizeof(float));
+  {
+    cudaError_t e = cudaMalloc(&raw_block, 6 * g.n * sizeof(float));
     if (e != cudaSuccess) rc = set_err(h, TTI_ERR_NOMEM, "device allocation failed: %s", cudaGetErrorString(e));
-    else
-      e = cudaMemcpy2DAsync(raw[k], (size_t)g.ldz * sizeof(float), src[k], (size_t)g.Nz * sizeof(float),
-                            (size_t)g.Nz * sizeof(float), g.Nx, cudaMemcpyHostToDevice, h->stream);
-    if (rc == TTI_OK && e != cudaSuccess) rc = set_err(h, TTI_ERR_CUDA, "model upload: %s", cudaGetErrorString(e));
+  }
+  for (int k = 0; k < 6 && rc == TTI_OK; ++k) {
+    raw[k] = raw_block + (size_t)k * g.n;
+    const cudaError_t e = cudaMemcpy2DAsync(raw[k], (size_t)g.ldz * sizeof(float), src[k], (size_t)g.Nz * sizeof(float),
+                                            (size_t)g.Nz * sizeof(float), g.Nx, cudaMemcpyHostToDevice, h->stream);
+    if (e != cudaSuccess) rc = set_err(h, TTI_ERR_CUDA, "model upload: %s", cudaGetErrorString(e));
   }
   if (rc == TTI_OK) {
     // MEAL scalars evaluated with the host libm, as meal.c:23-29, 62-66 do
@@ -616,7 +617,7 @@ int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const floa
     }
     cudaStreamSynchronize(h->stream);
   }
-  for (auto p : raw) cudaFree(p);
+  cudaFree(raw_block);
   cudaFree(d_w);
   if (rc == TTI_OK && (h->use_fused || h->use_tiled)) {
     fused::launch_pack(g, step_args(h).p, fused::Packed{h->pk_cf, h->pk_vsc, h->pk_sc, h->pk_c4}, c.variant,
@@ -856,35 +857,25 @@ int tti_fetch_traces(tti_handle *h, int kind, float *out)
   if (!h->d_rec[kind]) return set_err(h, TTI_ERR_ARG, "no receivers of kind %d", kind);
   CK(h, cudaSetDevice(h->device));
   const int n = h->nrec[kind], nts = h->nts;
-  // Chunks of receivers: transposed on the device into one of two staging
-  // buffers, copied to pinned memory, and copied on the host into the caller's
-  // [ntrace][nts] block while the next chunk is in flight.
+  // Chunks of receivers transposed on the device (time-major to the caller's
+  // [ntrace][nts]) and copied straight into the caller's block, whose pages
+  // are faulted in first from several host threads.
   constexpr size_t STAGE = (size_t)4 << 20;  // floats per chunk
-  for (int b = 0; b < 2; ++b) {
-    if (!h->d_stage[b]) CK(h, cudaMalloc(&h->d_stage[b], STAGE * sizeof(float)));
-    if (!h->h_stage[b]) CK(h, cudaMallocHost(&h->h_stage[b], STAGE * sizeof(float)));
-  }
-  if (!h->pev[5]) CK(h, cudaEventCreateWithFlags(&h->pev[5], cudaEventDisableTiming));
-  if (!h->pev[6]) CK(h, cudaEventCreateWithFlags(&h->pev[6], cudaEventDisableTiming));
+  if (!h->d_stage) CK(h, cudaMalloc(&h->d_stage, STAGE * sizeof(float)));
   if ((size_t)nts > STAGE || nts > 65535 * 32)
     return set_err(h, TTI_ERR_ARG, "trace of %d samples is longer than the fetch supports", nts);
+  prefault(out, sizeof(float) * (size_t)n * nts);
   const int per = (int)std::max<size_t>(1, STAGE / (size_t)nts);  // receivers per chunk
-  const int nchunk = (n + per - 1) / per;
-  for (int c = 0; c <= nchunk; ++c) {
-    if (c < nchunk) {
-      const int r0 = c * per, nr = std::min(per, n - r0), b = c & 1;
-      launch_transpose(h->d_rec[kind], h->d_stage[b], nts, n, r0, nr, h->stream);
-      h->launches++;
-      CK(h, cudaMemcpyAsync(h->h_stage[b], h->d_stage[b], sizeof(float) * (size_t)nr * nts, cudaMemcpyDeviceToHost,
-                            h->stream));
-      CK(h, cudaEventRecord(h->pev[5 + b], h->stream));
-    }
-    if (c > 0) {  // the previous chunk to the caller
-      const int p = c - 1, r0 = p * per, nr = std::min(per, n - r0), b = p & 1;
-      CK(h, cudaEventSynchronize(h->pev[5 + b]));
-      memcpy(out + (size_t)r0 * nts, h->h_stage[b], sizeof(float) * (size_t)nr * nts);
-    }
+  for (int r0 = 0; r0 < n; r0 += per) {
+    const int nr = std::min(per, n - r0);
+    launch_transpose(h->d_rec[kind], h->d_stage, nts, n, r0, nr, h->stream);
+    h->launches++;
+    // pageable destination: returns once the copy is complete, so the next
+    // chunk may overwrite the staging buffer
+    CK(h, cudaMemcpyAsync(out + (size_t)r0 * nts, h->d_stage, sizeof(float) * (size_t)nr * nts,
+                          cudaMemcpyDeviceToHost, h->stream));
   }
+  CK(h, cudaStreamSynchronize(h->stream));
   return TTI_OK;
 }
 

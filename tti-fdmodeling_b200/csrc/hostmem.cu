@@ -1,0 +1,79 @@
+// Host-side helpers of the transfer paths (no device code).
+//
+// A device-to-host copy into pageable memory that was never touched stops on a
+// page fault per 4 KiB page: on B200 hosts 2.2 GB/s for a fresh 95 MB buffer
+// against 20.8 GB/s into resident pages, and the driver's pinned staging plus a
+// single-threaded copy fares no better. Faulting the pages in from several
+// threads first, then copying straight from the device, avoids both the
+// faults on the copy path and the cost of pinning (13 ms to allocate and
+// 4.7 ms to free 32 MB of page-locked memory).
+#include <float.h>
+
+#include <algorithm>
+#include <thread>
+#include <vector>
+
+#include "ttifd_internal.cuh"
+
+namespace ttifd {
+namespace {
+
+int workers(size_t bytes)
+{
+  const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t by_size = std::max<size_t>(1, bytes >> 22);  // at least 4 MiB each
+  return (int)std::min<size_t>(std::min<size_t>(16, hw), by_size);
+}
+
+// f(begin, end) over [0, n) cut into nth contiguous ranges; the caller's
+// thread takes the last range
+template <class F>
+void split(size_t n, int nth, F f)
+{
+  std::vector<std::thread> th;
+  const size_t per = (n + nth - 1) / nth;
+  for (int t = 0; t < nth - 1; ++t) {
+    const size_t b = t * per, e = std::min(n, b + per);
+    if (b < e) th.emplace_back(f, b, e);
+  }
+  const size_t b = (size_t)(nth - 1) * per;
+  if (b < n) f(b, n);
+  for (auto &x : th) x.join();
+}
+
+}  // namespace
+
+void prefault(void *p, size_t bytes)
+{
+  if (!p || bytes == 0) return;
+  volatile char *c = static_cast<volatile char *>(p);
+  const size_t pages = (bytes + 4095) / 4096;
+  split(pages, workers(bytes), [c, bytes](size_t b, size_t e) {
+    for (size_t q = b; q < e; ++q) c[std::min(q * 4096, bytes - 1)] = 0;
+  });
+}
+
+float host_max(const float *a, size_t n, float init)
+{
+  if (n == 0) return init;
+  const int nth = workers(n * sizeof(float));
+  std::vector<float> part(nth, init);
+  const size_t per = (n + nth - 1) / nth;
+  split(n, nth, [&](size_t b, size_t e) {
+    // eight running maxima; (v > m ? v : m) keeps m for a NaN v, as fmaxf does
+    float m[8];
+    for (float &x : m) x = init;
+    size_t i = b;
+    for (; i + 8 <= e; i += 8)
+      for (int k = 0; k < 8; ++k) m[k] = a[i + k] > m[k] ? a[i + k] : m[k];
+    for (; i < e; ++i) m[0] = a[i] > m[0] ? a[i] : m[0];
+    float r = init;
+    for (float x : m) r = fmaxf(r, x);
+    part[b / per] = r;
+  });
+  float r = init;
+  for (float x : part) r = fmaxf(r, x);
+  return r;
+}
+
+}  // namespace ttifd

@@ -105,6 +105,12 @@ struct SourceSet {
   int nt;
 };
 
+// Host-memory helpers (hostmem.cu): fault in every page of a host range from
+// several threads before a pageable device-to-host copy; the maximum of n
+// floats (NaN entries ignored, as fmaxf does) from several threads.
+void prefault(void *p, size_t bytes);
+float host_max(const float *a, size_t n, float init);
+
 struct ReceiverSet {
   int n[3];
   const int *x[3], *z[3];  // padded-grid cells
@@ -148,9 +154,8 @@ struct tti_handle {
   double *d_energy = nullptr;  // [nt][2]
   int *d_flag = nullptr;       // nonfinite watchdog
   float *d_snap = nullptr;
-  float *h_snap = nullptr;     // pinned
-  float *d_stage[2] = {};      // trace fetch: device chunks (TTI_STAGE_FLOATS each)
-  float *h_stage[2] = {};      // trace fetch: pinned host chunks
+  float *h_snap = nullptr;     // snapshot handed to the callback (pageable, faulted in once)
+  float *d_stage = nullptr;    // trace fetch: device chunk of transposed traces
   size_t snap_cap = 0;
   bool have_model = false;
   int step_index = 0;
