@@ -44,7 +44,8 @@ struct GradState {
                             // Bond: c11 c13 c33 c55 c15 c35 (the rotated moduli)
   float *out[4] = {};       // vp eps delta theta
   float *ckpt = nullptr;    // (ncheck - 1) x the formulation's fields (5, tensor 8)
-  float *keep = nullptr;    // seg x 5 fields: vx vz and sxx szz sxz (tensor: txx tzz txz)
+  float *keep = nullptr;    // seg x nkeep fields per kept step (keep_fields: v, then P Q R S, sigma or tau)
+  int nkeep = 0;
   float *obs[3] = {};       // observed traces, time-major [nts][ntrace]
   float *res[3] = {};       // residuals, time-major
   float *gsrc = nullptr;    // [nsrc][nt]
@@ -52,8 +53,6 @@ struct GradState {
   double *d_J = nullptr;
   bool have_obs[3] = {};
   CUtensorMap *maps = nullptr;  // host copies, 64-byte aligned: T0..T3, TV0..TV5
-  CUtensorMap *slot_maps = nullptr;  // kept sxx, szz, sxz of every segment slot (seg x 3)
-  int slot_maps_n = 0;
   // velocity sources (stype 2-8): per source vm cells (ix, iz, index in the
   // rim list or -1; ix < 0: off the grid) with weights (wx, wz),
   // v[cell] += w src(t); the cells of all windows outside the velocity update,
@@ -72,14 +71,65 @@ constexpr int BZ = 32, BX = 8;
 struct AdjArgs {
   Grid g;
   Params p;
+  fused::Packed pk;  // packed parameters (null on the per-cell path)
   float *lam[8];
   float *T[4];
   float *TV[6];
   float *acc[7];
-  const float *keep[5];
-  float hx, hz;
-  int z_lo;  // first row of the transposed velocity stencils
+  const float *keep[6];  // this step's kept fields (keep_fields), null past them
+  float hx, hz, dt;
+  int z_lo;         // first row of the transposed velocity stencils
+  int undamped_ok;  // coef1 == 1, coef2 == dt on [E, Nx - E) x [und_z0, Nz - E) (checked at upload)
+  int und_z0;
 };
+
+__device__ __forceinline__ bool cell_undamped(const AdjArgs &a, int ix, int iz)
+{
+  const Grid &g = a.g;
+  return a.undamped_ok && ix >= g.E && ix < g.Nx - g.E && iz >= a.und_z0 && iz < g.Nz - g.E;
+}
+
+// Stress-node parameters of one cell: coef1, coef2 (the constants 1 and dt in
+// the undamped interior), c11 c13 c33 c55, and the formulation's pair
+// (coordinate: sin, cos theta; tensor: sin^2, cos^2; Bond: c15, c35), from the
+// packed arrays (PK) or the plain ones.
+struct SParams {
+  float c1, b, c11, c13, c33, c55, p, q;
+};
+template <bool PK, int V>
+__device__ __forceinline__ SParams stress_params(const AdjArgs &a, size_t i, bool und)
+{
+  SParams s;
+  if (und) {
+    s.c1 = 1.0f;
+    s.b = a.dt;
+  } else if (PK) {
+    const float2 cf = __ldg(a.pk.cf + i);
+    s.c1 = cf.x;
+    s.b = cf.y;
+  } else {
+    s.c1 = a.p.coef1[i];
+    s.b = a.p.coef2[i];
+  }
+  if (PK) {
+    const float4 c4 = __ldg(a.pk.c4 + i);
+    const float2 sc = __ldg(a.pk.sc + i);
+    s.c11 = c4.x;
+    s.c13 = c4.y;
+    s.c33 = c4.z;
+    s.c55 = c4.w;
+    s.p = sc.x;
+    s.q = sc.y;
+  } else {
+    s.c11 = a.p.c11[i];
+    s.c13 = a.p.c13[i];
+    s.c33 = a.p.c33[i];
+    s.c55 = a.p.c55[i];
+    s.p = V == TTI_BOND ? a.p.c15[i] : V == TTI_TENSOR ? a.p.s2[i] : a.p.sn[i];
+    s.q = V == TTI_BOND ? a.p.c35[i] : V == TTI_TENSOR ? a.p.c2[i] : a.p.cs[i];
+  }
+  return s;
+}
 
 __device__ __forceinline__ void pair_v(const float *a, size_t L, int ix, int iz, float &d1, float &d2)
 {
@@ -169,20 +219,34 @@ __global__ void k_adj_surface(SurfaceArgs a)
     if (lane == 0) atomicAdd(a.gsrc + (size_t)n * a.src.nt + a.it, v);
   }
   __syncwarp();
-  if (a.fs && lane == 0 && ix >= NH && ix < g.Nx - NH) {
+  if (a.fs && ix >= NH && ix < g.Nx - NH) {
+    // lane k moves image row izStart - k onto row izStart + k (distinct cells
+    // for each k); lane 0 then adds the sxx images onto the surface row in
+    // the order k = 1..5
     const size_t c = col + g.izStart;
     float *xx = a.lam[2], *zz = a.lam[3], *xz = a.lam[4];
-    for (int k = 1; k <= NH; ++k) {
-      xx[c] += 2.0f * xx[c - k];
-      xx[c + k] -= xx[c - k];
-      xx[c - k] = 0.0f;
-      zz[c + k] -= zz[c - k];
-      zz[c - k] = 0.0f;
-      xz[c + k] -= xz[c - k];
-      xz[c - k] = 0.0f;
+    float img = 0.0f;
+    if (lane >= 1 && lane <= NH) {
+      const size_t m = c - lane, p = c + lane;
+      img = xx[m];
+      xx[p] -= img;
+      zz[p] -= zz[m];
+      xz[p] -= xz[m];
+      xx[m] = 0.0f;
+      zz[m] = 0.0f;
+      xz[m] = 0.0f;
     }
-    xz[c] = 0.0f;
-    zz[c] = 0.0f;
+    float add[NH];
+#pragma unroll
+    for (int k = 1; k <= NH; ++k) add[k - 1] = __shfl_sync(0xffffffffu, img, k);
+    if (lane == 0) {
+      float t = xx[c];
+#pragma unroll
+      for (int k = 0; k < NH; ++k) t += 2.0f * add[k];
+      xx[c] = t;
+      xz[c] = 0.0f;
+      zz[c] = 0.0f;
+    }
   }
 }
 
@@ -231,8 +295,7 @@ __device__ float2 vsrc_dT(const VSrcArgs &a, int ix, int iz)
     d[f][0] = s1;
     d[f][1] = s2;
   }
-  return make_float2(a.hx * (d[0][0] + d[0][1]) + a.hz * (d[1][0] - d[1][1]),
-                     a.hx * (d[2][0] + d[2][1]) + a.hz * (d[3][0] - d[3][1]));
+  return make_float2(d[0][0] + d[1][1], d[2][0] + d[3][1]);  // T holds the combinations of store_T
 }
 
 constexpr int VSRC_THREADS = 256;
@@ -280,8 +343,22 @@ __global__ void __launch_bounds__(VSRC_THREADS) k_adj_vsource(VSrcArgs a)
   }
 }
 
+// The transposed stress stencils are minus the velocity-node pairs; with
+// t0..t3 the strain-rate adjoints (d/d vxx, vxz, vzx, vzz) they add to lambda_v
+//   x: hx (d1 + d2)(t0) + hz (d1 - d2)(t1) = d1(hx t0 + hz t1) + d2(hx t0 - hz t1)
+//   z: the same with t2, t3.
+// The stencils are linear, so T holds those four combinations and each needs
+// only one diagonal of the pair (40 taps a cell instead of 80).
+__device__ __forceinline__ void store_T(const AdjArgs &a, size_t i, float t0, float t1, float t2, float t3)
+{
+  a.T[0][i] = a.hx * t0 + a.hz * t1;
+  a.T[1][i] = a.hx * t0 - a.hz * t1;
+  a.T[2][i] = a.hx * t2 + a.hz * t3;
+  a.T[3][i] = a.hx * t2 - a.hz * t3;
+}
+
 // stress-half adjoint, local part: gradient sums, T0..T3, lambda_sigma *= coef1
-template <int V>
+template <int V, bool PK>
 __global__ void __launch_bounds__(BZ *BX) k_adj_stress_local(AdjArgs a)
 {
   pdl_sync();
@@ -289,14 +366,15 @@ __global__ void __launch_bounds__(BZ *BX) k_adj_stress_local(AdjArgs a)
   const int iz = blockIdx.x * BZ + threadIdx.x, ix = blockIdx.y * BX + threadIdx.y;
   if (!interior(g, ix, iz)) return;
   const size_t L = g.ldz, i = (size_t)ix * L + iz;
+  const SParams m = stress_params<PK, V>(a, i, cell_undamped(a, ix, iz));
+  const float la = a.lam[2][i], lb = a.lam[3][i], le = a.lam[4][i], b = m.b, c1 = m.c1;
+  const float c11 = m.c11, c13 = m.c13, c33 = m.c33, c55 = m.c55;
   float a1, a2, b1, b2;
   pair_s(a.keep[0], L, ix, iz, a1, a2);
   pair_s(a.keep[1], L, ix, iz, b1, b2);
   const float vxx = a.hx * (a1 + a2), vxz = a.hz * (a1 - a2), vzx = a.hx * (b1 + b2), vzz = a.hz * (b1 - b2);
   if (V == TTI_BOND) {  // sigma += coef2 H (vxx, vzz, vzx + vxz), H symmetric with c15, c35 (bond:836-873)
-    const float la = a.lam[2][i], lb = a.lam[3][i], le = a.lam[4][i], b = a.p.coef2[i], sh = vzx + vxz;
-    const float c11 = a.p.c11[i], c13 = a.p.c13[i], c15 = a.p.c15[i], c33 = a.p.c33[i], c35 = a.p.c35[i],
-                c55 = a.p.c55[i];
+    const float c15 = m.p, c35 = m.q, sh = vzx + vxz;
     a.acc[0][i] += b * la * vxx;
     a.acc[1][i] += b * (la * vzz + lb * vxx);
     a.acc[2][i] += b * lb * vzz;
@@ -304,11 +382,7 @@ __global__ void __launch_bounds__(BZ *BX) k_adj_stress_local(AdjArgs a)
     a.acc[4][i] += b * (la * sh + le * vxx);
     a.acc[5][i] += b * (lb * sh + le * vzz);
     const float Lsh = b * (c15 * la + c35 * lb + c55 * le);
-    a.T[0][i] = b * (c11 * la + c13 * lb + c15 * le);
-    a.T[1][i] = Lsh;
-    a.T[2][i] = Lsh;
-    a.T[3][i] = b * (c13 * la + c33 * lb + c35 * le);
-    const float c1 = a.p.coef1[i];
+    store_T(a, i, b * (c11 * la + c13 * lb + c15 * le), Lsh, Lsh, b * (c13 * la + c33 * lb + c35 * le));
     a.lam[2][i] = c1 * la;
     a.lam[3][i] = c1 * lb;
     a.lam[4][i] = c1 * le;
@@ -317,9 +391,7 @@ __global__ void __launch_bounds__(BZ *BX) k_adj_stress_local(AdjArgs a)
   if (V == TTI_TENSOR) {
     // forward (tensor:826-851): n = coef1 tau + coef2 H e(theta, v); tau' = n; sigma' = R(theta) n.
     // keep[2..4] hold tau before the stress half.
-    const float la = a.lam[2][i], lb = a.lam[3][i], le = a.lam[4][i], b = a.p.coef2[i], c1 = a.p.coef1[i];
-    const float s2 = a.p.s2[i], c2 = a.p.c2[i], st = a.p.s2t[i], cd = c2 - s2, sh = vxz + vzx;
-    const float c11 = a.p.c11[i], c13 = a.p.c13[i], c33 = a.p.c33[i], c55 = a.p.c55[i];
+    const float s2 = m.p, c2 = m.q, st = a.p.s2t[i], cd = c2 - s2, sh = vxz + vzx;
     const float exx = c2 * vxx + s2 * vzz - 0.5f * st * sh, ezz = s2 * vxx + c2 * vzz + 0.5f * st * sh;
     const float exz = st * (vxx - vzz) + cd * sh;
     const float nxx = c1 * a.keep[2][i] + b * (c11 * exx + c13 * ezz);
@@ -340,31 +412,22 @@ __global__ void __launch_bounds__(BZ *BX) k_adj_stress_local(AdjArgs a)
                    (la - lb) * rxx_ + le * rxz_;
     const float Lexx = b * (c11 * lxx + c13 * lzz), Lezz = b * (c13 * lxx + c33 * lzz), Lexz = b * c55 * lxz;
     const float Lsh = 0.5f * st * (Lezz - Lexx) + cd * Lexz;
-    a.T[0][i] = c2 * Lexx + s2 * Lezz + st * Lexz;
-    a.T[1][i] = Lsh;
-    a.T[2][i] = Lsh;
-    a.T[3][i] = s2 * Lexx + c2 * Lezz - st * Lexz;
+    store_T(a, i, c2 * Lexx + s2 * Lezz + st * Lexz, Lsh, Lsh, s2 * Lexx + c2 * Lezz - st * Lexz);
     a.lam[5][i] = c1 * lxx;
     a.lam[6][i] = c1 * lzz;
     a.lam[7][i] = c1 * lxz;
     a.lam[2][i] = a.lam[3][i] = a.lam[4][i] = 0.0f;  // sigma is overwritten by R tau
     return;
   }
-  const float s = a.p.sn[i], co = a.p.cs[i];
+  const float s = m.p, co = m.q;
   const float rxx = co * vxx - s * vxz, rxz = s * vxx + co * vxz;
   const float rzx = co * vzx - s * vzz, rzz = s * vzx + co * vzz;
-  const float la = a.lam[2][i], lb = a.lam[3][i], le = a.lam[4][i], b = a.p.coef2[i];
-  const float c11 = a.p.c11[i], c13 = a.p.c13[i], c33 = a.p.c33[i], c55 = a.p.c55[i];
   a.acc[0][i] += b * la * rxx;
   a.acc[1][i] += b * (la * rzz + lb * rxx);
   a.acc[2][i] += b * lb * rzz;
   a.acc[4][i] += b * (la * (c13 * rzx - c11 * rxz) + lb * (c33 * rzx - c13 * rxz) + le * c55 * (rxx - rzz));
   const float Lxx = b * (c11 * la + c13 * lb), Lzz = b * (c13 * la + c33 * lb), Lq = b * c55 * le;
-  a.T[0][i] = co * Lxx + s * Lq;
-  a.T[1][i] = co * Lq - s * Lxx;
-  a.T[2][i] = co * Lq + s * Lzz;
-  a.T[3][i] = co * Lzz - s * Lq;
-  const float c1 = a.p.coef1[i];
+  store_T(a, i, co * Lxx + s * Lq, co * Lq - s * Lxx, co * Lq + s * Lzz, co * Lzz - s * Lq);
   a.lam[2][i] = c1 * la;
   a.lam[3][i] = c1 * lb;
   a.lam[4][i] = c1 * le;
@@ -383,26 +446,26 @@ __global__ void __launch_bounds__(BZ *BX) k_adj_velocity(AdjArgs a)
   const float hx = a.hx, hz = a.hz;
   float lx, lz;
   {
-    float p1, p2, q1, q2, r1, r2, s1, s2;
-    pair_v(a.T[0], L, ix, iz, p1, p2);
-    pair_v(a.T[1], L, ix, iz, q1, q2);
-    pair_v(a.T[2], L, ix, iz, r1, r2);
-    pair_v(a.T[3], L, ix, iz, s1, s2);
-    lx = a.lam[0][i] - (hx * (p1 + p2) + hz * (q1 - q2));
-    lz = a.lam[1][i] - (hx * (r1 + r2) + hz * (s1 - s2));
+    float p1, q2, r1, s2, u;
+    pair_v(a.T[0], L, ix, iz, p1, u);
+    pair_v(a.T[1], L, ix, iz, u, q2);
+    pair_v(a.T[2], L, ix, iz, r1, u);
+    pair_v(a.T[3], L, ix, iz, u, s2);
+    lx = a.lam[0][i] - (p1 + q2);
+    lz = a.lam[1][i] - (r1 + s2);
   }
-  float a1, a2, b1, b2, e1, e2;
-  pair_v(a.keep[2], L, ix, iz, a1, a2);
-  pair_v(a.keep[3], L, ix, iz, b1, b2);
-  pair_v(a.keep[4], L, ix, iz, e1, e2);
-  const float sxx_x = hx * (a1 + a2), sxx_z = hx * (a1 - a2);  // 1/dx for both, as coord:633
-  const float szz_x = hx * (b1 + b2), szz_z = hz * (b1 - b2);
-  const float sxz_x = hx * (e1 + e2), sxz_z = hz * (e1 - e2);
   const float br = a.p.coef2[i] * a.p.invrho[i];
   const float Fx = br * lx, Fz = br * lz;
   // coordinate: rotation by theta_v; Bond: fx = sxx_x + sxz_z, fz = sxz_x + szz_z
   const float cv = V != TTI_COORDINATE ? 1.0f : a.p.csv[i], sv = V != TTI_COORDINATE ? 0.0f : a.p.snv[i];
-  if (V == TTI_COORDINATE) {
+  if (V == TTI_COORDINATE) {  // theta_v terms from the stencils of the kept sigma
+    float a1, a2, b1, b2, e1, e2;
+    pair_v(a.keep[2], L, ix, iz, a1, a2);
+    pair_v(a.keep[3], L, ix, iz, b1, b2);
+    pair_v(a.keep[4], L, ix, iz, e1, e2);
+    const float sxx_x = hx * (a1 + a2), sxx_z = hx * (a1 - a2);  // 1/dx for both, as coord:633
+    const float szz_x = hx * (b1 + b2), szz_z = hz * (b1 - b2);
+    const float sxz_x = hx * (e1 + e2), sxz_z = hz * (e1 - e2);
     a.acc[5][i] += Fx * (sxz_x - sxx_z) + Fz * (szz_x - sxz_z);
     a.acc[6][i] += Fx * (sxx_x + sxz_z) + Fz * (sxz_x + szz_z);
   }
@@ -494,19 +557,38 @@ __device__ __forceinline__ void vpair(const float *q, float &d1, float &d2)
   d2 = s2;
 }
 
+// one diagonal of the velocity-node pair of shared field q centred on (x, z)
+__device__ __forceinline__ float vdiag1(const float *q)
+{
+  constexpr int B = tiled::BZ;
+  float s = rsg(0) * (q[B + 1] - q[0]);
+#pragma unroll
+  for (int k = 2; k <= NH; ++k) s += rsg(k - 1) * (q[k * B + k] - q[(1 - k) * B + 1 - k]);
+  return s;
+}
+__device__ __forceinline__ float vdiag2(const float *q)
+{
+  constexpr int B = tiled::BZ;
+  float s = rsg(0) * (q[B] - q[1]);
+#pragma unroll
+  for (int k = 2; k <= NH; ++k) s += rsg(k - 1) * (q[k * B + 1 - k] - q[(1 - k) * B + k]);
+  return s;
+}
+
 // transposed stress stencils into lambda_v, then the velocity-half adjoint
-// (maps: T0..T3, kept sxx, szz, sxz)
+// (maps: T0..T3; coordinate: the theta_v terms from the kept stress
+// derivative combinations P Q R S that the forward velocity kernel wrote)
 template <int V>
-__global__ void __launch_bounds__(tiled::NT, 2) k_adj_velocity_tiled(const __grid_constant__ AdjTile at)
+__global__ void __launch_bounds__(tiled::NT, 3) k_adj_velocity_tiled(const __grid_constant__ AdjTile at)
 {
   pdl_sync();
   constexpr int F = tiled::FIELD, B = tiled::BZ;
   extern __shared__ __align__(128) float sm[];
-  unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm + 7 * F);
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm + 4 * F);
   const AdjArgs &a = at.a;
   const Grid &g = a.g;
   const TileCells c = tile_cells(at.z_base);
-  tiled::tma::issue_tiles(at.map, sm, bar, 7, c.z0, c.x0, 4);
+  tiled::tma::issue_tiles(at.map, sm, bar, 4, c.z0, c.x0, 4);
   const int z = c.z;
   const bool zin = z >= g.izStart && z < g.Nz - NH;
   if (!tiled::tma::wait_tiles(at.err, bar)) return;
@@ -518,24 +600,9 @@ __global__ void __launch_bounds__(tiled::NT, 2) k_adj_velocity_tiled(const __gri
     if (x >= g.Nx - NH) break;
     const size_t i = (size_t)x * g.ldz + z;
     const float *q = sm + (x - c.x0 + 4) * B + (z - c.z0 + 8);
-    float lx, lz;
-    {
-      float p1, p2, q1, q2;
-      vpair(q, p1, p2);
-      vpair(q + F, q1, q2);
-      lx = a.lam[0][i] - (hx * (p1 + p2) + hz * (q1 - q2));
-      vpair(q + 2 * F, p1, p2);
-      vpair(q + 3 * F, q1, q2);
-      lz = a.lam[1][i] - (hx * (p1 + p2) + hz * (q1 - q2));
-    }
-    float a1, a2, b1, b2, e1, e2;
-    vpair(q + 4 * F, a1, a2);
-    vpair(q + 5 * F, b1, b2);
-    vpair(q + 6 * F, e1, e2);
-    const float sxx_x = hx * (a1 + a2), sxx_z = hx * (a1 - a2);  // 1/dx for both, as coord:633
-    const float szz_x = hx * (b1 + b2), szz_z = hz * (b1 - b2);
-    const float sxz_x = hx * (e1 + e2), sxz_z = hz * (e1 - e2);
-    const float2 cf = __ldg(at.pk.cf + i);
+    const float lx = a.lam[0][i] - (vdiag1(q) + vdiag2(q + F));
+    const float lz = a.lam[1][i] - (vdiag1(q + 2 * F) + vdiag2(q + 3 * F));
+    const float2 cf = cell_undamped(a, x, z) ? make_float2(1.0f, a.dt) : __ldg(at.pk.cf + i);
     const float br = cf.y * __ldg(a.p.invrho + i);
     const float Fx = br * lx, Fz = br * lz;
     float sv = 0.0f, cv = 1.0f;  // tensor and Bond: fx = sxx_x + sxz_z, fz = sxz_x + szz_z
@@ -543,8 +610,9 @@ __global__ void __launch_bounds__(tiled::NT, 2) k_adj_velocity_tiled(const __gri
       const float2 vsc = __ldg(at.pk.vsc + i);
       sv = vsc.x;
       cv = vsc.y;
-      a.acc[5][i] += Fx * (sxz_x - sxx_z) + Fz * (szz_x - sxz_z);
-      a.acc[6][i] += Fx * (sxx_x + sxz_z) + Fz * (sxz_x + szz_z);
+      // P = sxz_x - sxx_z, Q = szz_x - sxz_z, R = sxx_x + sxz_z, S = sxz_x + szz_z
+      a.acc[5][i] += Fx * a.keep[2][i] + Fz * a.keep[3][i];
+      a.acc[6][i] += Fx * a.keep[4][i] + Fz * a.keep[5][i];
     }
     const float Axx_x = cv * Fx, Axx_z = -sv * Fx;
     const float Axz_x = sv * Fx + cv * Fz, Axz_z = cv * Fx - sv * Fz;
@@ -807,9 +875,13 @@ AdjArgs adj_args(tti_handle *h, int slot)
   for (int k = 0; k < 4; ++k) a.T[k] = s->T[k];
   for (int k = 0; k < 6; ++k) a.TV[k] = s->TV[k];
   for (int k = 0; k < 7; ++k) a.acc[k] = s->acc[k];
-  for (int k = 0; k < 5; ++k) a.keep[k] = s->keep + ((size_t)slot * 5 + k) * h->g.n;
+  for (int k = 0; k < 6; ++k) a.keep[k] = k < s->nkeep ? s->keep + ((size_t)slot * s->nkeep + k) * h->g.n : nullptr;
   a.hx = 0.5f * h->invdx;
   a.hz = 0.5f * h->invdz;
+  a.dt = h->cfg.dt;
+  a.pk = fused::Packed{h->pk_cf, h->pk_vsc, h->pk_sc, h->pk_c4};
+  a.undamped_ok = h->use_tiled && h->undamped_ok;
+  a.und_z0 = h->cfg.freesurface ? 0 : h->g.E;
   a.z_lo = h->cfg.freesurface ? std::max(NH, h->g.izStart - NH) : h->g.izStart;
   return a;
 }
@@ -963,9 +1035,10 @@ int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
     // the stress-half adjoint stays one thread per cell: it is bound by its
     // per-cell reads and writes, not by its two stencil fields
     const dim3 blk(BZ, BX), grd((g.Nz + BZ - 1) / BZ, (g.Nx + BX - 1) / BX);
-    if (c.variant == TTI_BOND) GCK(h, launch_pdl(k_adj_stress_local<TTI_BOND>, grd, blk, 0, h->stream, a));
-    else if (c.variant == TTI_TENSOR) GCK(h, launch_pdl(k_adj_stress_local<TTI_TENSOR>, grd, blk, 0, h->stream, a));
-    else GCK(h, launch_pdl(k_adj_stress_local<TTI_COORDINATE>, grd, blk, 0, h->stream, a));
+    if (c.variant == TTI_BOND) GCK(h, launch_pdl(k_adj_stress_local<TTI_BOND, true>, grd, blk, 0, h->stream, a));
+    else if (c.variant == TTI_TENSOR)
+      GCK(h, launch_pdl(k_adj_stress_local<TTI_TENSOR, true>, grd, blk, 0, h->stream, a));
+    else GCK(h, launch_pdl(k_adj_stress_local<TTI_COORDINATE, true>, grd, blk, 0, h->stream, a));
     if (int rc = launch_vsource(h, a, it)) return rc;
     AdjTile at;
     memset(&at, 0, sizeof at);
@@ -973,19 +1046,18 @@ int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
     at.pk = fused::Packed{h->pk_cf, h->pk_vsc, h->pk_sc, h->pk_c4};
     at.err = h->d_flag;
     for (int k = 0; k < 4; ++k) at.map[k] = s->maps[k];
-    for (int f = 0; f < 3; ++f) at.map[4 + f] = s->slot_maps[(size_t)slot * 3 + f];  // kept sxx, szz, sxz
     if (c.variant == TTI_COORDINATE)
-      GCK(h, launch_adj_tile(k_adj_velocity_tiled<TTI_COORDINATE>, at, 7, g.izStart, g, h->stream));
+      GCK(h, launch_adj_tile(k_adj_velocity_tiled<TTI_COORDINATE>, at, 4, g.izStart, g, h->stream));
     else  // tensor and Bond: no rotation at the velocity node
-      GCK(h, launch_adj_tile(k_adj_velocity_tiled<TTI_BOND>, at, 7, g.izStart, g, h->stream));
+      GCK(h, launch_adj_tile(k_adj_velocity_tiled<TTI_BOND>, at, 4, g.izStart, g, h->stream));
     for (int k = 0; k < 6; ++k) at.map[k] = s->maps[4 + k];
     GCK(h, launch_adj_tile(k_adj_vstencil_tiled, at, 6, a.z_lo, g, h->stream));
     return TTI_OK;
   }
   const dim3 blk(BZ, BX), grd((g.Nz + BZ - 1) / BZ, (g.Nx + BX - 1) / BX);
-  if (c.variant == TTI_BOND) k_adj_stress_local<TTI_BOND><<<grd, blk, 0, h->stream>>>(a);
-  else if (c.variant == TTI_TENSOR) k_adj_stress_local<TTI_TENSOR><<<grd, blk, 0, h->stream>>>(a);
-  else k_adj_stress_local<TTI_COORDINATE><<<grd, blk, 0, h->stream>>>(a);
+  if (c.variant == TTI_BOND) k_adj_stress_local<TTI_BOND, false><<<grd, blk, 0, h->stream>>>(a);
+  else if (c.variant == TTI_TENSOR) k_adj_stress_local<TTI_TENSOR, false><<<grd, blk, 0, h->stream>>>(a);
+  else k_adj_stress_local<TTI_COORDINATE, false><<<grd, blk, 0, h->stream>>>(a);
   if (int rc = launch_vsource(h, a, it)) return rc;
   if (c.variant == TTI_COORDINATE) k_adj_velocity<TTI_COORDINATE><<<grd, blk, 0, h->stream>>>(a);
   else k_adj_velocity<TTI_BOND><<<grd, blk, 0, h->stream>>>(a);  // tensor and Bond: no rotation at the velocity node
@@ -1017,7 +1089,6 @@ void grad_release(tti_handle *h)
   cudaFree(s->vrim_acc);
   cudaFree(s->d_J);
   free(s->maps);
-  free(s->slot_maps);
   delete s;
   h->grad = nullptr;
 }
@@ -1078,33 +1149,20 @@ int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
   ncheck = std::min(ncheck, nt);
   const int seg = (nt + ncheck - 1) / ncheck, nseg = (nt + seg - 1) / seg;
   const int nf = h->cfg.variant == TTI_TENSOR ? 8 : 5;  // fields of a full state (checkpoints)
-  const size_t n = h->g.n, state = 5 * n;
-  if (s->ncheck != nseg || s->seg != seg) {
+  const int nk = keep_fields(h);                       // fields of a kept step
+  const size_t n = h->g.n;
+  if (s->ncheck != nseg || s->seg != seg || s->nkeep != nk) {
     cudaFree(s->ckpt);
     cudaFree(s->keep);
     s->ckpt = s->keep = nullptr;
-    s->slot_maps_n = 0;  // the kept-state tensor maps point into the old buffer
     if (cudaMalloc(&s->ckpt, sizeof(float) * nf * n * std::max(1, nseg - 1)) != cudaSuccess ||
-        cudaMalloc(&s->keep, sizeof(float) * state * seg) != cudaSuccess) {
-      s->ncheck = s->seg = 0;
+        cudaMalloc(&s->keep, sizeof(float) * nk * n * seg) != cudaSuccess) {
+      s->ncheck = s->seg = s->nkeep = 0;
       return gerr(h, TTI_ERR_NOMEM, "device allocation of the checkpoints failed (use fewer steps per segment)");
     }
     s->ncheck = nseg;
     s->seg = seg;
-  }
-  if (h->use_tiled && s->slot_maps_n != seg) {
-    free(s->slot_maps);
-    s->slot_maps = nullptr;
-    s->slot_maps_n = 0;
-    void *mem = nullptr;
-    if (posix_memalign(&mem, 64, sizeof(CUtensorMap) * 3 * (size_t)seg) != 0)
-      return gerr(h, TTI_ERR_NOMEM, "host allocation failed");
-    s->slot_maps = static_cast<CUtensorMap *>(mem);
-    for (int k = 0; k < seg; ++k)
-      for (int f = 0; f < 3; ++f)
-        if (!tiled::encode_map(s->slot_maps + (size_t)k * 3 + f, h->g, s->keep + ((size_t)k * 5 + 2 + f) * n))
-          return gerr(h, TTI_ERR_CUDA, "cuTensorMapEncodeTiled failed");
-    s->slot_maps_n = seg;
+    s->nkeep = nk;
   }
   if (s->gsrc_n != h->nsrc * nt) {
     cudaFree(s->gsrc);
@@ -1127,8 +1185,8 @@ int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
         GCK(h, cudaMemcpyAsync(s->ckpt + ((size_t)q * nf + f) * n, h->fld[f], n * sizeof(float),
                                cudaMemcpyDeviceToDevice, h->stream));
     for (int k = q * seg; k < std::min(nt, (q + 1) * seg); ++k) {
-      float *keep[5];
-      for (int f = 0; f < 5; ++f) keep[f] = s->keep + ((size_t)(k - q * seg) * 5 + f) * n;
+      float *keep[6] = {};
+      for (int f = 0; f < nk; ++f) keep[f] = s->keep + ((size_t)(k - q * seg) * nk + f) * n;
       if ((rc = handle_step(h, tab, last ? keep : nullptr))) return rc;
     }
   }
@@ -1157,8 +1215,8 @@ int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
                                cudaMemcpyDeviceToDevice, h->stream));
       h->step_index = k0;
       for (int k = k0; k < k1; ++k) {
-        float *keep[5];
-        for (int f = 0; f < 5; ++f) keep[f] = s->keep + ((size_t)(k - k0) * 5 + f) * n;
+        float *keep[6] = {};
+        for (int f = 0; f < nk; ++f) keep[f] = s->keep + ((size_t)(k - k0) * nk + f) * n;
         if ((rc = handle_step(h, tab, keep))) return rc;
       }
     }

@@ -178,7 +178,13 @@ int launch_one_step(tti_handle *h, const SourceTables &tab, cudaEvent_t *ev = nu
     h->step_index++;
     return TTI_OK;
   }
-  tiled::HalfArgs ha;
+  tiled::HalfArgs ha{};
+  // what the gradient keeps of this step (the adjoint reads it per cell)
+  //   coordinate, tiled: vx vz, then the stress derivative combinations that
+  //     the velocity kernel writes (P Q R S, HalfArgs::kd)
+  //   coordinate, per-cell kernels: vx vz sxx szz sxz (the adjoint takes the stencils)
+  //   tensor: vx vz txx tzz txz; Bond: vx vz
+  const bool keep_kd = keep && h->use_tiled && c.variant == TTI_COORDINATE;
   if (h->use_tiled) {
     const CUtensorMap *tm = static_cast<const CUtensorMap *>(h->tmaps);
     ha.g = h->g;
@@ -196,16 +202,18 @@ int launch_one_step(tti_handle *h, const SourceTables &tab, cudaEvent_t *ev = nu
     ha.map[0] = tm[2];  // sxx szz sxz for the velocity update
     ha.map[1] = tm[3];
     ha.map[2] = tm[4];
+    if (keep_kd)
+      for (int k = 0; k < 4; ++k) ha.kd[k] = keep[2 + k];
   }
   if (ev) CK(h, cudaEventRecord(ev[0], h->stream));
   if (h->use_tiled) CK(h, tiled::launch_velocity(ha, c.variant, h->exact, h->stream));
   else launch_velocity(a, h->stream);
   if (ev) CK(h, cudaEventRecord(ev[1], h->stream));
   if (vsrc) launch_sources(a, s, &tab, c.stype, 0, it, h->stream);
-  if (keep) {  // vx vz, and sxx szz sxz (tensor: txx tzz txz, which the tensor adjoint reads)
+  if (keep) {  // v after the sources, and sigma or tau where the adjoint reads them
     const bool t = c.variant == TTI_TENSOR;
     float *const src[5] = {h->fld[0], h->fld[1], h->fld[t ? 5 : 2], h->fld[t ? 6 : 3], h->fld[t ? 7 : 4]};
-    launch_copy5(src, keep, h->g.n, h->stream);
+    launch_copy5(src, keep, keep_fields(h) == 5 ? 5 : 2, h->g.n, h->stream);
     h->launches++;
   }
   if (ev) CK(h, cudaEventRecord(ev[2], h->stream));
@@ -321,6 +329,12 @@ int copy_out_pitched(tti_handle *h, const float *src, float *out)
 }  // namespace
 
 namespace ttifd {
+int keep_fields(const tti_handle *h)
+{
+  if (h->cfg.variant == TTI_TENSOR) return 5;
+  if (h->cfg.variant == TTI_BOND) return 2;
+  return h->use_tiled ? 6 : 5;
+}
 StepArgs handle_step_args(const tti_handle *h) { return step_args(h); }
 void handle_source_tables(const tti_handle *h, SourceTables *t) { source_tables(h, t); }
 int handle_step(tti_handle *h, const SourceTables &tab, float *const *keep)

@@ -91,7 +91,7 @@ int build_tables(tti_batch *b)
     const tti_config &c = h->cfg;
     const StepArgs a = handle_step_args(h);
     const CUtensorMap *tm = static_cast<const CUtensorMap *>(h->tmaps);
-    tiled::HalfArgs ha;
+    tiled::HalfArgs ha{};
     memset(&ha, 0, sizeof ha);
     ha.g = h->g;
     ha.f = a.f;

@@ -90,7 +90,8 @@ void launch_post_batch(const BatchPost *d, int n, int maxNx, const int *step, cu
 void launch_sources_batch(const BatchSrc *d, int n, const int *step, cudaStream_t st);
 void launch_advance(int *step, cudaStream_t st);
 // dst[f][0..n) = src[f][0..n), f < 5 (n a multiple of 4, 16-byte aligned arrays)
-void launch_copy5(float *const *src, float *const *dst, size_t n, cudaStream_t st);
+// the first nf (<= 5) of the arrays src[] into dst[], n floats each, one launch
+void launch_copy5(float *const *src, float *const *dst, int nf, size_t n, cudaStream_t st);
 // out[r - r0][t] = in[t][r] for t < nts, r0 <= r < r0 + nr (in has n columns)
 void launch_transpose(const float *in, float *out, int nts, int n, int r0, int nr, cudaStream_t st);
 // Pack a snapshot (kind 1..7) of the physical (savew = 0) or padded area
@@ -104,6 +105,12 @@ int handle_check_flag(tti_handle *h);
 // one time step; `keep` (5 device arrays or null) receives vx vz sxx szz sxz
 // between the velocity sources and the stress update
 int handle_step(tti_handle *h, const SourceTables &tab, float *const *keep);
+// Fields of one kept step of the gradient (the arrays `keep` of handle_step
+// points at): 6 for the coordinate rotation on the tiled kernels (vx vz and
+// the stress derivative combinations P Q R S), 5 on the per-cell kernels
+// (vx vz sxx szz sxz) and for the tensor rotation (vx vz txx tzz txz), 2 for
+// Bond (vx vz).
+int keep_fields(const tti_handle *h);
 // frees the gradient's device memory of h (adjoint.cu)
 void grad_release(tti_handle *h);
 int create_handle(tti_handle **out, const tti_config *cfg, int device, const tti_handle *share, bool force_tiled);

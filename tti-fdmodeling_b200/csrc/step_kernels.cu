@@ -468,26 +468,29 @@ void launch_sources_batch(const BatchSrc *d, int n, const int *step, cudaStream_
   if (n > 0) k_sources_batch<<<n, 128, 0, st>>>(d, step);
 }
 
-// five state arrays copied in one launch (the gradient's kept states)
+// up to five state arrays copied in one launch (the gradient's kept states)
 struct Copy5 {
   const float4 *src[5];
   float4 *dst[5];
+  int nf;
 };
 __global__ void k_copy5(Copy5 c, size_t n4)
 {
   pdl_sync();
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n4; q += (size_t)gridDim.x * blockDim.x) {
 #pragma unroll
-    for (int f = 0; f < 5; ++f) c.dst[f][q] = c.src[f][q];
+    for (int f = 0; f < 5; ++f)
+      if (f < c.nf) c.dst[f][q] = c.src[f][q];
   }
 }
 
-void launch_copy5(float *const *src, float *const *dst, size_t n, cudaStream_t st)
+void launch_copy5(float *const *src, float *const *dst, int nf, size_t n, cudaStream_t st)
 {
   Copy5 c;
+  c.nf = std::min(nf, 5);
   for (int f = 0; f < 5; ++f) {
-    c.src[f] = reinterpret_cast<const float4 *>(src[f]);
-    c.dst[f] = reinterpret_cast<float4 *>(dst[f]);
+    c.src[f] = f < c.nf ? reinterpret_cast<const float4 *>(src[f]) : nullptr;
+    c.dst[f] = f < c.nf ? reinterpret_cast<float4 *>(dst[f]) : nullptr;
   }
   const size_t n4 = n / 4;
   launch_pdl(k_copy5, dim3((unsigned)std::min<size_t>((n4 + 255) / 256, 148 * 16)), dim3(256), 0, st, c, n4);

@@ -41,7 +41,6 @@ __device__ __forceinline__ Cells cells_of(const HalfArgs &a, int tz, int tx)
 }
 
 // true when every cell of the tile lies where coef1 = 1 and coef2 = dt
-// true when every cell of the tile lies where coef1 = 1 and coef2 = dt
 __device__ __forceinline__ bool tile_undamped(const HalfArgs &a, const Cells &c)
 {
   const Grid &g = a.g;
@@ -58,7 +57,7 @@ __device__ __forceinline__ float coef(const HalfArgs &a, int k)
   return Q ? a.hc[k] : rsg(k);
 }
 
-template <int V, bool X, bool Q>
+template <int V, bool X, bool Q, bool K = false>
 __device__ __forceinline__ void velocity_tile(const HalfArgs &a, const CUtensorMap *map, float *sm, int tz, int tx)
 {
   using A = Ar<X>;
@@ -121,6 +120,12 @@ __device__ __forceinline__ void velocity_tile(const HalfArgs &a, const CUtensorM
       const float szz_x = dx_(1);
       fx = A::add(A::add(A::sub(A::mul(cv, sxx_x), A::mul(sv, sxx_z)), A::mul(sv, sxz_x)), A::mul(cv, sxz_z));
       fz = A::add(A::add(A::sub(A::mul(cv, sxz_x), A::mul(sv, sxz_z)), A::mul(sv, szz_x)), A::mul(cv, szz_z));
+      if (K) {
+        a.kd[0][gi] = sxz_x - sxx_z;
+        a.kd[1][gi] = szz_x - sxz_z;
+        a.kd[2][gi] = sxx_x + sxz_z;
+        a.kd[3][gi] = sxz_x + szz_z;
+      }
     } else {
       fx = A::add(sxx_x, sxz_z);
       fz = A::add(sxz_x, szz_z);
@@ -272,12 +277,12 @@ __device__ __forceinline__ const HalfArgs *stage_args(const HalfArgs *src, float
   return dst;
 }
 
-template <int V, bool X, bool Q>
+template <int V, bool X, bool Q, bool K = false>
 __global__ void __launch_bounds__(NT, 4) k_velocity_tiled(const __grid_constant__ HalfArgs a)
 {
   extern __shared__ __align__(128) float sm[];
   pdl_sync();
-  velocity_tile<V, X, Q>(a, a.map, sm, blockIdx.x, blockIdx.y);
+  velocity_tile<V, X, Q, K>(a, a.map, sm, blockIdx.x, blockIdx.y);
 }
 
 template <int V, bool X, bool Q>
@@ -381,6 +386,7 @@ bool encode_map(CUtensorMap *map, const Grid &g, float *field)
 template <bool X, bool Q>
 cudaError_t velocity_xq(const HalfArgs &a, int variant, cudaStream_t st)
 {
+  if (variant == TTI_COORDINATE && a.kd[0]) return launch_k(k_velocity_tiled<TTI_COORDINATE, X, Q, true>, a, 3, st);
   if (variant == TTI_COORDINATE) return launch_k(k_velocity_tiled<TTI_COORDINATE, X, Q>, a, 3, st);
   if (variant == TTI_TENSOR) return launch_k(k_velocity_tiled<TTI_TENSOR, X, Q>, a, 3, st);
   return launch_k(k_velocity_tiled<TTI_BOND, X, Q>, a, 3, st);
