@@ -76,7 +76,7 @@ struct AdjArgs {
   float *T[4];
   float *TV[6];
   float *acc[7];
-  const float *keep[6];  // this step's kept fields (keep_fields), null past them
+  const float *keep[8];  // this step's kept fields (keep_fields), null past them
   float hx, hz, dt;
   int z_lo;         // first row of the transposed velocity stencils
   int undamped_ok;  // coef1 == 1, coef2 == dt on [E, Nx - E) x [und_z0, Nz - E) (checked at upload)
@@ -357,7 +357,10 @@ __device__ __forceinline__ void store_T(const AdjArgs &a, size_t i, float t0, fl
   a.T[3][i] = a.hx * t2 - a.hz * t3;
 }
 
-// stress-half adjoint, local part: gradient sums, T0..T3, lambda_sigma *= coef1
+// stress-half adjoint, local part: gradient sums, T0..T3, lambda_sigma *= coef1.
+// PK (tiled path): packed parameters, and the strain rates the forward stress
+// kernel kept (keep[0..3], tensor tau keep[4..6]); otherwise the stencils of
+// the kept v (keep[0..1], tensor tau keep[2..4]).
 template <int V, bool PK>
 __global__ void __launch_bounds__(BZ *BX) k_adj_stress_local(AdjArgs a)
 {
@@ -369,10 +372,22 @@ __global__ void __launch_bounds__(BZ *BX) k_adj_stress_local(AdjArgs a)
   const SParams m = stress_params<PK, V>(a, i, cell_undamped(a, ix, iz));
   const float la = a.lam[2][i], lb = a.lam[3][i], le = a.lam[4][i], b = m.b, c1 = m.c1;
   const float c11 = m.c11, c13 = m.c13, c33 = m.c33, c55 = m.c55;
-  float a1, a2, b1, b2;
-  pair_s(a.keep[0], L, ix, iz, a1, a2);
-  pair_s(a.keep[1], L, ix, iz, b1, b2);
-  const float vxx = a.hx * (a1 + a2), vxz = a.hz * (a1 - a2), vzx = a.hx * (b1 + b2), vzz = a.hz * (b1 - b2);
+  float vxx, vxz, vzx, vzz;
+  if (PK) {
+    vxx = a.keep[0][i];
+    vxz = a.keep[1][i];
+    vzx = a.keep[2][i];
+    vzz = a.keep[3][i];
+  } else {
+    float a1, a2, b1, b2;
+    pair_s(a.keep[0], L, ix, iz, a1, a2);
+    pair_s(a.keep[1], L, ix, iz, b1, b2);
+    vxx = a.hx * (a1 + a2);
+    vxz = a.hz * (a1 - a2);
+    vzx = a.hx * (b1 + b2);
+    vzz = a.hz * (b1 - b2);
+  }
+  const float *const *tau = a.keep + (PK ? 4 : 2);
   if (V == TTI_BOND) {  // sigma += coef2 H (vxx, vzz, vzx + vxz), H symmetric with c15, c35 (bond:836-873)
     const float c15 = m.p, c35 = m.q, sh = vzx + vxz;
     a.acc[0][i] += b * la * vxx;
@@ -389,14 +404,14 @@ __global__ void __launch_bounds__(BZ *BX) k_adj_stress_local(AdjArgs a)
     return;
   }
   if (V == TTI_TENSOR) {
-    // forward (tensor:826-851): n = coef1 tau + coef2 H e(theta, v); tau' = n; sigma' = R(theta) n.
-    // keep[2..4] hold tau before the stress half.
+    // forward (tensor:826-851): n = coef1 tau + coef2 H e(theta, v); tau' = n; sigma' = R(theta) n,
+    // with tau the kept one from before the stress half.
     const float s2 = m.p, c2 = m.q, st = a.p.s2t[i], cd = c2 - s2, sh = vxz + vzx;
     const float exx = c2 * vxx + s2 * vzz - 0.5f * st * sh, ezz = s2 * vxx + c2 * vzz + 0.5f * st * sh;
     const float exz = st * (vxx - vzz) + cd * sh;
-    const float nxx = c1 * a.keep[2][i] + b * (c11 * exx + c13 * ezz);
-    const float nzz = c1 * a.keep[3][i] + b * (c13 * exx + c33 * ezz);
-    const float nxz = c1 * a.keep[4][i] + b * c55 * exz;
+    const float nxx = c1 * tau[0][i] + b * (c11 * exx + c13 * ezz);
+    const float nzz = c1 * tau[1][i] + b * (c13 * exx + c33 * ezz);
+    const float nxz = c1 * tau[2][i] + b * c55 * exz;
     // lambda_n = lambda_tau' + R^T lambda_sigma'
     const float lxx = a.lam[5][i] + c2 * la + s2 * lb - 0.5f * st * le;
     const float lzz = a.lam[6][i] + s2 * la + c2 * lb + 0.5f * st * le;
@@ -611,8 +626,8 @@ __global__ void __launch_bounds__(tiled::NT, 3) k_adj_velocity_tiled(const __gri
       sv = vsc.x;
       cv = vsc.y;
       // P = sxz_x - sxx_z, Q = szz_x - sxz_z, R = sxx_x + sxz_z, S = sxz_x + szz_z
-      a.acc[5][i] += Fx * a.keep[2][i] + Fz * a.keep[3][i];
-      a.acc[6][i] += Fx * a.keep[4][i] + Fz * a.keep[5][i];
+      a.acc[5][i] += Fx * a.keep[4][i] + Fz * a.keep[5][i];
+      a.acc[6][i] += Fx * a.keep[6][i] + Fz * a.keep[7][i];
     }
     const float Axx_x = cv * Fx, Axx_z = -sv * Fx;
     const float Axz_x = sv * Fx + cv * Fz, Axz_z = cv * Fx - sv * Fz;
@@ -875,7 +890,7 @@ AdjArgs adj_args(tti_handle *h, int slot)
   for (int k = 0; k < 4; ++k) a.T[k] = s->T[k];
   for (int k = 0; k < 6; ++k) a.TV[k] = s->TV[k];
   for (int k = 0; k < 7; ++k) a.acc[k] = s->acc[k];
-  for (int k = 0; k < 6; ++k) a.keep[k] = k < s->nkeep ? s->keep + ((size_t)slot * s->nkeep + k) * h->g.n : nullptr;
+  for (int k = 0; k < 8; ++k) a.keep[k] = k < s->nkeep ? s->keep + ((size_t)slot * s->nkeep + k) * h->g.n : nullptr;
   a.hx = 0.5f * h->invdx;
   a.hz = 0.5f * h->invdz;
   a.dt = h->cfg.dt;
@@ -1185,7 +1200,7 @@ int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
         GCK(h, cudaMemcpyAsync(s->ckpt + ((size_t)q * nf + f) * n, h->fld[f], n * sizeof(float),
                                cudaMemcpyDeviceToDevice, h->stream));
     for (int k = q * seg; k < std::min(nt, (q + 1) * seg); ++k) {
-      float *keep[6] = {};
+      float *keep[8] = {};
       for (int f = 0; f < nk; ++f) keep[f] = s->keep + ((size_t)(k - q * seg) * nk + f) * n;
       if ((rc = handle_step(h, tab, last ? keep : nullptr))) return rc;
     }
@@ -1215,7 +1230,7 @@ int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
                                cudaMemcpyDeviceToDevice, h->stream));
       h->step_index = k0;
       for (int k = k0; k < k1; ++k) {
-        float *keep[6] = {};
+        float *keep[8] = {};
         for (int f = 0; f < nk; ++f) keep[f] = s->keep + ((size_t)(k - k0) * nk + f) * n;
         if ((rc = handle_step(h, tab, keep))) return rc;
       }

@@ -179,12 +179,13 @@ int launch_one_step(tti_handle *h, const SourceTables &tab, cudaEvent_t *ev = nu
     return TTI_OK;
   }
   tiled::HalfArgs ha{};
-  // what the gradient keeps of this step (the adjoint reads it per cell)
-  //   coordinate, tiled: vx vz, then the stress derivative combinations that
-  //     the velocity kernel writes (P Q R S, HalfArgs::kd)
-  //   coordinate, per-cell kernels: vx vz sxx szz sxz (the adjoint takes the stencils)
-  //   tensor: vx vz txx tzz txz; Bond: vx vz
-  const bool keep_kd = keep && h->use_tiled && c.variant == TTI_COORDINATE;
+  // What the gradient keeps of this step (keep_fields). Tiled kernels: the
+  // stress kernel writes the strain rates vxx vxz vzx vzz (keep[0..3]) and for
+  // the tensor rotation the tau it starts from (keep[4..6]); the coordinate
+  // velocity kernel writes the stress derivative combinations P Q R S
+  // (keep[4..7]). Per-cell kernels: a copy of vx vz and sxx szz sxz (tensor:
+  // txx tzz txz) after the sources, from whose stencils the adjoint works.
+  const bool keep_tiled = keep && h->use_tiled;
   if (h->use_tiled) {
     const CUtensorMap *tm = static_cast<const CUtensorMap *>(h->tmaps);
     ha.g = h->g;
@@ -202,18 +203,18 @@ int launch_one_step(tti_handle *h, const SourceTables &tab, cudaEvent_t *ev = nu
     ha.map[0] = tm[2];  // sxx szz sxz for the velocity update
     ha.map[1] = tm[3];
     ha.map[2] = tm[4];
-    if (keep_kd)
-      for (int k = 0; k < 4; ++k) ha.kd[k] = keep[2 + k];
+    if (keep_tiled && c.variant == TTI_COORDINATE)
+      for (int k = 0; k < 4; ++k) ha.kd[k] = keep[4 + k];
   }
   if (ev) CK(h, cudaEventRecord(ev[0], h->stream));
   if (h->use_tiled) CK(h, tiled::launch_velocity(ha, c.variant, h->exact, h->stream));
   else launch_velocity(a, h->stream);
   if (ev) CK(h, cudaEventRecord(ev[1], h->stream));
   if (vsrc) launch_sources(a, s, &tab, c.stype, 0, it, h->stream);
-  if (keep) {  // v after the sources, and sigma or tau where the adjoint reads them
+  if (keep && !keep_tiled) {  // v after the sources, and sigma or tau
     const bool t = c.variant == TTI_TENSOR;
     float *const src[5] = {h->fld[0], h->fld[1], h->fld[t ? 5 : 2], h->fld[t ? 6 : 3], h->fld[t ? 7 : 4]};
-    launch_copy5(src, keep, keep_fields(h) == 5 ? 5 : 2, h->g.n, h->stream);
+    launch_copy5(src, keep, 5, h->g.n, h->stream);
     h->launches++;
   }
   if (ev) CK(h, cudaEventRecord(ev[2], h->stream));
@@ -221,6 +222,8 @@ int launch_one_step(tti_handle *h, const SourceTables &tab, cudaEvent_t *ev = nu
     const CUtensorMap *tm = static_cast<const CUtensorMap *>(h->tmaps);
     ha.map[0] = tm[0];  // vx vz for the stress update
     ha.map[1] = tm[1];
+    for (int k = 0; k < 4; ++k) ha.kd[k] = keep_tiled ? keep[k] : nullptr;
+    for (int k = 0; k < 3; ++k) ha.kt[k] = keep_tiled && c.variant == TTI_TENSOR ? keep[4 + k] : nullptr;
     CK(h, tiled::launch_stress(ha, c.variant, h->exact, h->stream));
   } else {
     launch_stress(a, h->stream);
@@ -331,9 +334,8 @@ int copy_out_pitched(tti_handle *h, const float *src, float *out)
 namespace ttifd {
 int keep_fields(const tti_handle *h)
 {
-  if (h->cfg.variant == TTI_TENSOR) return 5;
-  if (h->cfg.variant == TTI_BOND) return 2;
-  return h->use_tiled ? 6 : 5;
+  if (!h->use_tiled) return 5;
+  return h->cfg.variant == TTI_COORDINATE ? 8 : h->cfg.variant == TTI_TENSOR ? 7 : 4;
 }
 StepArgs handle_step_args(const tti_handle *h) { return step_args(h); }
 void handle_source_tables(const tti_handle *h, SourceTables *t) { source_tables(h, t); }

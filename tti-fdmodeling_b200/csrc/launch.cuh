@@ -104,12 +104,13 @@ void handle_source_tables(const tti_handle *h, SourceTables *t);
 int handle_check_flag(tti_handle *h);
 // one time step; `keep` (5 device arrays or null) receives vx vz sxx szz sxz
 // between the velocity sources and the stress update
-int handle_step(tti_handle *h, const SourceTables &tab, float *const *keep);
+int handle_step(tti_handle *h, const SourceTables &tab, float *const *keep);  // keep: 8 pointers or null
 // Fields of one kept step of the gradient (the arrays `keep` of handle_step
-// points at): 6 for the coordinate rotation on the tiled kernels (vx vz and
-// the stress derivative combinations P Q R S), 5 on the per-cell kernels
-// (vx vz sxx szz sxz) and for the tensor rotation (vx vz txx tzz txz), 2 for
-// Bond (vx vz).
+// points at). Tiled kernels: the strain rates vxx vxz vzx vzz, then for the
+// coordinate rotation the stress derivative combinations P Q R S (8 fields),
+// for the tensor rotation txx tzz txz before the stress half (7), for Bond
+// nothing more (4). Per-cell kernels: vx vz after the velocity half and the
+// stresses (tensor: tau) before the stress half (5).
 int keep_fields(const tti_handle *h);
 // frees the gradient's device memory of h (adjoint.cu)
 void grad_release(tti_handle *h);

@@ -33,10 +33,13 @@ struct alignas(64) HalfArgs {
   int tiles_z; // batched launches: tile rows of this instance's grid
   int square;  // FMA mode with dx == dz: stencil coefficients hc fold in h = 0.5 / dx
   float hc[5]; // h * C_k
-  // coordinate velocity update, gradient forward pass: per cell the stress
-  // derivative combinations the adjoint's theta_v terms need
-  // (sxz_x - sxx_z, szz_x - sxz_z, sxx_x + sxz_z, sxz_x + szz_z); null: none
+  // Gradient forward pass (null: nothing kept). Velocity update, coordinate
+  // rotation: per cell the stress derivative combinations the adjoint's
+  // theta_v terms need (sxz_x - sxx_z, szz_x - sxz_z, sxx_x + sxz_z,
+  // sxz_x + szz_z). Stress update: the strain rates vxx vxz vzx vzz (not
+  // rotated), and for the tensor rotation the tau it starts from (kt).
   float *kd[4];
+  float *kt[3];
 };
 
 // Sets square / hc for FMA-mode launches on grids with dx == dz.

@@ -213,7 +213,7 @@ __device__ __forceinline__ void stress_store(const HalfArgs &a, size_t gi, float
 }
 
 // Stress update of tile (tz, tx); `map` holds the tensor maps of vx, vz.
-template <int V, bool X, bool Q>
+template <int V, bool X, bool Q, bool K = false>
 __device__ __forceinline__ void stress_tile(const HalfArgs &a, const CUtensorMap *map, float *sm, int tz, int tx)
 {
   using A = Ar<X>;
@@ -255,6 +255,17 @@ __device__ __forceinline__ void stress_tile(const HalfArgs &a, const CUtensorMap
     const float vxz = Q ? d[0][0] - d[0][1] : A::mul(A::mul(0.5f, A::sub(d[0][0], d[0][1])), invdz);
     const float vzx = Q ? d[1][0] + d[1][1] : A::mul(A::mul(0.5f, A::add(d[1][0], d[1][1])), invdx);
     const float vzz = Q ? d[1][0] - d[1][1] : A::mul(A::mul(0.5f, A::sub(d[1][0], d[1][1])), invdz);
+    if (K) {
+      a.kd[0][gi] = vxx;
+      a.kd[1][gi] = vxz;
+      a.kd[2][gi] = vzx;
+      a.kd[3][gi] = vzz;
+      if (V == TTI_TENSOR) {
+        a.kt[0][gi] = p.o0;
+        a.kt[1][gi] = p.o1;
+        a.kt[2][gi] = p.o2;
+      }
+    }
     stress_store<V, X>(a, gi, vxx, vxz, vzx, vzz, p);
   }
 }
@@ -277,20 +288,22 @@ __device__ __forceinline__ const HalfArgs *stage_args(const HalfArgs *src, float
   return dst;
 }
 
+// K (the gradient's forward pass also writes what the adjoint keeps): three
+// CTAs per SM, so the extra live values fit in registers without spilling
 template <int V, bool X, bool Q, bool K = false>
-__global__ void __launch_bounds__(NT, 4) k_velocity_tiled(const __grid_constant__ HalfArgs a)
+__global__ void __launch_bounds__(NT, K ? 3 : 4) k_velocity_tiled(const __grid_constant__ HalfArgs a)
 {
   extern __shared__ __align__(128) float sm[];
   pdl_sync();
   velocity_tile<V, X, Q, K>(a, a.map, sm, blockIdx.x, blockIdx.y);
 }
 
-template <int V, bool X, bool Q>
-__global__ void __launch_bounds__(NT, 4) k_stress_tiled(const __grid_constant__ HalfArgs a)
+template <int V, bool X, bool Q, bool K = false>
+__global__ void __launch_bounds__(NT, K ? 3 : 4) k_stress_tiled(const __grid_constant__ HalfArgs a)
 {
   extern __shared__ __align__(128) float sm[];
   pdl_sync();
-  stress_tile<V, X, Q>(a, a.map, sm, blockIdx.x, blockIdx.y);
+  stress_tile<V, X, Q, K>(a, a.map, sm, blockIdx.x, blockIdx.y);
 }
 
 template <int V, bool X, bool Q>
@@ -395,9 +408,14 @@ cudaError_t velocity_xq(const HalfArgs &a, int variant, cudaStream_t st)
 template <bool X, bool Q>
 cudaError_t stress_xq(const HalfArgs &a, int variant, cudaStream_t st)
 {
-  if (variant == TTI_COORDINATE) return launch_k(k_stress_tiled<TTI_COORDINATE, X, Q>, a, 2, st);
-  if (variant == TTI_TENSOR) return launch_k(k_stress_tiled<TTI_TENSOR, X, Q>, a, 2, st);
-  return launch_k(k_stress_tiled<TTI_BOND, X, Q>, a, 2, st);
+  const bool k = a.kd[0] != nullptr;
+  if (variant == TTI_COORDINATE)
+    return k ? launch_k(k_stress_tiled<TTI_COORDINATE, X, Q, true>, a, 2, st)
+             : launch_k(k_stress_tiled<TTI_COORDINATE, X, Q>, a, 2, st);
+  if (variant == TTI_TENSOR)
+    return k ? launch_k(k_stress_tiled<TTI_TENSOR, X, Q, true>, a, 2, st)
+             : launch_k(k_stress_tiled<TTI_TENSOR, X, Q>, a, 2, st);
+  return k ? launch_k(k_stress_tiled<TTI_BOND, X, Q, true>, a, 2, st) : launch_k(k_stress_tiled<TTI_BOND, X, Q>, a, 2, st);
 }
 
 cudaError_t launch_velocity(const HalfArgs &a, int variant, bool exact, cudaStream_t st)
