@@ -62,6 +62,7 @@ struct GradState {
   int2 *vrim = nullptr;
   double *vrim_acc = nullptr;
   int vm = 0, vrim_n = 0;
+  int surf_zorg = -1;  // row origin of the stress-half adjoint that folds in the column work; -1: a separate launch
 };
 
 namespace {
@@ -181,18 +182,17 @@ struct SurfaceArgs {
   int it, fs, tensor;
 };
 
-__global__ void k_adj_surface(SurfaceArgs a)
+// The column work for rows [r0, r1) of column ix, one warp.
+__device__ __forceinline__ void surface_warp(const SurfaceArgs &a, int ix, int r0, int r1, int lane)
 {
-  pdl_sync();
   const Grid &g = a.g;
-  const int lane = threadIdx.x & 31;
-  const int ix = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (ix >= g.Nx) return;
   const size_t col = (size_t)ix * g.ldz;
   for (int k = 0; k < 3; ++k) {
     if (!a.res[k]) continue;
     for (int j = a.colptr[k][ix] + lane; j < a.colptr[k][ix + 1]; j += 32) {
-      const size_t c = col + a.rzs[k][j];
+      const int rz = a.rzs[k][j];
+      if (rz < r0 || rz >= r1) continue;
+      const size_t c = col + rz;
       const float r = a.res[k][a.rid[k][j]];
       if (k == TTI_REC_VX) atomicAdd(a.lam[0] + c, r);
       else if (k == TTI_REC_VZ) atomicAdd(a.lam[1] + c, r);
@@ -208,7 +208,7 @@ __global__ void k_adj_surface(SurfaceArgs a)
     if (dx < -NH || dx > NH) continue;
     const int iz = a.src.z[n] + lane - NH;
     float v = 0.0f;
-    if (lane <= 2 * NH && iz >= 0 && iz < g.Nz) {
+    if (lane <= 2 * NH && iz >= 0 && iz < g.Nz && iz >= r0 && iz < r1) {
       const size_t c = col + iz;
       float l = a.lam[2][c] + a.lam[3][c];
       if (a.tensor) l += a.lam[5][c] + a.lam[6][c];  // the source also adds to tau
@@ -216,10 +216,10 @@ __global__ void k_adj_surface(SurfaceArgs a)
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (lane == 0) atomicAdd(a.gsrc + (size_t)n * a.src.nt + a.it, v);
+    if (lane == 0 && v != 0.0f) atomicAdd(a.gsrc + (size_t)n * a.src.nt + a.it, v);
   }
   __syncwarp();
-  if (a.fs && ix >= NH && ix < g.Nx - NH) {
+  if (a.fs && ix >= NH && ix < g.Nx - NH && g.izStart - NH >= r0 && g.izStart + NH < r1) {
     // lane k moves image row izStart - k onto row izStart + k (distinct cells
     // for each k); lane 0 then adds the sxx images onto the surface row in
     // the order k = 1..5
@@ -248,6 +248,15 @@ __global__ void k_adj_surface(SurfaceArgs a)
       zz[c] = 0.0f;
     }
   }
+  __syncwarp();
+}
+
+__global__ void k_adj_surface(SurfaceArgs a)
+{
+  pdl_sync();
+  const int ix = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (ix >= a.g.Nx) return;
+  surface_warp(a, ix, 0, a.g.Nz, threadIdx.x & 31);
 }
 
 // Adjoint of the velocity sources (coord:674-802), between the stress-half
@@ -360,13 +369,20 @@ __device__ __forceinline__ void store_T(const AdjArgs &a, size_t i, float t0, fl
 // stress-half adjoint, local part: gradient sums, T0..T3, lambda_sigma *= coef1.
 // PK (tiled path): packed parameters, and the strain rates the forward stress
 // kernel kept (keep[0..3], tensor tau keep[4..6]); otherwise the stencils of
-// the kept v (keep[0..1], tensor tau keep[2..4]).
-template <int V, bool PK>
-__global__ void __launch_bounds__(BZ *BX) k_adj_stress_local(AdjArgs a)
+// the kept v (keep[0..1], tensor tau keep[2..4]). Block rows start at z_org.
+// SURF: each warp (one column, 32 rows) first does the column work of its
+// rows (surface_warp): the residual injection, the source gradient and, in the
+// block whose rows hold izStart - 5 .. izStart + 5, the free-surface adjoint.
+// That is all of it when z_org is at or above every receiver row, source
+// window row and image row; the host checks this.
+template <int V, bool PK, bool SURF>
+__global__ void __launch_bounds__(BZ *BX) k_adj_stress_local(AdjArgs a, SurfaceArgs sa, int z_org)
 {
   pdl_sync();
   const Grid &g = a.g;
-  const int iz = blockIdx.x * BZ + threadIdx.x, ix = blockIdx.y * BX + threadIdx.y;
+  const int r0 = z_org + blockIdx.x * BZ;
+  const int iz = r0 + threadIdx.x, ix = blockIdx.y * BX + threadIdx.y;
+  if (SURF && ix < g.Nx) surface_warp(sa, ix, r0, r0 + BZ, threadIdx.x);
   if (!interior(g, ix, iz)) return;
   const size_t L = g.ldz, i = (size_t)ix * L + iz;
   const SParams m = stress_params<PK, V>(a, i, cell_undamped(a, ix, iz));
@@ -606,17 +622,28 @@ __global__ void __launch_bounds__(tiled::NT, 3) k_adj_velocity_tiled(const __gri
   tiled::tma::issue_tiles(at.map, sm, bar, 4, c.z0, c.x0, 4);
   const int z = c.z;
   const bool zin = z >= g.izStart && z < g.Nz - NH;
+  // this row's lambda_v, loaded while the halo boxes are in flight
+  constexpr int NJ = tiled::TX / 4;
+  float l[NJ][2];
+#pragma unroll
+  for (int j = 0; j < NJ; ++j) {
+    const int x = c.xc + j;
+    const size_t i = (size_t)x * g.ldz + z;
+    const bool on = zin && x < g.Nx - NH;
+    l[j][0] = on ? a.lam[0][i] : 0.0f;
+    l[j][1] = on ? a.lam[1][i] : 0.0f;
+  }
   if (!tiled::tma::wait_tiles(at.err, bar)) return;
   if (!zin) return;
   const float hx = a.hx, hz = a.hz;
 #pragma unroll
-  for (int j = 0; j < tiled::TX / 4; ++j) {
+  for (int j = 0; j < NJ; ++j) {
     const int x = c.xc + j;
     if (x >= g.Nx - NH) break;
     const size_t i = (size_t)x * g.ldz + z;
     const float *q = sm + (x - c.x0 + 4) * B + (z - c.z0 + 8);
-    const float lx = a.lam[0][i] - (vdiag1(q) + vdiag2(q + F));
-    const float lz = a.lam[1][i] - (vdiag1(q + 2 * F) + vdiag2(q + 3 * F));
+    const float lx = l[j][0] - (vdiag1(q) + vdiag2(q + F));
+    const float lz = l[j][1] - (vdiag1(q + 2 * F) + vdiag2(q + 3 * F));
     const float2 cf = cell_undamped(a, x, z) ? make_float2(1.0f, a.dt) : __ldg(at.pk.cf + i);
     const float br = cf.y * __ldg(a.p.invrho + i);
     const float Fx = br * lx, Fz = br * lz;
@@ -656,10 +683,22 @@ __global__ void __launch_bounds__(tiled::NT, 2) k_adj_vstencil_tiled(const __gri
   tiled::tma::issue_tiles(at.map, sm, bar, 6, c.z0, c.x0, 5);
   const int z = c.z;
   const bool zin = z >= a.z_lo && z < g.Nz - NH;
+  // this row's lambda_sigma, loaded while the halo boxes are in flight
+  constexpr int NJ = tiled::TX / 4;
+  float l[NJ][3];
+#pragma unroll
+  for (int j = 0; j < NJ; ++j) {
+    const int x = c.xc + j;
+    const size_t i = (size_t)x * g.ldz + z;
+    const bool on = zin && x < g.Nx - NH;
+    l[j][0] = on ? a.lam[2][i] : 0.0f;
+    l[j][1] = on ? a.lam[3][i] : 0.0f;
+    l[j][2] = on ? a.lam[4][i] : 0.0f;
+  }
   if (!tiled::tma::wait_tiles(at.err, bar)) return;
   if (!zin) return;
 #pragma unroll
-  for (int j = 0; j < tiled::TX / 4; ++j) {
+  for (int j = 0; j < NJ; ++j) {
     const int x = c.xc + j;
     if (x >= g.Nx - NH) break;
     const size_t i = (size_t)x * g.ldz + z;
@@ -671,9 +710,9 @@ __global__ void __launch_bounds__(tiled::NT, 2) k_adj_vstencil_tiled(const __gri
     spair(q + 3 * F, u, q2);
     spair(q + 4 * F, r1, u);
     spair(q + 5 * F, u, r2);
-    a.lam[2][i] -= p1 + p2;
-    a.lam[3][i] -= q1 + q2;
-    a.lam[4][i] -= r1 + r2;
+    a.lam[2][i] = l[j][0] - (p1 + p2);
+    a.lam[3][i] = l[j][1] - (q1 + q2);
+    a.lam[4][i] = l[j][2] - (r1 + r2);
   }
 }
 
@@ -984,6 +1023,35 @@ int vsource_tables(tti_handle *h, const SourceTables &tab)
   return TTI_OK;
 }
 
+// Row origin for the stress-half adjoint with the column work folded in: the
+// highest of the image rows (free surface), the receiver rows and the stress
+// source's window rows, so that every warp's rows hold all the column work
+// below them; -1 when the free-surface rows would not fall in one warp.
+int surface_origin(tti_handle *h, int *z_org)
+{
+  const Grid &g = h->g;
+  const tti_config &c = h->cfg;
+  int z = c.freesurface == 1 ? g.izStart - NH : g.izStart;
+  std::vector<int> rows;
+  for (int k = 0; k < 3; ++k) {
+    if (h->nrec[k] <= 0) continue;
+    rows.resize(h->nrec[k]);
+    GCK(h, cudaMemcpyAsync(rows.data(), h->d_rz[k], sizeof(int) * rows.size(), cudaMemcpyDeviceToHost, h->stream));
+    GCK(h, cudaStreamSynchronize(h->stream));
+    for (int r : rows) z = std::min(z, r);
+  }
+  if (c.stype == 1 && h->nsrc > 0) {
+    rows.resize(h->nsrc);
+    GCK(h, cudaMemcpyAsync(rows.data(), h->d_sz, sizeof(int) * rows.size(), cudaMemcpyDeviceToHost, h->stream));
+    GCK(h, cudaStreamSynchronize(h->stream));
+    for (int r : rows) z = std::min(z, std::max(0, r - NH));
+  }
+  z = std::max(z, 0);
+  // the free-surface adjoint needs rows izStart - 5 .. izStart + 5 in the first warp's 32 rows
+  *z_org = c.freesurface == 1 && z < g.izStart + NH + 1 - BZ ? -1 : z;
+  return TTI_OK;
+}
+
 int launch_vsource(tti_handle *h, const AdjArgs &a, int it)
 {
   GradState *s = h->grad;
@@ -1018,42 +1086,56 @@ int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
   const int it = c.mode == 2 ? c.nt - 1 - n : n;
   const AdjArgs a = adj_args(h, slot);
   const Grid &g = h->g;
-  {  // injection, source gradient and free-surface adjoint: one column-parallel launch
-    SurfaceArgs sa;
-    memset(&sa, 0, sizeof sa);
-    sa.g = g;
-    for (int k = 0; k < 8; ++k) sa.lam[k] = a.lam[k];
-    const bool inject = c.seistype > 0 && it % c.mt == 0;
-    bool any = false;
-    for (int k = 0; k < 3; ++k) {
-      const bool on = inject && s->res[k] && h->nrec[k] > 0;
-      sa.colptr[k] = h->d_rcol[k];
-      sa.rzs[k] = h->d_rzs[k];
-      sa.rid[k] = h->d_rid[k];
-      sa.res[k] = on ? s->res[k] + (size_t)(it / c.mt) * h->nrec[k] : nullptr;
-      any = any || on;
-    }
-    const bool ssrc = h->nsrc > 0 && c.stype == 1;
-    sa.src = SourceSet{ssrc ? h->nsrc : 0, h->d_sx, h->d_sz, h->d_src, c.nt};
-    memcpy(sa.k1.k1, tab.k1, sizeof sa.k1.k1);
-    sa.gsrc = s->gsrc;
-    sa.it = it;
-    sa.fs = c.freesurface == 1;
-    sa.tensor = c.variant == TTI_TENSOR;
-    if (any || ssrc || sa.fs) {
-      GCK(h, launch_pdl(k_adj_surface, dim3((g.Nx + 3) / 4), dim3(128), 0, h->stream, sa));
-      h->launches++;
-    }
+  // injection, source gradient and free-surface adjoint: folded into the
+  // stress-half adjoint on the tiled path where its row origin covers them,
+  // else one column-parallel launch before it
+  SurfaceArgs sa;
+  memset(&sa, 0, sizeof sa);
+  sa.g = g;
+  for (int k = 0; k < 8; ++k) sa.lam[k] = a.lam[k];
+  const bool inject = c.seistype > 0 && it % c.mt == 0;
+  bool any = false;
+  for (int k = 0; k < 3; ++k) {
+    const bool on = inject && s->res[k] && h->nrec[k] > 0;
+    sa.colptr[k] = h->d_rcol[k];
+    sa.rzs[k] = h->d_rzs[k];
+    sa.rid[k] = h->d_rid[k];
+    sa.res[k] = on ? s->res[k] + (size_t)(it / c.mt) * h->nrec[k] : nullptr;
+    any = any || on;
+  }
+  const bool ssrc = h->nsrc > 0 && c.stype == 1;
+  sa.src = SourceSet{ssrc ? h->nsrc : 0, h->d_sx, h->d_sz, h->d_src, c.nt};
+  memcpy(sa.k1.k1, tab.k1, sizeof sa.k1.k1);
+  sa.gsrc = s->gsrc;
+  sa.it = it;
+  sa.fs = c.freesurface == 1;
+  sa.tensor = c.variant == TTI_TENSOR;
+  const bool merged = h->use_tiled && s->surf_zorg >= 0;
+  if ((any || ssrc || sa.fs) && !merged) {
+    GCK(h, launch_pdl(k_adj_surface, dim3((g.Nx + 3) / 4), dim3(128), 0, h->stream, sa));
+    h->launches++;
   }
   h->launches += 3;
   if (h->use_tiled) {  // TMA halo tiles (the per-cell kernels below serve TTIFD_KERNEL=naive)
-    // the stress-half adjoint stays one thread per cell: it is bound by its
-    // per-cell reads and writes, not by its two stencil fields
-    const dim3 blk(BZ, BX), grd((g.Nz + BZ - 1) / BZ, (g.Nx + BX - 1) / BX);
-    if (c.variant == TTI_BOND) GCK(h, launch_pdl(k_adj_stress_local<TTI_BOND, true>, grd, blk, 0, h->stream, a));
-    else if (c.variant == TTI_TENSOR)
-      GCK(h, launch_pdl(k_adj_stress_local<TTI_TENSOR, true>, grd, blk, 0, h->stream, a));
-    else GCK(h, launch_pdl(k_adj_stress_local<TTI_COORDINATE, true>, grd, blk, 0, h->stream, a));
+    // the stress-half adjoint stays one thread per cell: with the kept strain
+    // rates it has no stencil, only per-cell reads and writes
+    const int z0 = merged ? s->surf_zorg : 0;
+    const dim3 blk(BZ, BX), grd((g.Nz - z0 + BZ - 1) / BZ, (g.Nx + BX - 1) / BX);
+    if (merged) {
+      if (c.variant == TTI_BOND)
+        GCK(h, launch_pdl(k_adj_stress_local<TTI_BOND, true, true>, grd, blk, 0, h->stream, a, sa, z0));
+      else if (c.variant == TTI_TENSOR)
+        GCK(h, launch_pdl(k_adj_stress_local<TTI_TENSOR, true, true>, grd, blk, 0, h->stream, a, sa, z0));
+      else
+        GCK(h, launch_pdl(k_adj_stress_local<TTI_COORDINATE, true, true>, grd, blk, 0, h->stream, a, sa, z0));
+    } else {
+      if (c.variant == TTI_BOND)
+        GCK(h, launch_pdl(k_adj_stress_local<TTI_BOND, true, false>, grd, blk, 0, h->stream, a, sa, z0));
+      else if (c.variant == TTI_TENSOR)
+        GCK(h, launch_pdl(k_adj_stress_local<TTI_TENSOR, true, false>, grd, blk, 0, h->stream, a, sa, z0));
+      else
+        GCK(h, launch_pdl(k_adj_stress_local<TTI_COORDINATE, true, false>, grd, blk, 0, h->stream, a, sa, z0));
+    }
     if (int rc = launch_vsource(h, a, it)) return rc;
     AdjTile at;
     memset(&at, 0, sizeof at);
@@ -1070,9 +1152,9 @@ int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
     return TTI_OK;
   }
   const dim3 blk(BZ, BX), grd((g.Nz + BZ - 1) / BZ, (g.Nx + BX - 1) / BX);
-  if (c.variant == TTI_BOND) k_adj_stress_local<TTI_BOND, false><<<grd, blk, 0, h->stream>>>(a);
-  else if (c.variant == TTI_TENSOR) k_adj_stress_local<TTI_TENSOR, false><<<grd, blk, 0, h->stream>>>(a);
-  else k_adj_stress_local<TTI_COORDINATE, false><<<grd, blk, 0, h->stream>>>(a);
+  if (c.variant == TTI_BOND) k_adj_stress_local<TTI_BOND, false, false><<<grd, blk, 0, h->stream>>>(a, sa, 0);
+  else if (c.variant == TTI_TENSOR) k_adj_stress_local<TTI_TENSOR, false, false><<<grd, blk, 0, h->stream>>>(a, sa, 0);
+  else k_adj_stress_local<TTI_COORDINATE, false, false><<<grd, blk, 0, h->stream>>>(a, sa, 0);
   if (int rc = launch_vsource(h, a, it)) return rc;
   if (c.variant == TTI_COORDINATE) k_adj_velocity<TTI_COORDINATE><<<grd, blk, 0, h->stream>>>(a);
   else k_adj_velocity<TTI_BOND><<<grd, blk, 0, h->stream>>>(a);  // tensor and Bond: no rotation at the velocity node
@@ -1189,6 +1271,7 @@ int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
   SourceTables tab;
   handle_source_tables(h, &tab);
   if ((rc = vsource_tables(h, tab))) return rc;
+  if ((rc = surface_origin(h, &s->surf_zorg))) return rc;
   // pass 1: forward with a checkpoint at every segment start but the last,
   // whose states are kept directly (ncheck = 1: all states, no recomputation)
   if ((rc = tti_reset(h))) return rc;
