@@ -63,6 +63,7 @@ struct GradState {
   double *vrim_acc = nullptr;
   int vm = 0, vrim_n = 0;
   int surf_zorg = -1;  // row origin of the stress-half adjoint that folds in the column work; -1: a separate launch
+  int surf_zend = 0;   // rows at or below this hold no column work
 };
 
 namespace {
@@ -374,15 +375,16 @@ __device__ __forceinline__ void store_T(const AdjArgs &a, size_t i, float t0, fl
 // rows (surface_warp): the residual injection, the source gradient and, in the
 // block whose rows hold izStart - 5 .. izStart + 5, the free-surface adjoint.
 // That is all of it when z_org is at or above every receiver row, source
-// window row and image row; the host checks this.
+// window row and image row; the host checks this. Blocks from row z_end down
+// have no column work and skip it.
 template <int V, bool PK, bool SURF>
-__global__ void __launch_bounds__(BZ *BX) k_adj_stress_local(AdjArgs a, SurfaceArgs sa, int z_org)
+__global__ void __launch_bounds__(BZ *BX) k_adj_stress_local(AdjArgs a, SurfaceArgs sa, int z_org, int z_end)
 {
   pdl_sync();
   const Grid &g = a.g;
   const int r0 = z_org + blockIdx.x * BZ;
   const int iz = r0 + threadIdx.x, ix = blockIdx.y * BX + threadIdx.y;
-  if (SURF && ix < g.Nx) surface_warp(sa, ix, r0, r0 + BZ, threadIdx.x);
+  if (SURF && ix < g.Nx && r0 < z_end) surface_warp(sa, ix, r0, r0 + BZ, threadIdx.x);
   if (!interior(g, ix, iz)) return;
   const size_t L = g.ldz, i = (size_t)ix * L + iz;
   const SParams m = stress_params<PK, V>(a, i, cell_undamped(a, ix, iz));
@@ -1027,26 +1029,34 @@ int vsource_tables(tti_handle *h, const SourceTables &tab)
 // highest of the image rows (free surface), the receiver rows and the stress
 // source's window rows, so that every warp's rows hold all the column work
 // below them; -1 when the free-surface rows would not fall in one warp.
-int surface_origin(tti_handle *h, int *z_org)
+int surface_origin(tti_handle *h, int *z_org, int *z_end)
 {
   const Grid &g = h->g;
   const tti_config &c = h->cfg;
   int z = c.freesurface == 1 ? g.izStart - NH : g.izStart;
+  int e = c.freesurface == 1 ? g.izStart + NH + 1 : 0;
   std::vector<int> rows;
   for (int k = 0; k < 3; ++k) {
     if (h->nrec[k] <= 0) continue;
     rows.resize(h->nrec[k]);
     GCK(h, cudaMemcpyAsync(rows.data(), h->d_rz[k], sizeof(int) * rows.size(), cudaMemcpyDeviceToHost, h->stream));
     GCK(h, cudaStreamSynchronize(h->stream));
-    for (int r : rows) z = std::min(z, r);
+    for (int r : rows) {
+      z = std::min(z, r);
+      e = std::max(e, r + 1);
+    }
   }
   if (c.stype == 1 && h->nsrc > 0) {
     rows.resize(h->nsrc);
     GCK(h, cudaMemcpyAsync(rows.data(), h->d_sz, sizeof(int) * rows.size(), cudaMemcpyDeviceToHost, h->stream));
     GCK(h, cudaStreamSynchronize(h->stream));
-    for (int r : rows) z = std::min(z, std::max(0, r - NH));
+    for (int r : rows) {
+      z = std::min(z, std::max(0, r - NH));
+      e = std::max(e, std::min(g.Nz, r + NH + 1));
+    }
   }
   z = std::max(z, 0);
+  *z_end = e;
   // the free-surface adjoint needs rows izStart - 5 .. izStart + 5 in the first warp's 32 rows
   *z_org = c.freesurface == 1 && z < g.izStart + NH + 1 - BZ ? -1 : z;
   return TTI_OK;
@@ -1123,18 +1133,18 @@ int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
     const dim3 blk(BZ, BX), grd((g.Nz - z0 + BZ - 1) / BZ, (g.Nx + BX - 1) / BX);
     if (merged) {
       if (c.variant == TTI_BOND)
-        GCK(h, launch_pdl(k_adj_stress_local<TTI_BOND, true, true>, grd, blk, 0, h->stream, a, sa, z0));
+        GCK(h, launch_pdl(k_adj_stress_local<TTI_BOND, true, true>, grd, blk, 0, h->stream, a, sa, z0, s->surf_zend));
       else if (c.variant == TTI_TENSOR)
-        GCK(h, launch_pdl(k_adj_stress_local<TTI_TENSOR, true, true>, grd, blk, 0, h->stream, a, sa, z0));
+        GCK(h, launch_pdl(k_adj_stress_local<TTI_TENSOR, true, true>, grd, blk, 0, h->stream, a, sa, z0, s->surf_zend));
       else
-        GCK(h, launch_pdl(k_adj_stress_local<TTI_COORDINATE, true, true>, grd, blk, 0, h->stream, a, sa, z0));
+        GCK(h, launch_pdl(k_adj_stress_local<TTI_COORDINATE, true, true>, grd, blk, 0, h->stream, a, sa, z0, s->surf_zend));
     } else {
       if (c.variant == TTI_BOND)
-        GCK(h, launch_pdl(k_adj_stress_local<TTI_BOND, true, false>, grd, blk, 0, h->stream, a, sa, z0));
+        GCK(h, launch_pdl(k_adj_stress_local<TTI_BOND, true, false>, grd, blk, 0, h->stream, a, sa, z0, s->surf_zend));
       else if (c.variant == TTI_TENSOR)
-        GCK(h, launch_pdl(k_adj_stress_local<TTI_TENSOR, true, false>, grd, blk, 0, h->stream, a, sa, z0));
+        GCK(h, launch_pdl(k_adj_stress_local<TTI_TENSOR, true, false>, grd, blk, 0, h->stream, a, sa, z0, s->surf_zend));
       else
-        GCK(h, launch_pdl(k_adj_stress_local<TTI_COORDINATE, true, false>, grd, blk, 0, h->stream, a, sa, z0));
+        GCK(h, launch_pdl(k_adj_stress_local<TTI_COORDINATE, true, false>, grd, blk, 0, h->stream, a, sa, z0, s->surf_zend));
     }
     if (int rc = launch_vsource(h, a, it)) return rc;
     AdjTile at;
@@ -1152,9 +1162,9 @@ int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
     return TTI_OK;
   }
   const dim3 blk(BZ, BX), grd((g.Nz + BZ - 1) / BZ, (g.Nx + BX - 1) / BX);
-  if (c.variant == TTI_BOND) k_adj_stress_local<TTI_BOND, false, false><<<grd, blk, 0, h->stream>>>(a, sa, 0);
-  else if (c.variant == TTI_TENSOR) k_adj_stress_local<TTI_TENSOR, false, false><<<grd, blk, 0, h->stream>>>(a, sa, 0);
-  else k_adj_stress_local<TTI_COORDINATE, false, false><<<grd, blk, 0, h->stream>>>(a, sa, 0);
+  if (c.variant == TTI_BOND) k_adj_stress_local<TTI_BOND, false, false><<<grd, blk, 0, h->stream>>>(a, sa, 0, 0);
+  else if (c.variant == TTI_TENSOR) k_adj_stress_local<TTI_TENSOR, false, false><<<grd, blk, 0, h->stream>>>(a, sa, 0, 0);
+  else k_adj_stress_local<TTI_COORDINATE, false, false><<<grd, blk, 0, h->stream>>>(a, sa, 0, 0);
   if (int rc = launch_vsource(h, a, it)) return rc;
   if (c.variant == TTI_COORDINATE) k_adj_velocity<TTI_COORDINATE><<<grd, blk, 0, h->stream>>>(a);
   else k_adj_velocity<TTI_BOND><<<grd, blk, 0, h->stream>>>(a);  // tensor and Bond: no rotation at the velocity node
@@ -1271,7 +1281,7 @@ int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
   SourceTables tab;
   handle_source_tables(h, &tab);
   if ((rc = vsource_tables(h, tab))) return rc;
-  if ((rc = surface_origin(h, &s->surf_zorg))) return rc;
+  if ((rc = surface_origin(h, &s->surf_zorg, &s->surf_zend))) return rc;
   // pass 1: forward with a checkpoint at every segment start but the last,
   // whose states are kept directly (ncheck = 1: all states, no recomputation)
   if ((rc = tti_reset(h))) return rc;
