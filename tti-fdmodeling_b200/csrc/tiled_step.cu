@@ -57,6 +57,32 @@ __device__ __forceinline__ float coef(const HalfArgs &a, int k)
   return Q ? a.hc[k] : rsg(k);
 }
 
+// While the halo boxes are in flight, lanes of each warp ask L2 for the
+// per-cell lines the velocity update reads after the wait (vx, vz, invrho,
+// coef1/coef2 outside the undamped interior, sin/cos theta_v for the
+// coordinate rotation): the warp's 32 rows are one 128-byte line per column
+// and array (two for the float2 arrays).
+template <bool ROT>
+__device__ __forceinline__ void prefetch_cells(const HalfArgs &a, const Cells &c, bool und)
+{
+  const int lane = threadIdx.x & 31, col = lane >> 3, k = lane & 7;
+  const int x = c.xc + col, z = c.zr - lane;  // the warp's first row
+  if (col >= TX / 4 || x >= a.g.Nx - NH || z >= a.g.Nz - NH) return;
+  const size_t gi = (size_t)x * a.g.ldz + z;
+  const void *p = nullptr;
+  switch (k) {
+  case 0: p = a.f.vx + gi; break;
+  case 1: p = a.f.vz + gi; break;
+  case 2: p = a.p.invrho + gi; break;
+  case 3: p = und ? nullptr : (const void *)(a.pk.cf + gi); break;
+  case 4: p = und ? nullptr : (const void *)(a.pk.cf + gi + 16); break;
+  case 5: p = ROT ? (const void *)(a.pk.vsc + gi) : nullptr; break;
+  case 6: p = ROT ? (const void *)(a.pk.vsc + gi + 16) : nullptr; break;
+  default: break;
+  }
+  if (p) asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 template <int V, bool X, bool Q, bool K = false>
 __device__ __forceinline__ void velocity_tile(const HalfArgs &a, const CUtensorMap *map, float *sm, int tz, int tx)
 {
@@ -69,6 +95,7 @@ __device__ __forceinline__ void velocity_tile(const HalfArgs &a, const CUtensorM
   const bool und = tile_undamped(a, c);
   const int z = c.zr;
   const bool zin = z >= g.izStart && z < g.Nz - NH;
+  prefetch_cells<V == TTI_COORDINATE>(a, c, und);
   if (!tma::wait_tiles(a.err, bar)) return;
   if (!zin) return;
   const float invdx = a.invdx, invdz = a.invdz;
