@@ -672,7 +672,9 @@ __global__ void __launch_bounds__(tiled::NT, 3) k_adj_velocity_tiled(const __gri
   }
 }
 
-// transposed velocity stencils into lambda_sigma (maps: TV0..TV5), rows from z_lo
+// transposed velocity stencils into lambda_sigma (maps: TV0..TV5), rows from
+// z_lo. The boxes arrive in three pairs (sxx: TV0 TV1, szz: TV2 TV3, sxz: TV4
+// TV5), each component computed as soon as its pair has landed.
 __global__ void __launch_bounds__(tiled::NT, 2) k_adj_vstencil_tiled(const __grid_constant__ AdjTile at)
 {
   pdl_sync();
@@ -682,7 +684,7 @@ __global__ void __launch_bounds__(tiled::NT, 2) k_adj_vstencil_tiled(const __gri
   const AdjArgs &a = at.a;
   const Grid &g = a.g;
   const TileCells c = tile_cells(at.z_base);
-  tiled::tma::issue_tiles(at.map, sm, bar, 6, c.z0, c.x0, 5);
+  tiled::tma::issue_groups(at.map, sm, bar, 3, 2, c.z0, c.x0, 5);
   const int z = c.z;
   const bool zin = z >= a.z_lo && z < g.Nz - NH;
   // this row's lambda_sigma, loaded while the halo boxes are in flight
@@ -697,31 +699,35 @@ __global__ void __launch_bounds__(tiled::NT, 2) k_adj_vstencil_tiled(const __gri
     l[j][1] = on ? a.lam[3][i] : 0.0f;
     l[j][2] = on ? a.lam[4][i] : 0.0f;
   }
-  if (!tiled::tma::wait_tiles(at.err, bar)) return;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    if (!tiled::tma::wait_group(at.err, bar, q, 3)) return;
+    if (!zin) continue;
+#pragma unroll
+    for (int j = 0; j < NJ; ++j) {
+      const float *p = sm + (c.xc + j - c.x0 + 5) * B + (z - c.z0 + 8) + 2 * q * F;
+      float d1, d2, u;
+      spair(p, d1, u);
+      spair(p + F, u, d2);
+      l[j][q] -= d1 + d2;
+    }
+  }
   if (!zin) return;
 #pragma unroll
   for (int j = 0; j < NJ; ++j) {
     const int x = c.xc + j;
     if (x >= g.Nx - NH) break;
     const size_t i = (size_t)x * g.ldz + z;
-    const float *q = sm + (x - c.x0 + 5) * B + (z - c.z0 + 8);
-    float p1, p2, q1, q2, r1, r2, u;
-    spair(q, p1, u);
-    spair(q + F, u, p2);
-    spair(q + 2 * F, q1, u);
-    spair(q + 3 * F, u, q2);
-    spair(q + 4 * F, r1, u);
-    spair(q + 5 * F, u, r2);
-    a.lam[2][i] = l[j][0] - (p1 + p2);
-    a.lam[3][i] = l[j][1] - (q1 + q2);
-    a.lam[4][i] = l[j][2] - (r1 + r2);
+    a.lam[2][i] = l[j][0];
+    a.lam[3][i] = l[j][1];
+    a.lam[4][i] = l[j][2];
   }
 }
 
 template <typename K>
 cudaError_t launch_adj_tile(K kernel, const AdjTile &at, int nfields, int z_first, const Grid &g, cudaStream_t st)
 {
-  const size_t bytes = (size_t)nfields * tiled::FIELD * sizeof(float) + 16;
+  const size_t bytes = (size_t)nfields * tiled::FIELD * sizeof(float) + 64;  // + up to 8 barriers
   static std::mutex mu;
   static const void *done[8];
   static int ndone = 0;

@@ -150,6 +150,41 @@ __device__ __forceinline__ bool wait_tiles(int *err, unsigned long long *bar)
   return true;
 }
 
+// The halo boxes of ng groups of `per` fields each, one barrier per group
+// (bars[0..ng)), so that a CTA can work on a group while the next is in flight.
+__device__ __forceinline__ void issue_groups(const CUtensorMap *map, float *sm, unsigned long long *bars, int ng,
+                                             int per, int z0, int x0, int xoff)
+{
+  constexpr unsigned BOX_BYTES = BX * BZ * 4;
+  const int t = threadIdx.x;
+  if (t == 0) {
+    for (int q = 0; q < ng; ++q) mbar_init(bars + q, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (t == 0)
+    for (int q = 0; q < ng; ++q) {
+      mbar_arrive_expect_tx(bars + q, per * BOX_BYTES);
+      for (int f = q * per; f < (q + 1) * per; ++f) tma_load_2d(sm + f * FIELD, map + f, z0 - 8, x0 - xoff, bars + q);
+    }
+}
+
+// Waits for group q of issue_groups (every thread of the CTA calls it); after a
+// timeout returns false to all threads, having given the groups from q on a
+// bounded time to land.
+__device__ __forceinline__ bool wait_group(int *err, unsigned long long *bars, int q, int ng)
+{
+  const bool ok = mbar_wait(bars + q, 0);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) {
+      atomicOr(err, 4);
+      for (int r = q; r < ng; ++r) mbar_wait(bars + r, 0, 1u << 16);
+    }
+    return false;
+  }
+  return true;
+}
+
 }  // namespace tma
 }  // namespace tiled
 }  // namespace ttifd

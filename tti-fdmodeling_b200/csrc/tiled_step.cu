@@ -240,6 +240,37 @@ __device__ __forceinline__ void stress_store(const HalfArgs &a, size_t gi, float
 }
 
 // Stress update of tile (tz, tx); `map` holds the tensor maps of vx, vz.
+// The same for the stress update: sigma (tensor: tau), coef1/coef2 outside the
+// undamped interior, c11 c13 c33 c55 (four lines), the formulation's pair
+// (two lines) and, for the tensor rotation, sin 2 theta.
+template <int V>
+__device__ __forceinline__ void prefetch_scells(const HalfArgs &a, const Cells &c, bool und)
+{
+  constexpr int SLOTS = V == TTI_TENSOR ? 12 : 11;
+  const int lane = threadIdx.x & 31, z = c.zr - lane;
+  if (z >= a.g.Nz - NH) return;
+  for (int q = lane; q < (TX / 4) * SLOTS; q += 32) {
+    const int col = q / SLOTS, k = q % SLOTS, x = c.xc + col;
+    if (x >= a.g.Nx - NH) continue;
+    const size_t gi = (size_t)x * a.g.ldz + z;
+    const void *p = nullptr;
+    if (k < 3) {
+      const float *o = V == TTI_TENSOR ? (k == 0 ? a.f.txx : k == 1 ? a.f.tzz : a.f.txz)
+                                       : (k == 0 ? a.f.sxx : k == 1 ? a.f.szz : a.f.sxz);
+      p = o + gi;
+    } else if (k < 5) {
+      p = und ? nullptr : (const void *)(a.pk.cf + gi + 16 * (k - 3));
+    } else if (k < 9) {
+      p = a.pk.c4 + gi + 8 * (k - 5);
+    } else if (k < 11) {
+      p = a.pk.sc + gi + 16 * (k - 9);
+    } else {
+      p = a.p.s2t + gi;
+    }
+    if (p) asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+  }
+}
+
 template <int V, bool X, bool Q, bool K = false>
 __device__ __forceinline__ void stress_tile(const HalfArgs &a, const CUtensorMap *map, float *sm, int tz, int tx)
 {
@@ -251,6 +282,7 @@ __device__ __forceinline__ void stress_tile(const HalfArgs &a, const CUtensorMap
   const bool und = tile_undamped(a, c);
   const int z = c.zr;
   const bool zin = z >= g.izStart && z < g.Nz - NH;
+  prefetch_scells<V>(a, c, und);
   if (!tma::wait_tiles(a.err, bar)) return;
   if (!zin) return;
   const float invdx = a.invdx, invdz = a.invdz;
