@@ -400,7 +400,7 @@ int create_handle(tti_handle **out, const tti_config *cfg, int device, const tti
     return fail(TTI_ERR_CUDA);
   }
   auto alloc = [&](float **p) -> int {
-    cudaError_t e = cudaMalloc(p, g.n * sizeof(float));
+    cudaError_t e = pool_alloc(reinterpret_cast<void **>(p), g.n * sizeof(float), h->stream);
     if (e != cudaSuccess)
       return set_err(h, TTI_ERR_NOMEM, "device allocation of %zu bytes failed: %s", g.n * sizeof(float),
                      cudaGetErrorString(e));
@@ -450,10 +450,12 @@ int create_handle(tti_handle **out, const tti_config *cfg, int device, const tti
     h->pk_sc = share->pk_sc;
     h->pk_c4 = share->pk_c4;
   } else if (h->use_fused || h->use_tiled) {
-    bool okp = cudaMalloc(&h->pk_cf, g.n * sizeof(float2)) == cudaSuccess &&
-               cudaMalloc(&h->pk_sc, g.n * sizeof(float2)) == cudaSuccess &&
-               cudaMalloc(&h->pk_c4, g.n * sizeof(float4)) == cudaSuccess &&
-               (cfg->variant != TTI_COORDINATE || cudaMalloc(&h->pk_vsc, g.n * sizeof(float2)) == cudaSuccess);
+    auto palloc = [&](void *p, size_t bytes) {
+      return pool_alloc(static_cast<void **>(p), bytes, h->stream) == cudaSuccess;
+    };
+    bool okp = palloc(&h->pk_cf, g.n * sizeof(float2)) && palloc(&h->pk_sc, g.n * sizeof(float2)) &&
+               palloc(&h->pk_c4, g.n * sizeof(float4)) &&
+               (cfg->variant != TTI_COORDINATE || palloc(&h->pk_vsc, g.n * sizeof(float2)));
     if (!okp) {
       set_err(h, TTI_ERR_NOMEM, "device allocation of the packed parameters failed");
       return fail(TTI_ERR_NOMEM);
@@ -501,14 +503,15 @@ int tti_destroy(tti_handle *h)
   if (!h) return TTI_OK;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
-  for (auto &p : h->fld) cudaFree(p);
-  for (auto &p : h->fld2) cudaFree(p);
+  cudaStream_t fs = h->stream;  // pool blocks are released in stream order
+  for (auto &p : h->fld) pool_free(p, fs);
+  for (auto &p : h->fld2) pool_free(p, fs);
   if (!h->owner) {
-    for (auto &p : h->par) cudaFree(p);
-    cudaFree(h->pk_cf);
-    cudaFree(h->pk_vsc);
-    cudaFree(h->pk_sc);
-    cudaFree(h->pk_c4);
+    for (auto &p : h->par) pool_free(p, fs);
+    pool_free(h->pk_cf, fs);
+    pool_free(h->pk_vsc, fs);
+    pool_free(h->pk_sc, fs);
+    pool_free(h->pk_c4, fs);
   }
   for (int k = 0; k < 3; ++k) {
     cudaFree(h->d_rx[k]);
@@ -522,9 +525,10 @@ int tti_destroy(tti_handle *h)
   cudaFree(h->d_sz);
   cudaFree(h->d_src);
   cudaFree(h->d_energy);
-  cudaFree(h->m_eps);
-  cudaFree(h->m_delta);
-  cudaFree(h->m_theta);
+  pool_free(h->m_eps, fs);
+  pool_free(h->m_delta, fs);
+  pool_free(h->m_theta, fs);
+  if (fs) cudaStreamSynchronize(fs);
   grad_release(h);
   cudaFree(h->d_flag);
   cudaFree(h->d_snap);
@@ -573,7 +577,7 @@ int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const floa
   float *d_w = nullptr, *raw_block = nullptr;
   int rc = TTI_OK;
   {
-    cudaError_t e = cudaMalloc(&raw_block, 6 * g.n * sizeof(float));
+    cudaError_t e = pool_alloc(reinterpret_cast<void **>(&raw_block), 6 * g.n * sizeof(float), h->stream);
     if (e != cudaSuccess) rc = set_err(h, TTI_ERR_NOMEM, "device allocation failed: %s", cudaGetErrorString(e));
   }
   for (int k = 0; k < 6 && rc == TTI_OK; ++k) {
@@ -625,7 +629,7 @@ int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const floa
   if (rc == TTI_OK) {
     for (int k = 0; k < (c.variant == TTI_BOND ? 3 : 2); ++k) {
       float *&dst = k == 0 ? h->m_eps : k == 1 ? h->m_delta : h->m_theta;
-      if (!dst && cudaMalloc(&dst, g.n * sizeof(float)) != cudaSuccess) {
+      if (!dst && pool_alloc(reinterpret_cast<void **>(&dst), g.n * sizeof(float), h->stream) != cudaSuccess) {
         rc = set_err(h, TTI_ERR_NOMEM, "device allocation failed");
         break;
       }
@@ -633,7 +637,7 @@ int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const floa
     }
     cudaStreamSynchronize(h->stream);
   }
-  cudaFree(raw_block);
+  pool_free(raw_block, h->stream);
   cudaFree(d_w);
   if (rc == TTI_OK && (h->use_fused || h->use_tiled)) {
     fused::launch_pack(g, step_args(h).p, fused::Packed{h->pk_cf, h->pk_vsc, h->pk_sc, h->pk_c4}, c.variant,

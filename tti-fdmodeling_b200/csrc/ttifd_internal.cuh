@@ -105,6 +105,12 @@ struct SourceSet {
   int nt;
 };
 
+// Bulk device arrays of a handle from the library's per-device pool
+// (devmem.cu), ordered on stream st; the caller synchronises st before other
+// streams use the memory.
+cudaError_t pool_alloc(void **p, size_t bytes, cudaStream_t st);
+void pool_free(void *p, cudaStream_t st);
+
 // Host-memory helpers (hostmem.cu): fault in every page of a host range from
 // several threads before a pageable device-to-host copy; the maximum of n
 // floats (NaN entries ignored, as fmaxf does) from several threads.
