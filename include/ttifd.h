@@ -194,8 +194,10 @@ int tti_fetch_energy(tti_handle *h, float *ek, float *ep);
  * `ncheck` segments: a forward pass saves the state at each segment start
  * (the checkpoints) and keeps the last segment's states, then the discrete
  * adjoint runs backwards, recomputing each earlier segment from its
- * checkpoint. Memory: (ncheck - 1) + ceil(nt / ncheck) states of 5 fields;
- * ncheck = 1 keeps every state and recomputes nothing. The shot's gradient is
+ * checkpoint. Memory: ncheck - 1 checkpoints of a full state (5 fields,
+ * tensor 8) and ceil(nt / ncheck) kept steps of 8 fields (coordinate), 7
+ * (tensor) or 4 (Bond) on the default kernels, 5 on the per-cell kernels;
+ * ncheck = 1 keeps every step and recomputes nothing. The shot's gradient is
  * ADDED to the handle's sums (so several
  * shots accumulate; tti_grad_zero clears them). Conventions: vs and rho are
  * held fixed; the MEAL arrays coef1, coef2, Beta stay those of the uploaded
