@@ -283,12 +283,12 @@ int do_snapshot(tti_handle *h, tti_snapshot_fn fn, void *user, int it)
   const int nxo = h->cfg.savew == 0 ? g.Nx - 2 * g.E : g.Nx;
   const size_t n = (size_t)nzo * nxo;
   if (h->snap_cap < n) {
-    cudaFree(h->d_snap);
+    pool_free(h->d_snap, h->stream);
     free(h->h_snap);
     h->d_snap = nullptr;
     h->h_snap = nullptr;
     h->snap_cap = 0;
-    CK(h, cudaMalloc(&h->d_snap, n * sizeof(float)));
+    CK(h, pool_alloc(reinterpret_cast<void **>(&h->d_snap), n * sizeof(float), h->stream));
     h->h_snap = static_cast<float *>(malloc(n * sizeof(float)));
     if (!h->h_snap) return set_err(h, TTI_ERR_NOMEM, "host allocation of the snapshot buffer failed");
     prefault(h->h_snap, n * sizeof(float));
@@ -479,8 +479,9 @@ int create_handle(tti_handle **out, const tti_config *cfg, int device, const tti
   }
   for (int p = 0; p < TTI_P_COUNT && !share; ++p)
     if (param_used(cfg->variant, p) && (rc = alloc(&h->par[p]))) return fail(rc);
-  if (cudaMalloc(&h->d_flag, sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&h->d_energy, sizeof(double) * 2 * (size_t)cfg->nt) != cudaSuccess) {
+  if (pool_alloc(reinterpret_cast<void **>(&h->d_flag), sizeof(int), h->stream) != cudaSuccess ||
+      pool_alloc(reinterpret_cast<void **>(&h->d_energy), sizeof(double) * 2 * (size_t)cfg->nt, h->stream) !=
+          cudaSuccess) {
     set_err(h, TTI_ERR_NOMEM, "device allocation failed");
     return fail(TTI_ERR_NOMEM);
   }
@@ -514,26 +515,26 @@ int tti_destroy(tti_handle *h)
     pool_free(h->pk_c4, fs);
   }
   for (int k = 0; k < 3; ++k) {
-    cudaFree(h->d_rx[k]);
-    cudaFree(h->d_rz[k]);
-    cudaFree(h->d_rec[k]);
-    cudaFree(h->d_rcol[k]);
-    cudaFree(h->d_rzs[k]);
-    cudaFree(h->d_rid[k]);
+    pool_free(h->d_rx[k], fs);
+    pool_free(h->d_rz[k], fs);
+    pool_free(h->d_rec[k], fs);
+    pool_free(h->d_rcol[k], fs);
+    pool_free(h->d_rzs[k], fs);
+    pool_free(h->d_rid[k], fs);
   }
-  cudaFree(h->d_sx);
-  cudaFree(h->d_sz);
-  cudaFree(h->d_src);
-  cudaFree(h->d_energy);
+  pool_free(h->d_sx, fs);
+  pool_free(h->d_sz, fs);
+  pool_free(h->d_src, fs);
+  pool_free(h->d_energy, fs);
+  pool_free(h->d_flag, fs);
   pool_free(h->m_eps, fs);
   pool_free(h->m_delta, fs);
   pool_free(h->m_theta, fs);
+  pool_free(h->d_snap, fs);
+  pool_free(h->d_stage, fs);
   if (fs) cudaStreamSynchronize(fs);
   grad_release(h);
-  cudaFree(h->d_flag);
-  cudaFree(h->d_snap);
   free(h->h_snap);
-  cudaFree(h->d_stage);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   free(h->tmaps);
@@ -597,7 +598,7 @@ int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const floa
       const float d = (0.1f * l) / (0.1f * nl);
       w[l] = expf(logf(2.0f) * powf(d, alpha)) - 1.0f;
     }
-    cudaError_t e = cudaMalloc(&d_w, sizeof(float) * (nl + 1));
+    cudaError_t e = pool_alloc(reinterpret_cast<void **>(&d_w), sizeof(float) * (nl + 1), h->stream);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(d_w, w.data(), sizeof(float) * (nl + 1), cudaMemcpyHostToDevice, h->stream);
     if (e != cudaSuccess) rc = set_err(h, TTI_ERR_CUDA, "MEAL table upload: %s", cudaGetErrorString(e));
@@ -638,7 +639,7 @@ int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const floa
     cudaStreamSynchronize(h->stream);
   }
   pool_free(raw_block, h->stream);
-  cudaFree(d_w);
+  pool_free(d_w, h->stream);
   if (rc == TTI_OK && (h->use_fused || h->use_tiled)) {
     fused::launch_pack(g, step_args(h).p, fused::Packed{h->pk_cf, h->pk_vsc, h->pk_sc, h->pk_c4}, c.variant,
                        h->stream);
@@ -650,13 +651,13 @@ int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const floa
     // verify that on the device instead of assuming the MEAL rim geometry
     int *cnt = nullptr;
     int bad = -1;
-    if (cudaMalloc(&cnt, sizeof(int)) == cudaSuccess) {
+    if (pool_alloc(reinterpret_cast<void **>(&cnt), sizeof(int), h->stream) == cudaSuccess) {
       cudaMemsetAsync(cnt, 0, sizeof(int), h->stream);
       fused::launch_check_undamped(g, h->par[TTI_P_COEF1], h->par[TTI_P_COEF2], c.dt, c.freesurface ? 0 : g.E, cnt,
                                    h->stream);
       cudaMemcpyAsync(&bad, cnt, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+      pool_free(cnt, h->stream);
       cudaStreamSynchronize(h->stream);
-      cudaFree(cnt);
     }
     h->undamped_ok = bad == 0;
   }
@@ -687,9 +688,9 @@ int tti_set_source(tti_handle *h, int ntrace, const int *posx, const int *posz, 
                      posx[i], c.nx);
   }
   CK(h, cudaSetDevice(h->device));
-  cudaFree(h->d_sx);
-  cudaFree(h->d_sz);
-  cudaFree(h->d_src);
+  pool_free(h->d_sx, h->stream);
+  pool_free(h->d_sz, h->stream);
+  pool_free(h->d_src, h->stream);
   h->d_sx = h->d_sz = nullptr;
   h->d_src = nullptr;
   h->nsrc = 0;
@@ -699,12 +700,13 @@ int tti_set_source(tti_handle *h, int ntrace, const int *posx, const int *posz, 
     x[i] = posx[i] + h->g.E;
     z[i] = posz[i] + h->g.E;
   }
-  CK(h, cudaMalloc(&h->d_sx, sizeof(int) * ntrace));
-  CK(h, cudaMalloc(&h->d_sz, sizeof(int) * ntrace));
-  CK(h, cudaMalloc(&h->d_src, sizeof(float) * (size_t)ntrace * c.nt));
-  CK(h, cudaMemcpy(h->d_sx, x.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice));
-  CK(h, cudaMemcpy(h->d_sz, z.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice));
-  CK(h, cudaMemcpy(h->d_src, src, sizeof(float) * (size_t)ntrace * c.nt, cudaMemcpyHostToDevice));
+  CK(h, pool_alloc(reinterpret_cast<void **>(&h->d_sx), sizeof(int) * ntrace, h->stream));
+  CK(h, pool_alloc(reinterpret_cast<void **>(&h->d_sz), sizeof(int) * ntrace, h->stream));
+  CK(h, pool_alloc(reinterpret_cast<void **>(&h->d_src), sizeof(float) * (size_t)ntrace * c.nt, h->stream));
+  CK(h, cudaMemcpyAsync(h->d_sx, x.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemcpyAsync(h->d_sz, z.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemcpyAsync(h->d_src, src, sizeof(float) * (size_t)ntrace * c.nt, cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
   h->nsrc = ntrace;
   return TTI_OK;
 }
@@ -723,9 +725,9 @@ int tti_set_receivers(tti_handle *h, int kind, int ntrace, const int *posx, cons
                      posx[i], c.nx);
   }
   CK(h, cudaSetDevice(h->device));
-  cudaFree(h->d_rx[kind]);
-  cudaFree(h->d_rz[kind]);
-  cudaFree(h->d_rec[kind]);
+  pool_free(h->d_rx[kind], h->stream);
+  pool_free(h->d_rz[kind], h->stream);
+  pool_free(h->d_rec[kind], h->stream);
   h->d_rx[kind] = h->d_rz[kind] = nullptr;
   h->d_rec[kind] = nullptr;
   h->nrec[kind] = 0;
@@ -735,12 +737,14 @@ int tti_set_receivers(tti_handle *h, int kind, int ntrace, const int *posx, cons
     x[i] = posx[i] + h->g.E;
     z[i] = posz[i] + h->g.E;
   }
-  CK(h, cudaMalloc(&h->d_rx[kind], sizeof(int) * ntrace));
-  CK(h, cudaMalloc(&h->d_rz[kind], sizeof(int) * ntrace));
-  CK(h, cudaMalloc(&h->d_rec[kind], sizeof(float) * (size_t)ntrace * h->nts));
-  CK(h, cudaMemcpy(h->d_rx[kind], x.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice));
-  CK(h, cudaMemcpy(h->d_rz[kind], z.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice));
-  CK(h, cudaMemset(h->d_rec[kind], 0, sizeof(float) * (size_t)ntrace * h->nts));
+  CK(h, pool_alloc(reinterpret_cast<void **>(&h->d_rx[kind]), sizeof(int) * ntrace, h->stream));
+  CK(h, pool_alloc(reinterpret_cast<void **>(&h->d_rz[kind]), sizeof(int) * ntrace, h->stream));
+  // the traces (ntrace x nts floats, the largest of these) from the handle's pool
+  CK(h, pool_alloc(reinterpret_cast<void **>(&h->d_rec[kind]), sizeof(float) * (size_t)ntrace * h->nts, h->stream));
+  CK(h, cudaMemcpyAsync(h->d_rx[kind], x.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemcpyAsync(h->d_rz[kind], z.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemsetAsync(h->d_rec[kind], 0, sizeof(float) * (size_t)ntrace * h->nts, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
   // receivers grouped by padded-grid column for the fused step
   {
     const int Nx = h->g.Nx;
@@ -753,16 +757,17 @@ int tti_set_receivers(tti_handle *h, int kind, int ntrace, const int *posx, cons
       zs[i] = z[order[i]];
       ids[i] = order[i];
     }
-    cudaFree(h->d_rcol[kind]);
-    cudaFree(h->d_rzs[kind]);
-    cudaFree(h->d_rid[kind]);
+    pool_free(h->d_rcol[kind], h->stream);
+    pool_free(h->d_rzs[kind], h->stream);
+    pool_free(h->d_rid[kind], h->stream);
     h->d_rcol[kind] = h->d_rzs[kind] = h->d_rid[kind] = nullptr;
-    CK(h, cudaMalloc(&h->d_rcol[kind], sizeof(int) * (Nx + 1)));
-    CK(h, cudaMalloc(&h->d_rzs[kind], sizeof(int) * ntrace));
-    CK(h, cudaMalloc(&h->d_rid[kind], sizeof(int) * ntrace));
-    CK(h, cudaMemcpy(h->d_rcol[kind], colptr.data(), sizeof(int) * (Nx + 1), cudaMemcpyHostToDevice));
-    CK(h, cudaMemcpy(h->d_rzs[kind], zs.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice));
-    CK(h, cudaMemcpy(h->d_rid[kind], ids.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice));
+    CK(h, pool_alloc(reinterpret_cast<void **>(&h->d_rcol[kind]), sizeof(int) * (Nx + 1), h->stream));
+    CK(h, pool_alloc(reinterpret_cast<void **>(&h->d_rzs[kind]), sizeof(int) * ntrace, h->stream));
+    CK(h, pool_alloc(reinterpret_cast<void **>(&h->d_rid[kind]), sizeof(int) * ntrace, h->stream));
+    CK(h, cudaMemcpyAsync(h->d_rcol[kind], colptr.data(), sizeof(int) * (Nx + 1), cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaMemcpyAsync(h->d_rzs[kind], zs.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaMemcpyAsync(h->d_rid[kind], ids.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));  // the host vectors go out of scope
   }
   h->nrec[kind] = ntrace;
   return TTI_OK;
@@ -881,7 +886,7 @@ int tti_fetch_traces(tti_handle *h, int kind, float *out)
   // [ntrace][nts]) and copied straight into the caller's block, whose pages
   // are faulted in first from several host threads.
   constexpr size_t STAGE = (size_t)4 << 20;  // floats per chunk
-  if (!h->d_stage) CK(h, cudaMalloc(&h->d_stage, STAGE * sizeof(float)));
+  if (!h->d_stage) CK(h, pool_alloc(reinterpret_cast<void **>(&h->d_stage), STAGE * sizeof(float), h->stream));
   if ((size_t)nts > STAGE || nts > 65535 * 32)
     return set_err(h, TTI_ERR_ARG, "trace of %d samples is longer than the fetch supports", nts);
   prefault(out, sizeof(float) * (size_t)n * nts);
