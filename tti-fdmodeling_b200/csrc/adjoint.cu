@@ -537,12 +537,12 @@ __global__ void __launch_bounds__(BZ *BX) k_adj_velocity_stencil(AdjArgs a)
 }
 
 // ---------------------------------------------------------------- tiled adjoint
-// The three adjoint passes on the forward path's 128 x 16 tiles: every stencil
-// tap comes from a TMA halo box in shared memory (one 2D copy per field, the
-// box origin rounded down to a 16-byte boundary, zeros outside the array),
-// per-cell parameters from the packed arrays.
+// The two stencil passes of the adjoint on the forward path's 128 x 16 tiles:
+// every stencil tap comes from a TMA halo box in shared memory (one 2D copy per
+// field, the box origin rounded down to a 16-byte boundary, zeros outside the
+// array), per-cell parameters from the packed arrays.
 struct alignas(64) AdjTile {
-  CUtensorMap map[7];
+  CUtensorMap map[6];  // velocity pass: T0..T3; stress-node pass: TV0..TV5
   AdjArgs a;
   fused::Packed pk;
   int z_base;  // first tile row (multiple of 4)
@@ -571,20 +571,6 @@ __device__ __forceinline__ void spair(const float *q, float &d1, float &d2)
   for (int k = 2; k <= NH; ++k) {
     s1 += rsg(k - 1) * (q[(k - 1) * B + k - 1] - q[-k * B - k]);
     s2 += rsg(k - 1) * (q[(k - 1) * B - k] - q[-k * B + k - 1]);
-  }
-  d1 = s1;
-  d2 = s2;
-}
-
-// velocity-node pair of shared field q centred on (x, z)
-__device__ __forceinline__ void vpair(const float *q, float &d1, float &d2)
-{
-  constexpr int B = tiled::BZ;
-  float s1 = rsg(0) * (q[B + 1] - q[0]), s2 = rsg(0) * (q[B] - q[1]);
-#pragma unroll
-  for (int k = 2; k <= NH; ++k) {
-    s1 += rsg(k - 1) * (q[k * B + k] - q[(1 - k) * B + 1 - k]);
-    s2 += rsg(k - 1) * (q[k * B + 1 - k] - q[(1 - k) * B + k]);
   }
   d1 = s1;
   d2 = s2;
