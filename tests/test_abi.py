@@ -4,6 +4,7 @@ import ctypes
 import os
 import re
 
+import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -68,3 +69,15 @@ def test_batch_argument_checks(models, model_of, what, gpu_lib):
         ttifd.Batch([dict(base, **m) for m in models], model_of)
     assert e.value.code == ttifd.ERR_ARG
     assert what in str(e.value)
+
+
+@pytest.mark.parametrize("shape", [(3, 5), (7, 1126), (2400, 1126), (7872, 1126)])
+def test_snapshot_copy_is_exact(shape):
+    """The wrapper hands each snapshot to the callback as a copy of the library's
+    buffer; large ones are copied in row blocks from several threads."""
+    import ttifd
+
+    a = np.random.default_rng(1).standard_normal(shape).astype(np.float32)
+    b = ttifd._copy(a)
+    assert b is not a and b.shape == a.shape and b.dtype == a.dtype
+    assert np.array_equal(a, b)

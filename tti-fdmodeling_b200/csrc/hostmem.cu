@@ -6,12 +6,19 @@
 // pages in from several threads first (16 threads: 2.6 ms for 95 MB, 1.7 ms
 // with the huge-page hint), then copying straight from the device (about
 // 9 GB/s), avoids both the faults on the copy path and the cost of pinning
-// (13 ms to allocate and 4.7 ms to free 32 MB of page-locked memory).
+// (13 ms to allocate and 4.7 ms to free 32 MB of page-locked memory) on
+// every handle. Where page-locked chunks can be had once per process, staging
+// a trace fetch through two of them with a multi-threaded host copy into the
+// caller's fresh block is faster still (15.5 GB/s): pinned_chunk hands out
+// 16 MB chunks from a process-wide free list and they stay allocated until
+// exit.
 #include <float.h>
 #include <stdint.h>
 #include <sys/mman.h>
 
 #include <algorithm>
+#include <cstring>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -43,7 +50,41 @@ void split(size_t n, int nth, F f)
   for (auto &x : th) x.join();
 }
 
+std::mutex g_pin_mu;
+std::vector<float *> g_pin_free;  // page-locked staging chunks not in use
+
 }  // namespace
+
+void parallel_copy(void *dst, const void *src, size_t bytes)
+{
+  const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const int nth = (int)std::min<size_t>(std::min<size_t>(16, hw), std::max<size_t>(1, bytes >> 20));
+  char *d = static_cast<char *>(dst);
+  const char *q = static_cast<const char *>(src);
+  split(bytes, nth, [d, q](size_t b, size_t e) { memcpy(d + b, q + b, e - b); });
+}
+
+float *pinned_chunk()
+{
+  {
+    std::lock_guard<std::mutex> lock(g_pin_mu);
+    if (!g_pin_free.empty()) {
+      float *p = g_pin_free.back();
+      g_pin_free.pop_back();
+      return p;
+    }
+  }
+  float *p = nullptr;
+  if (cudaMallocHost(reinterpret_cast<void **>(&p), PIN_CHUNK * sizeof(float)) != cudaSuccess) return nullptr;
+  return p;
+}
+
+void pinned_release(float *p)
+{
+  if (!p) return;
+  std::lock_guard<std::mutex> lock(g_pin_mu);
+  g_pin_free.push_back(p);
+}
 
 void prefault(void *p, size_t bytes)
 {

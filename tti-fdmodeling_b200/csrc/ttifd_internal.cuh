@@ -116,6 +116,13 @@ void pool_free(void *p, cudaStream_t st);
 // floats (NaN entries ignored, as fmaxf does) from several threads.
 void prefault(void *p, size_t bytes);
 float host_max(const float *a, size_t n, float init);
+// memcpy from up to 16 host threads (1 MiB or more each)
+void parallel_copy(void *dst, const void *src, size_t bytes);
+// Page-locked staging chunks of PIN_CHUNK floats from a process-wide free list
+// (allocated on first need, kept until exit); null when none can be had.
+constexpr size_t PIN_CHUNK = (size_t)4 << 20;
+float *pinned_chunk();
+void pinned_release(float *p);
 
 struct ReceiverSet {
   int n[3];

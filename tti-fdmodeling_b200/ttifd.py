@@ -26,6 +26,30 @@ PARAMS = ["D", "Beta", "coef1", "coef2", "invrho", "c11", "c13", "c15", "c33", "
 P = {name: i for i, name in enumerate(PARAMS)}
 
 
+_COPY_POOL = None
+
+
+def _copy(src: np.ndarray) -> np.ndarray:
+    """A new array with the contents of `src`. Large arrays are copied in row
+    blocks from a few threads (numpy releases the GIL while it copies), so the
+    page faults of the fresh destination are taken in parallel: a 35 MB
+    snapshot copies in about a third of the single-threaded time."""
+    global _COPY_POOL
+    out = np.empty_like(src)
+    nth = min(8, os.cpu_count() or 1, src.shape[0])
+    if src.nbytes < (8 << 20) or nth < 2:
+        np.copyto(out, src)
+        return out
+    if _COPY_POOL is None:
+        from concurrent.futures import ThreadPoolExecutor
+        _COPY_POOL = ThreadPoolExecutor(max_workers=8, thread_name_prefix="ttifd-copy")
+    step = -(-src.shape[0] // nth)
+    blocks = [slice(b, min(b + step, src.shape[0])) for b in range(0, src.shape[0], step)]
+    for f in [_COPY_POOL.submit(np.copyto, out[b], src[b]) for b in blocks]:
+        f.result()
+    return out
+
+
 class TTIError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"[{code}] {msg}")
@@ -207,7 +231,7 @@ class Modeling:
         else:
             def _cb(user, it, kind, data, nzo, nxo):
                 try:
-                    arr = np.ctypeslib.as_array(data, shape=(nxo, nzo)).copy()
+                    arr = _copy(np.ctypeslib.as_array(data, shape=(nxo, nzo)))
                     snapshot(it, kind, arr)
                     return 0
                 except Exception:  # abort the run
