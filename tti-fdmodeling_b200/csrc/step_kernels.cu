@@ -302,10 +302,31 @@ __global__ void k_energy(Grid g, Fields f, Params p, int nz, int nx, double *out
 // rows of the window), and the receiver samples (isoelastic.c:103-144; lanes
 // over the column's receivers). Columns do not interact, so one launch
 // replaces three; the warp makes each phase one memory round trip.
-__device__ void post_column(const Grid &g, const Fields &f, const PostArgs &p, int ix, int it, int irec)
+// PDL: the warp reads the column's receiver geometry (static since the
+// receivers were set) before waiting for the previous kernel, so those loads
+// overlap its tail.
+__device__ void post_column(const Grid &g, const Fields &f, const PostArgs &p, int ix, int it, int irec,
+                            bool pdl = false)
 {
   const int lane = threadIdx.x & 31;
   const size_t col = (size_t)ix * g.ldz;
+  // the first 32 receivers of each component in this column, one per lane
+  int rb[3] = {0, 0, 0}, re[3] = {0, 0, 0}, rzl[3] = {0, 0, 0}, ridl[3] = {0, 0, 0};
+  if (irec >= 0) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      if (p.colptr[k]) {
+        rb[k] = p.colptr[k][ix];
+        re[k] = p.colptr[k][ix + 1];
+      }
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      if (rb[k] + lane < re[k]) {
+        rzl[k] = p.rz[k][rb[k] + lane];
+        ridl[k] = p.rid[k][rb[k] + lane];
+      }
+  }
+  if (pdl) pdl_sync();
   if (p.freesurface && ix >= NH && ix < g.Nx - NH) {
     const size_t c = col + g.izStart;
     const float sxx0 = f.sxx[c];
@@ -346,28 +367,44 @@ __device__ void post_column(const Grid &g, const Fields &f, const PostArgs &p, i
     }
   }
   if (irec >= 0) {
+    // all three components' samples loaded before any is stored
+    float v[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
     for (int k = 0; k < 3; ++k) {
-      if (!p.colptr[k]) continue;
-      const int b = p.colptr[k][ix], e = p.colptr[k][ix + 1];
-      for (int j = b + lane; j < e; j += 32) {
-        const size_t c = col + p.rz[k][j];
-        float v;
-        if (k == TTI_REC_VX) v = f.vx[c];
-        else if (k == TTI_REC_VZ) v = f.vz[c];
-        else v = __fmul_rn(0.5f, __fadd_rn(f.sxx[c], f.szz[c]));
-        p.rec[k][(size_t)irec * p.nrec[k] + p.rid[k][j]] = v;
-        if (!isfinite(v)) atomicOr(p.flag, 1);
-      }
+      if (rb[k] + lane >= re[k]) continue;
+      const size_t c = col + rzl[k];
+      if (k == TTI_REC_VX) v[k] = f.vx[c];
+      else if (k == TTI_REC_VZ) v[k] = f.vz[c];
+      else v[k] = __fmul_rn(0.5f, __fadd_rn(f.sxx[c], f.szz[c]));
     }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      if (rb[k] + lane >= re[k]) continue;
+      p.rec[k][(size_t)irec * p.nrec[k] + ridl[k]] = v[k];
+      if (!isfinite(v[k])) atomicOr(p.flag, 1);
+    }
+    // columns with more than 32 receivers of a component
+    for (int k = 0; k < 3; ++k)
+      for (int j = rb[k] + 32 + lane; j < re[k]; j += 32) {
+        const size_t c = col + p.rz[k][j];
+        float w;
+        if (k == TTI_REC_VX) w = f.vx[c];
+        else if (k == TTI_REC_VZ) w = f.vz[c];
+        else w = __fmul_rn(0.5f, __fadd_rn(f.sxx[c], f.szz[c]));
+        p.rec[k][(size_t)irec * p.nrec[k] + p.rid[k][j]] = w;
+        if (!isfinite(w)) atomicOr(p.flag, 1);
+      }
   }
 }
 
 __global__ void k_post(Grid g, Fields f, PostArgs p)
 {
-  pdl_sync();
   const int ix = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (ix >= g.Nx) return;
-  post_column(g, f, p, ix, p.it, p.irec);
+  if (ix >= g.Nx) {
+    pdl_sync();
+    return;
+  }
+  post_column(g, f, p, ix, p.it, p.irec, true);
 }
 
 // Batched: blockIdx.y = instance; time index and receiver slot from the step counter.
