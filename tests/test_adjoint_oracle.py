@@ -199,3 +199,32 @@ def test_velocity_source_gradient_matches_central_differences(stype, variant):
                 fd = (_misfit(adj, mp, dobs) - _misfit(adj, mm, dobs)) / (2 * step)
                 an = g[name][ix, iz]
                 assert abs(fd - an) <= 1e-3 * max(abs(an), 1e-2 * np.abs(g[name]).max()), (name, ix, iz, fd, an)
+
+
+@pytest.mark.parametrize("mt,seistype,variant", [(3, 3, "coordinate_rotation"), (2, 1, "tensor_rotation"),
+                                                 (4, 2, "bond_transformation")])
+def test_dot_product_sampling_and_components(mt, seistype, variant):
+    """Traces every mt-th step, and only the components seistype records
+    (1: vx vz, 2: p): the adjoint injects the residual at those steps only."""
+    cfg = dict(CFG, freesurface=1 if variant != "bond_transformation" else 0, variant=variant, mt=mt,
+               seistype=seistype)
+    m = synthetic.layered_model(cfg["nz"], cfg["nx"], seed=5, nlayers=4)
+    pads = synthetic.padded(m, cfg["ealThick"])
+    with AdjointOracle(cfg, pads) as adj:
+        adj.set_model(*pads)
+        w = synthetic.ricker(cfg["nt"], cfg["dt"], cfg["fpeak"])
+        adj.set_source([24], [3], w[None, :])
+        gx = np.arange(0, cfg["nx"], 3)
+        for k in (0, 1, 2):
+            adj.set_receivers(k, gx, 2)
+        d = adj.forward()
+        want = [seistype in (1, 3), seistype in (1, 3), seistype in (2, 3)]
+        for x, on in zip(d, want):  # components not recorded stay zero
+            assert x.shape[1] == (cfg["nt"] - 1) // mt + 1
+            assert (np.abs(x).max() > 0) == on
+        rng = np.random.default_rng(2)
+        r = [rng.standard_normal(x.shape) if x is not None else None for x in d]
+        _, _, gsrc = adj.gradient([a - b if a is not None else None for a, b in zip(d, r)])
+        lhs = sum(float(np.sum(a * b)) for a, b in zip(d, r) if a is not None)
+        rhs = float(np.sum(gsrc[0] * w))
+        assert abs(lhs - rhs) <= 1e-10 * abs(lhs), (lhs, rhs)
