@@ -251,8 +251,10 @@ int tti_batch_upload_model(tti_batch *b, int m, const float *vp, const float *vs
  * steps (0: no graph). */
 int tti_batch_set_order(tti_batch *b, int group, int graph_steps);
 /* Times every group size in {all, 1, 2, 4, 8, 16} (those below the shot
- * count) with and without a graph on nsteps steps, keeps the fastest and
- * resets the batch. Outputs (may be NULL): the choice and its ms per step. */
+ * count) with and without a graph of 20 steps, each over nsteps steps (at
+ * least one graph replay, at most the longest instance's nt) in two rounds,
+ * keeps the fastest and resets the batch. Outputs (may be NULL): the choice
+ * and its ms per step. */
 int tti_batch_autotune(tti_batch *b, int nsteps, int *group, int *graph_steps, float *ms_per_step);
 /* Zeroes every instance and rebuilds the launch tables from the current
  * sources and receivers. */
