@@ -594,6 +594,31 @@ __device__ __forceinline__ float vdiag2(const float *q)
   return s;
 }
 
+// While the halo boxes are in flight, the lanes of each warp ask L2 for the
+// per-cell lines the velocity-half adjoint reads after the wait (coef1/coef2,
+// invrho; coordinate also sin/cos theta_v, the kept P Q R S and the two theta_v
+// sums): one 128-byte line per column and array, two for the float2 arrays.
+template <int V>
+__device__ __forceinline__ void prefetch_adj_velocity(const AdjTile &at, const TileCells &c)
+{
+  constexpr int SLOTS = V == TTI_COORDINATE ? 11 : 3;
+  const AdjArgs &a = at.a;
+  const int lane = threadIdx.x & 31, z = c.z - lane;  // the warp's first row
+  if (z >= a.g.Nz - NH) return;
+  for (int q = lane; q < (tiled::TX / 4) * SLOTS; q += 32) {
+    const int col = q / SLOTS, k = q % SLOTS, x = c.xc + col;
+    if (x >= a.g.Nx - NH) continue;
+    const size_t i = (size_t)x * a.g.ldz + z;
+    const void *p;
+    if (k < 2) p = at.pk.cf + i + 16 * k;
+    else if (k == 2) p = a.p.invrho + i;
+    else if (k < 5) p = at.pk.vsc + i + 16 * (k - 3);
+    else if (k < 9) p = a.keep[4 + (k - 5)] + i;
+    else p = a.acc[5 + (k - 9)] + i;
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+  }
+}
+
 // transposed stress stencils into lambda_v, then the velocity-half adjoint
 // (maps: T0..T3; coordinate: the theta_v terms from the kept stress
 // derivative combinations P Q R S that the forward velocity kernel wrote)
@@ -621,6 +646,7 @@ __global__ void __launch_bounds__(tiled::NT, 3) k_adj_velocity_tiled(const __gri
     l[j][0] = on ? a.lam[0][i] : 0.0f;
     l[j][1] = on ? a.lam[1][i] : 0.0f;
   }
+  prefetch_adj_velocity<V>(at, c);
   if (!tiled::tma::wait_tiles(at.err, bar)) return;
   if (!zin) return;
   const float hx = a.hx, hz = a.hz;
