@@ -74,8 +74,10 @@ float *pinned_chunk()
       return p;
     }
   }
+  // portable: a chunk serves handles on any device of the process
   float *p = nullptr;
-  if (cudaMallocHost(reinterpret_cast<void **>(&p), PIN_CHUNK * sizeof(float)) != cudaSuccess) return nullptr;
+  if (cudaHostAlloc(reinterpret_cast<void **>(&p), PIN_CHUNK * sizeof(float), cudaHostAllocPortable) != cudaSuccess)
+    return nullptr;
   return p;
 }
 
