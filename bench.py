@@ -139,41 +139,109 @@ def geometry(rank: int):
 
 
 # ---------------------------------------------------------------- our arm
-def run_ours(args, rank, world, local_rank):
+def workload_config(variant: str, world: int) -> dict:
+    """The `config` block of both arms (same keys, so the two lines compare)."""
+    E = WORKLOAD["ealThick"] + 5
+    Nz, Nx = WORKLOAD["nz"] + 2 * E, WORKLOAD["nx"] + 2 * E
+    return {"workload": f"plain forward, {variant}, salt-like synthetic {WORKLOAD['nz']}x{WORKLOAD['nx']} "
+                        f"(padded {Nz}x{Nx}), freesurface, 12 Hz Ricker at the surface centre, "
+                        f"{WORKLOAD['nx']} receivers at z=2",
+            "variant": variant, "nz": WORKLOAD["nz"], "nx": WORKLOAD["nx"], "Nz": Nz, "Nx": Nx, "cells": Nz * Nx,
+            "dt": WORKLOAD["dt"], "parallelism": f"shots x{world}",
+            "l2": "inputs larger than L2 (>= 16 arrays x 41 MB per step)"}
+
+
+def traffic_per_launch(variant: str):
+    """DRAM bytes per launch of the two half-step kernels from the committed ncu
+    summary (scaled from a narrower capture, as the file says), or None."""
+    tfile = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        d = json.load(open(tfile))
+        return d.get(variant), d.get("_note", "")
+    except Exception:
+        return None, ""
+
+
+def measure_plain(variant, K, W, nprof, rank, world, local_rank, clock_window_s=1.0):
+    """Device-resident throughput of the plain path for one formulation: K timed
+    steps (CUDA events on the library's stream, max over ranks), the per-phase
+    split over `nprof` more steps, and the step-level roofline. The clock
+    sampler runs over the timed region and then over `clock_window_s` seconds
+    of the same steps (the timed region alone is too short for nvidia-smi)."""
     import ttifd
 
-    variant = args.variant
-    K, W = args.steps, args.warmup
     m = model()
     pads = synthetic.padded(m, WORKLOAD["ealThick"])
     sx, sz, gx, gz = geometry(rank)
-    cfg = dict(WORKLOAD, variant=variant, nt=W + K + args.profile_steps)
+    extra = 4000
+    cfg = dict(WORKLOAD, variant=variant, nt=W + K + nprof + extra)
     wav = synthetic.ricker(cfg["nt"], cfg["dt"], cfg["fpeak"])
-    h = ttifd.Modeling(device=local_rank, **cfg)
-    h.upload_model(*pads)
-    h.set_source([sx], [sz], wav[None, :])
-    for k in (0, 1, 2):
-        h.set_receivers(k, gx, gz)
-    cells = h.Nz * h.Nx
-    h.reset()
-    h.step(W)
-    dist_barrier()
-    l0 = h.kernel_launches
-    with ClockSampler(local_rank) as clk:
-        h.step(K)
-        ms = h.elapsed_ms
-    launches = h.kernel_launches - l0
-    ms_max = dist_max(ms)
-    # per-phase device time (events on the library's stream)
-    pv, ps, po = h.profile_steps(args.profile_steps)
-    h.close()
-    value = cells * K * world / (ms_max / 1e3) / 1e9
+    with ttifd.Modeling(device=local_rank, **cfg) as h:
+        h.upload_model(*pads)
+        h.set_source([sx], [sz], wav[None, :])
+        for k in (0, 1, 2):
+            h.set_receivers(k, gx, gz)
+        cells = h.Nz * h.Nx
+        h.reset()
+        h.step(W)
+        dist_barrier()
+        l0 = h.kernel_launches
+        with ClockSampler(local_rank) as clk:
+            h.step(K)
+            ms = h.elapsed_ms
+            launches = h.kernel_launches - l0
+            # the same steps again, untimed, so that the sampler sees the load
+            t0, left = time.perf_counter(), extra
+            while time.perf_counter() - t0 < clock_window_s and left > 0:
+                n = min(left, 500)
+                h.step(n)
+                left -= n
+        ms_max = dist_max(ms)
+        pv, ps, po = h.profile_steps(nprof)
+        Nz, Nx, E = h.Nz, h.Nx, h.E
+    peak, src = peaks()
+    step_ms = ms_max / K
+    alg = ALG_BYTES_STEP[variant]
+    achieved = alg * cells / (step_ms / 1e3) / 1e9
+    interior = (Nx - 10) * (Nz - 5 - E)  # free surface: rows [E, Nz-5)
+    traffic, tnote = traffic_per_launch(variant)
+    kernels = {}
+    for name, t in (("velocity", pv), ("stress", ps)):
+        if t == 0.0:
+            continue
+        kms = t / nprof
+        b = ALG_BYTES_HALF[variant][name] * interior
+        k = {"kernel": f"k_{name}_tiled<{variant}>", "alg_bytes_per_cell": ALG_BYTES_HALF[variant][name],
+             "cells_per_launch": interior, "launch_ms": kms, "achieved_GBps": b / (kms / 1e3) / 1e9,
+             "frac": b / (kms / 1e3) / 1e9 / peak}
+        if traffic and name in traffic:
+            k["ncu_dram_bytes"] = traffic[name]
+            k["ncu_frac"] = traffic[name] / (kms / 1e3) / 1e9 / peak
+        kernels[name] = k
+    step_traffic = sum(traffic[n] for n in ("velocity", "stress")) if traffic and ps > 0 else None
+    roof = {"bound": "hbm", "kernel": "time step (velocity + stress half-steps + column pass)",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": src,
+            "alg_bytes_per_cell_update": alg, "cells_per_step": cells, "step_ms": step_ms,
+            "traffic": step_traffic,
+            "traffic_note": ("DRAM bytes per step (velocity + stress launches) from ncu, scaled by interior cells "
+                             "from a narrower capture: " + tnote) if step_traffic else None,
+            "kernels": kernels,
+            "phase_ms_per_step": {"velocity": pv / nprof, "stress": ps / nprof, "other": po / nprof}}
+    return {"value": cells * K * world / (ms_max / 1e3) / 1e9, "ms_per_step": step_ms, "cells": cells,
+            "launches": launches, "roofline": roof, "clocks": clk.summary()}
 
-    # e2e: the whole public-API sequence from host buffers (pinned by the
-    # library where it stages): upload + precompute, geometry, K steps with
-    # snapshots delivered to the host, traces fetched.
+
+def measure_e2e(variant, K, rank, world, local_rank):
+    """The whole public-API sequence from host buffers: create, upload +
+    device precompute, geometry, K steps with snapshots delivered to the host,
+    traces fetched, destroy (wall clock, max over ranks)."""
+    import ttifd
+
+    m = model()
+    pads = synthetic.padded(m, WORKLOAD["ealThick"])
+    sx, sz, gx, gz = geometry(rank)
     cfg_e = dict(WORKLOAD, variant=variant, nt=K)
-    wav_e = wav[:K]
+    wav_e = synthetic.ricker(K, cfg_e["dt"], cfg_e["fpeak"])
     dist_barrier()
     phases = {}
     t0 = time.perf_counter()
@@ -190,55 +258,36 @@ def run_ours(args, rank, world, local_rank):
         phases["run"] = time.perf_counter() - t0 - sum(phases.values())
         trs = [he.fetch_traces(k) for k in (0, 1, 2)]
         phases["fetch"] = time.perf_counter() - t0 - sum(phases.values())
+        cells = he.Nz * he.Nx
     t_e2e = dist_max(time.perf_counter() - t0)
     phases["destroy"] = t_e2e - sum(phases.values())
     h2d = sum(a.nbytes for a in pads) + wav_e.nbytes + 3 * 2 * gx.nbytes
     d2h = sum(snaps) + sum(t.nbytes for t in trs)
-    e2e = {"value": cells * K * world / t_e2e / 1e9, "unit": "Gcell/s", "h2d_bytes_per_step": h2d / K,
-           "d2h_bytes_per_step": d2h / K, "wall_s": t_e2e, "phases_s": phases,
-           "includes": "tti_create..tti_destroy: model upload + device precompute, geometry, K steps, snapshots to host, traces"}
+    return {"value": cells * K * world / t_e2e / 1e9, "unit": "Gcell/s", "h2d_bytes_per_step": h2d / K,
+            "d2h_bytes_per_step": d2h / K, "wall_s": t_e2e, "phases_s": phases,
+            "includes": "tti_create..tti_destroy: model upload + device precompute, geometry, K steps, "
+                        "snapshots to host, traces"}
 
-    # roofline of the dominant kernel (per-launch algorithmic bytes / event time)
-    n = args.profile_steps
-    peak, src = peaks()
-    if ps == 0.0:  # one fused kernel per step: a launch is one whole time step
-        dom = "fused"
-        kname = f"k_fused<{variant}>"
-        alg = ALG_BYTES_STEP[variant]
-        units = cells
-        t_launch = pv / n / 1e3
-    else:
-        interior = (h.Nx - 10) * (h.Nz - 5 - h.E)  # freesurface: rows [E, Nz-5)
-        dom = "stress" if ps >= pv else "velocity"
-        kname = f"k_{dom}<{variant}>"
-        alg = ALG_BYTES_HALF[variant][dom]
-        units = interior
-        t_launch = (ps if dom == "stress" else pv) / n / 1e3
-    bytes_launch = alg * units
-    achieved = bytes_launch / t_launch / 1e9
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-    if os.path.exists(tfile):
-        try:
-            traffic = json.load(open(tfile)).get(variant, {}).get(dom)
-        except Exception:
-            traffic = None
-    roof = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": src, "traffic": traffic,
-            "alg_bytes_per_cell": alg, "cells_per_launch": units, "launch_ms": t_launch * 1e3,
-            "step": {"alg_bytes_per_cell_update": ALG_BYTES_STEP[variant],
-                     "achieved_GBps": ALG_BYTES_STEP[variant] * cells * K / (ms / 1e3) / 1e9,
-                     "frac": ALG_BYTES_STEP[variant] * cells * K / (ms / 1e3) / 1e9 / peak},
-            "phase_ms_per_step": {"velocity": pv / n, "stress": ps / n, "other": po / n}}
-    line = {"metric": "Gcell-updates/s", "value": value, "unit": "Gcell/s", "n_gpus": world, "steps": K,
-            "warmup": W, "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"plain forward, {variant}, salt-like synthetic 1126x7872 (padded 1256x8002), "
-                                   "freesurface, 12 Hz Ricker, 7872 receivers",
-                       "variant": variant, "nz": WORKLOAD["nz"], "nx": WORKLOAD["nx"], "Nz": h.Nz, "Nx": h.Nx,
-                       "cells": cells, "dt": WORKLOAD["dt"], "parallelism": f"shots x{world}",
-                       "l2": "inputs larger than L2 (>= 16 arrays x 41 MB per step)"},
-            "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary()}
+
+def run_ours(args, rank, world, local_rank):
+    variant = args.variant
+    K, W = args.steps, args.warmup
+    p = measure_plain(variant, K, W, args.profile_steps, rank, world, local_rank)
+    e2e = measure_e2e(variant, K, rank, world, local_rank)
+    line = {"metric": "Gcell-updates/s", "value": p["value"], "unit": "Gcell/s", "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": p["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": workload_config(variant, world),
+            "roofline": p["roofline"], "e2e": e2e, "gpu_launches": p["launches"], "clocks": p["clocks"]}
+    if not args.no_variants:
+        # the other two formulations on the same workload (BASELINE config: all three)
+        line["variants"] = {}
+        for v in ALG_BYTES_STEP:
+            if v == variant:
+                continue
+            q = measure_plain(v, K, W, args.profile_steps, rank, world, local_rank, clock_window_s=0.5)
+            q["e2e"] = measure_e2e(v, K, rank, world, local_rank)
+            q["config"] = workload_config(v, world)
+            line["variants"][v] = q
     return line
 
 
@@ -440,8 +489,10 @@ def run_reference_cpu(variant: str, budget_s: float = 20.0, max_steps: int = 400
             wav = synthetic.ricker(nt, WORKLOAD["dt"], WORKLOAD["fpeak"])
             synthetic.write_su_source(os.path.join(work, "src.su"), wav[None, :], [sx], [sz], WORKLOAD["dt"])
             synthetic.write_su_receivers(os.path.join(work, "rec.su"), gx, gz)
-            a = [f"{k}={v}" for k, v in WORKLOAD.items() if k not in ("wsave",)] + [
-                f"nt={nt}", "wsave=0", "shotID=1", f"sourcefile={work}/src.su", f"recposfile={work}/rec.su"]
+            # the same getpar values as our arm's workload (snapshots every
+            # snap_sample steps written by the reference inside its timed loop)
+            a = [f"{k}={v}" for k, v in WORKLOAD.items()] + [
+                f"nt={nt}", "shotID=1", f"sourcefile={work}/src.su", f"recposfile={work}/rec.su"]
             a += [f"{k}file={files[k]}" for k in ("vp", "vs", "rho", "epsilon", "delta", "theta")]
             r = subprocess.run([prog] + a, cwd=work, env=env, capture_output=True, text=True)
             mt = re.search(r"Finite difference modeling takes ([0-9.eE+-]+) s", r.stdout)
@@ -502,6 +553,8 @@ def main():
     ap.add_argument("--grad-ncheck", type=int, default=1,
                     help="gradient segments (1: every state kept, as the 600x1200 case fits in HBM)")
     ap.add_argument("--no-grad", action="store_true", help="skip the gradient measurement")
+    ap.add_argument("--no-variants", action="store_true",
+                    help="skip the other two formulations on the same workload")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     WORKLOAD["nx"] = args.nx
@@ -516,8 +569,7 @@ def main():
                 line = {"impl": "reference", "metric": "Gcell-updates/s", "value": cb["value"], "unit": "Gcell/s",
                         "n_gpus": world, "steps": cb["steps"], "warmup": 0, "higher_is_better": True,
                         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                        "config": {"workload": f"plain forward, {args.variant}, salt-like synthetic 1126x7872",
-                                   "variant": args.variant},
+                        "config": workload_config(args.variant, world),
                         "cpu_baseline": cb,
                         "e2e": {"value": cb["value"], "unit": "Gcell/s", "h2d_bytes_per_step": 0,
                                 "d2h_bytes_per_step": 0}}

@@ -165,16 +165,28 @@ int tti_profile_steps(tti_handle *h, int nsteps, float ms[3]);
 int tti_kernel_launches(const tti_handle *h, long long *n);
 
 /* Snapshot of the current wavefield without allocating device memory (no
- * counterpart in the reference). For callers that cannot allocate at the point
- * of the call, e.g. while a stream is being captured or under a fixed GPU
- * memory budget. `kind` as for tti_snapshot_fn; `out` receives nx_out records
- * of nz_out floats. The field is packed in a static device array of 16 Mi
- * floats (64 MiB per GPU, held from the library's first use on a device until
- * process exit); larger snapshots fail with TTI_ERR_ARG. Calls share that
- * array: calls whose GPU work overlaps race. The first call on each device
- * resolves the array's device address and should come before any stream
- * capture. */
+ * counterpart in the reference). For callers whose GPU memory must not grow
+ * at the point of the call: a host application whose device memory is
+ * budgeted by another framework's pool, or code that runs while another
+ * stream of the process is being captured into a CUDA graph (a device
+ * allocation there is refused and spoils that capture). `kind` as for
+ * tti_snapshot_fn; `out` receives nx_out records of nz_out floats.
+ * The field is packed in a static device array of 16 Mi floats (64 MiB per
+ * GPU); larger snapshots fail with TTI_ERR_ARG. With CUDA's default lazy
+ * module loading, the FIRST call on a device loads the library's snapshot
+ * module and so commits those 64 MiB (and resolves the array's device
+ * address); later calls allocate nothing, and the array is held until the
+ * process exits. Make that first call early (before a memory budget is fixed
+ * and before any stream capture starts). Calls share the array: calls whose
+ * GPU work overlaps race. The call copies to pageable memory and synchronises
+ * the handle's stream, so it returns TTI_ERR_STATE when that stream is being
+ * captured; captures of other streams (any capture mode, this thread or
+ * another) are left intact. */
 int tti_snapshot_static(tti_handle *h, int kind, float *out);
+/* The CUDA stream (a cudaStream_t) on which all of h's device work is
+ * ordered, for callers that order their own work after it (no counterpart in
+ * the reference). */
+int tti_get_stream(const tti_handle *h, void **stream);
 
 /* Recorded traces of one component, [ntrace][(nt-1)/mt+1] (Receiver2D.recv). */
 int tti_fetch_traces(tti_handle *h, int kind, float *out);
@@ -250,11 +262,19 @@ int tti_batch_upload_model(tti_batch *b, int m, const float *vp, const float *vs
  * 1: shot after shot), and the loop replays a CUDA graph of `graph_steps`
  * steps (0: no graph). */
 int tti_batch_set_order(tti_batch *b, int group, int graph_steps);
+/* In-tile schedule of the half-step kernels: 0 = row (one row of cells per
+ * thread, every stencil tap a shared-memory load), 1 = walk (each thread walks
+ * a diagonal, then an anti-diagonal, of the tile with the stencil taps in a
+ * sliding register window). Both give the same bits. */
+int tti_batch_set_schedule(tti_batch *b, int tile_schedule);
+/* The schedule in use (any output may be NULL). */
+int tti_batch_get_schedule(const tti_batch *b, int *group, int *graph_steps, int *tile_schedule);
 /* Times every group size in {all, 1, 2, 4, 8, 16} (those below the shot
- * count) with and without a graph of 20 steps, each over nsteps steps (at
- * least one graph replay, at most the longest instance's nt) in two rounds,
- * keeps the fastest and resets the batch. Outputs (may be NULL): the choice
- * and its ms per step. */
+ * count) with and without a graph of 20 steps, under both tile schedules,
+ * each over nsteps steps (at least one graph replay, at most the longest
+ * instance's nt) in two rounds, keeps the fastest and resets the batch.
+ * Outputs (may be NULL): the choice and its ms per step; the tile schedule
+ * chosen is read with tti_batch_get_schedule. */
 int tti_batch_autotune(tti_batch *b, int nsteps, int *group, int *graph_steps, float *ms_per_step);
 /* Zeroes every instance and rebuilds the launch tables from the current
  * sources and receivers. */

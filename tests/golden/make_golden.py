@@ -7,7 +7,7 @@ arrays, SU source and receiver files as bytes) and every file the reference
 wrote (SU traces, raw snapshots, setup dumps, energy text files), keyed by
 file name. Run from the repository root:
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle REF=<reference checkout> && python tests/golden/make_golden.py
 
 Needs the reference tree (read-only) only through the built programs.
 """
@@ -131,7 +131,7 @@ def run_case(name: str, seed: int) -> dict:
 
 def main():
     if not os.path.exists(os.path.join(REF, "sufdmod2dTTIelastic_coordinate_rotation")):
-        sys.exit("build the reference first: make -C oracle")
+        sys.exit("build the reference first: make -C oracle REF=<reference checkout>")
     for k, name in enumerate(CASES):
         rec = run_case(name, seed=100 + k)
         path = os.path.join(OUT, f"{name}.npz")

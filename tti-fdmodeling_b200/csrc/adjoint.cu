@@ -1282,6 +1282,9 @@ int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
     s->ckpt = s->keep = nullptr;
     if (cudaMalloc(&s->ckpt, sizeof(float) * nf * n * std::max(1, nseg - 1)) != cudaSuccess ||
         cudaMalloc(&s->keep, sizeof(float) * nk * n * seg) != cudaSuccess) {
+      cudaFree(s->ckpt);  // nothing half-allocated stays behind; the handle stays usable
+      cudaFree(s->keep);
+      s->ckpt = s->keep = nullptr;
       s->ncheck = s->seg = s->nkeep = 0;
       return gerr(h, TTI_ERR_NOMEM, "device allocation of the checkpoints failed (use fewer steps per segment)");
     }

@@ -199,6 +199,8 @@ int launch_one_step(tti_handle *h, const SourceTables &tab, cudaEvent_t *ev = nu
     ha.undamped_ok = h->undamped_ok;
     ha.freesurface = c.freesurface;
     tiled::set_square(ha, h->exact);
+    ha.walk = h->walk;
+    ha.wait_limit = h->wait_limit;
     ha.err = h->d_flag;
     ha.map[0] = tm[2];  // sxx szz sxz for the velocity update
     ha.map[1] = tm[3];
@@ -379,6 +381,11 @@ int create_handle(tti_handle **out, const tti_config *cfg, int device, const tti
   h->device = device;
   const char *ex = getenv("TTIFD_EXACT");
   h->exact = ex && ex[0] == '1';
+  const char *sched = getenv("TTIFD_SCHEDULE");
+  h->walk = sched && strcmp(sched, "walk") == 0;
+  // test hook: polls of the first TMA wait of the tiled kernels (the timeout path)
+  const char *wl = getenv("TTIFD_WAIT_LIMIT");
+  h->wait_limit = wl && *wl ? (unsigned)strtoul(wl, nullptr, 10) : tiled::tma::WAIT_LIMIT;
   Grid &g = h->g;
   g.E = cfg->ealThick + NH;
   g.Nz = cfg->nz + 2 * g.E;
@@ -872,6 +879,13 @@ int tti_kernel_launches(const tti_handle *h, long long *n)
   return TTI_OK;
 }
 
+int tti_get_stream(const tti_handle *h, void **stream)
+{
+  if (!h || !stream) return TTI_ERR_ARG;
+  *stream = static_cast<void *>(h->stream);
+  return TTI_OK;
+}
+
 int tti_elapsed_ms(const tti_handle *h, float *ms)
 {
   if (!h || !ms) return TTI_ERR_ARG;
@@ -893,7 +907,14 @@ int tti_fetch_traces(tti_handle *h, int kind, float *out)
     return set_err(h, TTI_ERR_ARG, "trace of %d samples is longer than the fetch supports", nts);
   const int per = (int)std::max<size_t>(1, STAGE / (size_t)nts);  // receivers per chunk
   const int nchunk = (n + per - 1) / per;
-  float *pin[2] = {pinned_chunk(), pinned_chunk()};
+  // A fetch of one chunk goes straight to the caller's block: staging would
+  // not overlap anything, and the first staged fetch of a process pays for
+  // page-locking the chunks (about 13 ms for two).
+  float *pin[2] = {nullptr, nullptr};
+  if (nchunk > 1) {
+    pin[0] = pinned_chunk();
+    pin[1] = pinned_chunk();
+  }
   for (int b = 0; b < 2 && pin[0] && pin[1]; ++b)
     if (!h->pev[5 + b] && cudaEventCreateWithFlags(&h->pev[5 + b], cudaEventDisableTiming) != cudaSuccess)
       pinned_release(pin[b]), pin[b] = nullptr;
@@ -916,7 +937,11 @@ int tti_fetch_traces(tti_handle *h, int kind, float *out)
         if (e == cudaSuccess) parallel_copy(out + (size_t)r0 * nts, pin[b], sizeof(float) * (size_t)nr * nts);
       }
     }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    // wait for the stream on the error path too: a device-to-host copy into a
+    // chunk may still be in flight, and a released chunk can go to another
+    // handle at once
+    const cudaError_t es = cudaStreamSynchronize(h->stream);
+    if (e == cudaSuccess) e = es;
     pinned_release(pin[0]);
     pinned_release(pin[1]);
     CK(h, e);

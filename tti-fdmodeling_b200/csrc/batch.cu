@@ -39,6 +39,7 @@ struct tti_batch {
   SourceTables *d_tab = nullptr;
   int *d_step = nullptr;
   int group = 0;  // work-table order: shots of a model interleaved tile by tile in groups of `group` (0: all)
+  bool walk = false;  // in-tile schedule of the half-step kernels: walk (true) or row
   int graph_steps = 20;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -106,6 +107,7 @@ int build_tables(tti_batch *b)
     ha.freesurface = c.freesurface;
     tiled::set_square(ha, b->exact);
     all_square = all_square && ha.square;
+    ha.wait_limit = h->wait_limit;
     ha.err = h->d_flag;
     ha.nt = c.nt;
     ha.tiles_z = (int)gr.x;
@@ -187,9 +189,11 @@ int build_tables(tti_batch *b)
 int launch_step(tti_batch *b)
 {
   const int n = (int)b->inst.size();
-  BCK(b, tiled::launch_velocity_batch(b->d_vel, b->d_work, b->nwork, b->d_step, b->variant, b->exact, b->square, b->stream));
+  BCK(b, tiled::launch_velocity_batch(b->d_vel, b->d_work, b->nwork, b->d_step, b->variant, b->exact, b->square,
+                                      b->walk, b->stream));
   if (b->any_vsrc) launch_sources_batch(b->d_src, n, b->d_step, b->stream);
-  BCK(b, tiled::launch_stress_batch(b->d_str, b->d_work, b->nwork, b->d_step, b->variant, b->exact, b->square, b->stream));
+  BCK(b, tiled::launch_stress_batch(b->d_str, b->d_work, b->nwork, b->d_step, b->variant, b->exact, b->square,
+                                    b->walk, b->stream));
   launch_post_batch(b->d_post, n, b->max_Nx, b->d_step, b->stream);
   launch_advance(b->d_step, b->stream);
   BCK(b, cudaGetLastError());
@@ -201,7 +205,7 @@ int launches_per_step(const tti_batch *b) { return 4 + (b->any_vsrc ? 1 : 0); }
 int ensure_graph(tti_batch *b)
 {
   if (b->exec || b->graph_steps <= 0) return TTI_OK;
-  BCK(b, tiled::prepare_batch(b->variant, b->exact, b->square));
+  BCK(b, tiled::prepare_batch(b->variant, b->exact, b->square, b->walk));
   BCK(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
   int rc = TTI_OK;
   for (int k = 0; k < b->graph_steps && rc == TTI_OK; ++k) rc = launch_step(b);
@@ -282,6 +286,8 @@ int tti_batch_create(tti_batch **out, int nmodels, const tti_config *cfg, int ni
   b->exact = ex && ex[0] == '1';
   const char *gs = getenv("TTIFD_GRAPH_STEPS");
   if (gs) b->graph_steps = atoi(gs);
+  const char *sched = getenv("TTIFD_SCHEDULE");
+  b->walk = sched && strcmp(sched, "walk") == 0;
   auto fail = [&](int rc, const std::string &msg) {
     tti_batch_destroy(b);
     return berr(nullptr, rc, "%s", msg.c_str());
@@ -355,6 +361,28 @@ int tti_batch_set_order(tti_batch *b, int group, int graph_steps)
   return TTI_OK;
 }
 
+int tti_batch_set_schedule(tti_batch *b, int tile_schedule)
+{
+  if (!b || tile_schedule < 0 || tile_schedule > 1) return berr(b, TTI_ERR_ARG, "tile schedule must be 0 or 1");
+  if ((tile_schedule == 1) != b->walk) {  // the captured launches select the kernels
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    b->walk = tile_schedule == 1;
+  }
+  return TTI_OK;
+}
+
+int tti_batch_get_schedule(const tti_batch *b, int *group, int *graph_steps, int *tile_schedule)
+{
+  if (!b) return TTI_ERR_ARG;
+  if (group) *group = b->group;
+  if (graph_steps) *graph_steps = b->graph_steps;
+  if (tile_schedule) *tile_schedule = b->walk ? 1 : 0;
+  return TTI_OK;
+}
+
 int tti_batch_reset(tti_batch *b)
 {
   if (!b) return TTI_ERR_ARG;
@@ -418,40 +446,46 @@ int tti_batch_autotune(tti_batch *b, int nsteps, int *group, int *graph_steps, f
   for (int g : {1, 2, 4, 8, 16})
     if (g < ninst_max) groups.push_back(g);
   const int graphs[] = {0, 20};
+  const int NS = 2;  // tile schedules: row, walk
   // Each candidate is timed twice, in two rounds over all of them, and keeps
   // its faster time; a graph candidate is timed over at least one replay of
   // its graph (the step loop only replays it when that many steps remain).
   const int warm = std::min(2, nsteps);
-  std::vector<float> t_best(groups.size() * 2, -1.0f);
+  std::vector<float> t_best(groups.size() * 2 * NS, -1.0f);
   for (int round = 0; round < 2; ++round)
+    for (int ts = 0; ts < NS; ++ts)
+      for (size_t gi = 0; gi < groups.size(); ++gi)
+        for (int q = 0; q < 2; ++q) {
+          const int g = groups[gi], gs = graphs[q];
+          int timed = nsteps - warm;
+          if (gs > 0) timed = std::max(timed, gs);
+          timed = std::min(timed, b->max_nt - warm);
+          if (timed <= 0) continue;
+          int rc = tti_batch_set_order(b, g, gs);
+          if (!rc) rc = tti_batch_set_schedule(b, ts);
+          if (!rc) rc = tti_batch_reset(b);
+          if (!rc) rc = tti_batch_step(b, warm);  // warm-up (and graph instantiation)
+          if (!rc) rc = tti_batch_step(b, timed);
+          if (rc) return rc;
+          const float t = b->last_ms / timed;
+          float &tb = t_best[(ts * groups.size() + gi) * 2 + q];
+          if (tb < 0 || t < tb) tb = t;
+        }
+  float best = -1.0f;
+  int bg = 0, bs = 20, bt = 0;
+  for (int ts = 0; ts < NS; ++ts)
     for (size_t gi = 0; gi < groups.size(); ++gi)
       for (int q = 0; q < 2; ++q) {
-        const int g = groups[gi], gs = graphs[q];
-        int timed = nsteps - warm;
-        if (gs > 0) timed = std::max(timed, gs);
-        timed = std::min(timed, b->max_nt - warm);
-        if (timed <= 0) continue;
-        int rc = tti_batch_set_order(b, g, gs);
-        if (!rc) rc = tti_batch_reset(b);
-        if (!rc) rc = tti_batch_step(b, warm);  // warm-up (and graph instantiation)
-        if (!rc) rc = tti_batch_step(b, timed);
-        if (rc) return rc;
-        const float t = b->last_ms / timed;
-        float &tb = t_best[gi * 2 + q];
-        if (tb < 0 || t < tb) tb = t;
+        const float t = t_best[(ts * groups.size() + gi) * 2 + q];
+        if (t >= 0 && (best < 0 || t < best)) {
+          best = t;
+          bg = groups[gi];
+          bs = graphs[q];
+          bt = ts;
+        }
       }
-  float best = -1.0f;
-  int bg = 0, bs = 20;
-  for (size_t gi = 0; gi < groups.size(); ++gi)
-    for (int q = 0; q < 2; ++q) {
-      const float t = t_best[gi * 2 + q];
-      if (t >= 0 && (best < 0 || t < best)) {
-        best = t;
-        bg = groups[gi];
-        bs = graphs[q];
-      }
-    }
   int rc = tti_batch_set_order(b, bg, bs);
+  if (!rc) rc = tti_batch_set_schedule(b, bt);
   if (!rc) rc = tti_batch_reset(b);
   if (rc) return rc;
   if (group) *group = bg;

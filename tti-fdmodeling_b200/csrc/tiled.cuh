@@ -32,6 +32,8 @@ struct alignas(64) HalfArgs {
   int nt;      // batched launches: time steps of this instance (its CTAs idle once the step counter reaches it)
   int tiles_z; // batched launches: tile rows of this instance's grid
   int square;  // FMA mode with dx == dz: stencil coefficients hc fold in h = 0.5 / dx
+  int walk;    // the walk schedule of the tile (register windows along the diagonals)
+  unsigned wait_limit;  // polls of the first TMA wait before it gives up (tma::WAIT_LIMIT)
   float hc[5]; // h * C_k
   // Gradient forward pass (null: nothing kept). Velocity update, coordinate
   // rotation: per cell the stress derivative combinations the adjoint's
@@ -64,12 +66,13 @@ cudaError_t launch_stress(const HalfArgs &a, int variant, bool exact, cudaStream
 // instance's arguments (z_base set), `work` (device) the CTA -> (instance, tile)
 // table; `step` (device) is the shared step counter.
 // `square`: every instance has square (folded) coefficients (set_square).
+// `walk`: the walk schedule of the tile instead of the row schedule.
 cudaError_t launch_velocity_batch(const HalfArgs *inst, const Work *work, int nwork, const int *step, int variant,
-                                  bool exact, bool square, cudaStream_t st);
+                                  bool exact, bool square, bool walk, cudaStream_t st);
 cudaError_t launch_stress_batch(const HalfArgs *inst, const Work *work, int nwork, const int *step, int variant,
-                                bool exact, bool square, cudaStream_t st);
+                                bool exact, bool square, bool walk, cudaStream_t st);
 // Sets the kernels' shared-memory attributes (call before a stream capture).
-cudaError_t prepare_batch(int variant, bool exact, bool square);
+cudaError_t prepare_batch(int variant, bool exact, bool square, bool walk);
 
 // Device side of the TMA halo tiles, shared by the tiled forward and adjoint kernels.
 namespace tma {
@@ -90,8 +93,12 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, u
                : "memory");
 }
 
-// bounded wait (about a second) so a copy that never lands cannot hang the GPU
-__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, unsigned limit = 1u << 20)
+// Polls of a bounded TMA wait (about a second): a copy that never lands cannot
+// hang the GPU. A handle may lower it (TTIFD_WAIT_LIMIT at tti_create) to run
+// the timeout path without a fault.
+constexpr unsigned WAIT_LIMIT = 1u << 20;
+
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, unsigned limit = WAIT_LIMIT)
 {
   const unsigned a = smem_u32(bar);
   for (unsigned n = 0; n < limit; ++n) {
@@ -137,9 +144,9 @@ __device__ __forceinline__ void issue_tiles(const CUtensorMap *map, float *sm, u
 }
 
 // returns false (all threads) after a timed-out wait
-__device__ __forceinline__ bool wait_tiles(int *err, unsigned long long *bar)
+__device__ __forceinline__ bool wait_tiles(int *err, unsigned long long *bar, unsigned limit = WAIT_LIMIT)
 {
-  const bool ok = mbar_wait(bar, 0);
+  const bool ok = mbar_wait(bar, 0, limit);
   if (__syncthreads_or(!ok)) {
     if (threadIdx.x == 0) {
       atomicOr(err, 4);

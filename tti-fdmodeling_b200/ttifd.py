@@ -100,6 +100,7 @@ _SIGNATURES = {
     "profile_steps": (C.c_int, [C.c_void_p, C.c_int, _FP]),
     "kernel_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
     "snapshot_static": (C.c_int, [C.c_void_p, C.c_int, _FP]),
+    "get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "grad_set_observed": (C.c_int, [C.c_void_p, C.c_int, _FP]),
     "grad_zero": (C.c_int, [C.c_void_p]),
     "grad_run": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double)]),
@@ -117,6 +118,8 @@ _BATCH_SIGNATURES = {
     "batch_instance": (C.c_void_p, [C.c_void_p, C.c_int]),
     "batch_upload_model": (C.c_int, [C.c_void_p, C.c_int] + [_FP] * 6),
     "batch_set_order": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "batch_set_schedule": (C.c_int, [C.c_void_p, C.c_int]),
+    "batch_get_schedule": (C.c_int, [C.c_void_p, _IP, _IP, _IP]),
     "batch_autotune": (C.c_int, [C.c_void_p, C.c_int, _IP, _IP, _FP]),
     "batch_reset": (C.c_int, [C.c_void_p]),
     "batch_step": (C.c_int, [C.c_void_p, C.c_int]),
@@ -273,6 +276,13 @@ class Modeling:
         self._call("snapshot_static", self._h, kind, _f(out))
         return out
 
+    @property
+    def stream(self) -> int:
+        """The handle's CUDA stream (cudaStream_t) as an integer."""
+        s = C.c_void_p()
+        self._call("get_stream", self._h, C.byref(s))
+        return s.value or 0
+
     def fetch_traces(self, kind) -> np.ndarray:
         out = np.empty((self._nrec.get(kind, 0), self.nts), np.float32)
         self._call("fetch_traces", self._h, kind, _f(out))
@@ -399,11 +409,21 @@ class Batch:
         """Shots interleaved per tile in groups of `group` (0: all); graph of `graph_steps` steps (0: none)."""
         self._call("batch_set_order", self._b, group, graph_steps)
 
+    def set_schedule(self, tile_schedule):
+        """In-tile schedule of the half-step kernels: "row" (0) or "walk" (1)."""
+        ts = {"row": 0, "walk": 1}.get(tile_schedule, tile_schedule)
+        self._call("batch_set_schedule", self._b, ts)
+
+    def schedule(self) -> dict:
+        g, gs, ts = C.c_int(), C.c_int(), C.c_int()
+        self._call("batch_get_schedule", self._b, C.byref(g), C.byref(gs), C.byref(ts))
+        return {"group": g.value, "graph_steps": gs.value, "tile_schedule": ["row", "walk"][ts.value]}
+
     def autotune(self, nsteps: int) -> dict:
         """Times the schedules on nsteps steps, keeps the fastest, resets the batch."""
         g, gs, ms = C.c_int(), C.c_int(), C.c_float()
         self._call("batch_autotune", self._b, nsteps, C.byref(g), C.byref(gs), C.byref(ms))
-        return {"group": g.value, "graph_steps": gs.value, "ms_per_step": ms.value}
+        return dict(self.schedule(), ms_per_step=ms.value)
 
     def reset(self):
         self._call("batch_reset", self._b)
