@@ -58,7 +58,21 @@ CASES = {
     # thin absorbing rim (E = 7): the source window reaches the padded edge
     "bond_thin_rim": ("bond_transformation", dict(ealThick=2, eal_alpha=1.7, seistype=2, wsave=0), "salt",
                       [(0, 0)], (5, 0)),
+    # Grids of several 128-row x 16-column kernel tiles (padded 310 x 210: 3 tile rows, 13 tile
+    # columns, tile edges at padded row 128 and columns 5 + 16 k). The source windows straddle a
+    # tile corner or a column edge; the receiver rows lie on a tile edge (padded row 128) or just
+    # above it. Traces and the final p snapshot only (no setup dumps, to keep the files small).
+    "coord_tiles": ("coordinate_rotation", dict(nz=280, nx=180, nt=400, seistype=3, wsave=2, snap_sample=399),
+                    "salt", [(43, 113)], (1, 113)),
+    "tensor_tiles_fs": ("tensor_rotation", dict(nz=280, nx=180, nt=400, freesurface=1, seistype=3, wsave=2,
+                                                snap_sample=399), "salt", [(43, 2)], (1, 98)),
+    "bond_tiles": ("bond_transformation", dict(nz=280, nx=180, nt=400, seistype=3, wsave=2, snap_sample=399),
+                   "salt", [(59, 113)], (2, 112)),
 }
+# cases whose setup dumps (D_, Beta_, coef*, invrho_, c*_, vs_, rho_) are not kept in the fixture
+NO_DUMPS = {"coord_tiles", "tensor_tiles_fs", "bond_tiles"}
+DUMP_PREFIXES = ("D_", "Beta_", "coef1_", "coef2_", "invrho_", "c11_", "c13_", "c15_", "c33_", "c35_", "c55_",
+                 "vs_", "rho_")
 
 
 def make_model(kind: str, nz: int, nx: int, seed: int):
@@ -114,6 +128,8 @@ def run_case(name: str, seed: int) -> dict:
             full = os.path.join(work, fn)
             if fn in ("src.su", "rec.su") or fn in {os.path.basename(v) for v in files.values()}:
                 continue
+            if name in NO_DUMPS and fn.startswith(DUMP_PREFIXES):
+                continue
             out["out/" + fn] = np.frombuffer(open(full, "rb").read(), dtype=np.uint8)
         rec = {
             "meta": np.frombuffer(json.dumps(dict(variant=variant, params=p, args=args, kind=kind,
@@ -132,7 +148,10 @@ def run_case(name: str, seed: int) -> dict:
 def main():
     if not os.path.exists(os.path.join(REF, "sufdmod2dTTIelastic_coordinate_rotation")):
         sys.exit("build the reference first: make -C oracle REF=<reference checkout>")
+    only = set(sys.argv[1:])  # case names to (re)generate; none: all of them
     for k, name in enumerate(CASES):
+        if only and name not in only:
+            continue
         rec = run_case(name, seed=100 + k)
         path = os.path.join(OUT, f"{name}.npz")
         np.savez_compressed(path, **rec)

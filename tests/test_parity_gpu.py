@@ -41,10 +41,13 @@ def _compare(name, got, gold, rtol, peak):
     assert compared >= 3
 
 
+@pytest.mark.parametrize("schedule", ["row", "walk"])
 @pytest.mark.parametrize("name", helpers.golden_names())
-def test_gpu_matches_reference_build(name, gpu_lib):
+def test_gpu_matches_reference_build(name, schedule, gpu_lib, monkeypatch):
+    """The default (FMA) arithmetic with either in-tile schedule of the tiled kernels."""
     import ttifd
 
+    monkeypatch.setenv("TTIFD_SCHEDULE", schedule)
     case = helpers.load_golden(name)
     got = helpers.run_backend(ttifd.Modeling, case)
     _compare(name, got, helpers.golden_arrays(case), TRACE_RTOL, TRACE_PEAK)
