@@ -223,6 +223,19 @@ int tti_grad_set_observed(tti_handle *h, int kind, const float *dobs);
 int tti_grad_zero(tti_handle *h);
 /* tti_elapsed_ms afterwards gives the device time of the whole run. */
 int tti_grad_run(tti_handle *h, int ncheck, double *misfit);
+/* The same gradient under binomial checkpointing (Revolve: Griewank and
+ * Walther, ACM TOMS 26(1), 2000). The nt steps are cut into macro-steps of
+ * `keep_steps` steps; the adjoint of a macro-step runs right after a forward
+ * recomputation of it that keeps its steps (keep_steps kept steps in memory),
+ * and the states at macro-step starts live in `snapshots` full-state slots
+ * placed by the binomial rule, which minimises the macro-steps advanced for
+ * that memory. Memory: snapshots full states + keep_steps kept steps. The
+ * result is bit-identical to tti_grad_run's. keep_steps = 1 is classic
+ * Revolve; snapshots >= nt / keep_steps - 1 recomputes every macro-step once. */
+int tti_grad_run_binomial(tti_handle *h, int snapshots, int keep_steps, double *misfit);
+/* Macro-steps the binomial schedule advances (recording passes excluded) to
+ * reverse `macro_steps` of them with `snapshots` slots; host only, no device. */
+long long tti_grad_schedule_cost(int macro_steps, int snapshots);
 int tti_grad_fetch(tti_handle *h, int which, float *out);
 /* dJ/d(source samples) of the last run, [nsrc][nt]: the stress source
  * (stype 1) reads the adjoint stresses after the residual injection; the

@@ -31,3 +31,9 @@ def gpu_lib():
 
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "tti-fdmodeling_b200"), "lib"], check=True)
     return ttifd.load()
+
+
+@pytest.fixture(scope="session")
+def gpu_free_lib(gpu_lib):
+    """The same library, for its host-only entry points (no device is touched)."""
+    return gpu_lib

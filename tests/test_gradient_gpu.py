@@ -91,6 +91,27 @@ def test_checkpoint_count_does_not_change_the_gradient(gpu_lib):
             assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("variant", ["coordinate_rotation", "tensor_rotation", "bond_transformation"])
+def test_binomial_schedule_equals_uniform(variant, gpu_lib):
+    """Binomial (Revolve) checkpointing, with slots from none to plenty and
+    macro-steps of 1 to 40 steps, gives the uniform schedule's gradient bit
+    for bit (the same forward steps and adjoint steps in the same order)."""
+    import ttifd
+
+    cfg, pads, true, w, gx = _case(1, variant=variant)
+    dobs = [np.zeros((gx.size, cfg["nt"]), np.float32) for _ in range(3)]
+    h, J0 = _device(cfg, pads, w, gx, dobs, 1)
+    with h:
+        ref = [h.grad_fetch(n) for n in NAMES]
+        for snapshots, keep in ((3, 1), (0, 40), (2, 17), (30, 7), (5, 220)):
+            h.grad_zero()
+            J = h.grad_run_binomial(snapshots, keep)
+            assert J == pytest.approx(J0, rel=1e-12)
+            for a, b, n in zip([h.grad_fetch(n) for n in NAMES], ref, NAMES):
+                assert np.array_equal(a, b), (snapshots, keep, n)
+    assert ttifd.schedule_cost(220, 3) > 220  # (3, 1) recomputes steps more than once
+
+
 def test_shots_accumulate(gpu_lib):
     cfg, pads, true, w, gx = _case(0)
     rng = np.random.default_rng(2)

@@ -1256,9 +1256,14 @@ int tti_grad_zero(tti_handle *h)
   return TTI_OK;
 }
 
-int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
+}  // extern "C"
+
+namespace {
+
+// Buffers and tables of a gradient run: `slots` full-state checkpoints and a
+// kept segment of `seg` steps (keep_fields each); the source tables in *tab.
+int grad_prepare(tti_handle *h, int slots, int seg, SourceTables *tab)
 {
-  if (!h || ncheck < 1) return TTI_ERR_ARG;
   int rc = grad_check(h);
   if (rc) return rc;
   GCK(h, cudaSetDevice(h->device));
@@ -1270,17 +1275,14 @@ int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
     const bool rec = (k < 2 ? want_v : want_p) && h->nrec[k] > 0;
     if (rec && !s->have_obs[k]) return gerr(h, TTI_ERR_STATE, "observed traces missing for a recorded component");
   }
-  const int nt = c.nt;
-  ncheck = std::min(ncheck, nt);
-  const int seg = (nt + ncheck - 1) / ncheck, nseg = (nt + seg - 1) / seg;
   const int nf = h->cfg.variant == TTI_TENSOR ? 8 : 5;  // fields of a full state (checkpoints)
   const int nk = keep_fields(h);                       // fields of a kept step
   const size_t n = h->g.n;
-  if (s->ncheck != nseg || s->seg != seg || s->nkeep != nk) {
+  if (s->ncheck != slots + 1 || s->seg != seg || s->nkeep != nk) {
     cudaFree(s->ckpt);
     cudaFree(s->keep);
     s->ckpt = s->keep = nullptr;
-    if (cudaMalloc(&s->ckpt, sizeof(float) * nf * n * std::max(1, nseg - 1)) != cudaSuccess ||
+    if (cudaMalloc(&s->ckpt, sizeof(float) * nf * n * std::max(1, slots)) != cudaSuccess ||
         cudaMalloc(&s->keep, sizeof(float) * nk * n * seg) != cudaSuccess) {
       cudaFree(s->ckpt);  // nothing half-allocated stays behind; the handle stays usable
       cudaFree(s->keep);
@@ -1288,10 +1290,11 @@ int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
       s->ncheck = s->seg = s->nkeep = 0;
       return gerr(h, TTI_ERR_NOMEM, "device allocation of the checkpoints failed (use fewer steps per segment)");
     }
-    s->ncheck = nseg;
+    s->ncheck = slots + 1;
     s->seg = seg;
     s->nkeep = nk;
   }
+  const int nt = c.nt;
   if (s->gsrc_n != h->nsrc * nt) {
     cudaFree(s->gsrc);
     s->gsrc = nullptr;
@@ -1299,27 +1302,19 @@ int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
     if (h->nsrc > 0) GCK(h, cudaMalloc(&s->gsrc, sizeof(float) * (size_t)h->nsrc * nt));
     s->gsrc_n = h->nsrc * nt;
   }
-  SourceTables tab;
-  handle_source_tables(h, &tab);
-  if ((rc = vsource_tables(h, tab))) return rc;
-  if ((rc = surface_origin(h, &s->surf_zorg, &s->surf_zend))) return rc;
-  // pass 1: forward with a checkpoint at every segment start but the last,
-  // whose states are kept directly (ncheck = 1: all states, no recomputation)
-  if ((rc = tti_reset(h))) return rc;
-  GCK(h, cudaEventRecord(h->ev0, h->stream));
-  for (int q = 0; q < nseg; ++q) {
-    const bool last = q == nseg - 1;
-    if (!last)
-      for (int f = 0; f < nf; ++f)
-        GCK(h, cudaMemcpyAsync(s->ckpt + ((size_t)q * nf + f) * n, h->fld[f], n * sizeof(float),
-                               cudaMemcpyDeviceToDevice, h->stream));
-    for (int k = q * seg; k < std::min(nt, (q + 1) * seg); ++k) {
-      float *keep[8] = {};
-      for (int f = 0; f < nk; ++f) keep[f] = s->keep + ((size_t)(k - q * seg) * nk + f) * n;
-      if ((rc = handle_step(h, tab, last ? keep : nullptr))) return rc;
-    }
-  }
-  // residuals and misfit
+  handle_source_tables(h, tab);
+  if ((rc = vsource_tables(h, *tab))) return rc;
+  return surface_origin(h, &s->surf_zorg, &s->surf_zend);
+}
+
+// Residuals d - dobs of every recorded component and J (read back into *J at
+// the end of the run), then the adjoint state zeroed.
+int grad_start_adjoint(tti_handle *h, double *J)
+{
+  GradState *s = h->grad;
+  const tti_config &c = h->cfg;
+  const bool want_v = c.seistype == 1 || c.seistype == 3, want_p = c.seistype == 2 || c.seistype == 3;
+  const size_t n = h->g.n;
   GCK(h, cudaMemsetAsync(s->d_J, 0, sizeof(double), h->stream));
   for (int k = 0; k < 3; ++k) {
     const bool rec = (k < 2 ? want_v : want_p) && h->nrec[k] > 0;
@@ -1328,36 +1323,252 @@ int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
     k_residual<<<std::min<size_t>(1024, (m + 255) / 256), 256, 0, h->stream>>>(h->d_rec[k], s->obs[k], s->res[k], m,
                                                                                s->d_J);
   }
-  double J = 0.0;
-  GCK(h, cudaMemcpyAsync(&J, s->d_J, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  // adjoint, segment by segment from the last
+  GCK(h, cudaMemcpyAsync(J, s->d_J, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   for (auto p : s->lam)
     if (p) GCK(h, cudaMemsetAsync(p, 0, n * sizeof(float), h->stream));
   for (auto p : s->T) GCK(h, cudaMemsetAsync(p, 0, n * sizeof(float), h->stream));
   if (s->gsrc) GCK(h, cudaMemsetAsync(s->gsrc, 0, sizeof(float) * (size_t)s->gsrc_n, h->stream));
   for (auto p : s->TV) GCK(h, cudaMemsetAsync(p, 0, n * sizeof(float), h->stream));
-  for (int q = nseg - 1; q >= 0; --q) {
-    const int k0 = q * seg, k1 = std::min(nt, (q + 1) * seg);
-    if (q < nseg - 1) {  // recompute the segment from its checkpoint
-      for (int f = 0; f < nf; ++f)
-        GCK(h, cudaMemcpyAsync(h->fld[f], s->ckpt + ((size_t)q * nf + f) * n, n * sizeof(float),
-                               cudaMemcpyDeviceToDevice, h->stream));
-      h->step_index = k0;
-      for (int k = k0; k < k1; ++k) {
-        float *keep[8] = {};
-        for (int f = 0; f < nk; ++f) keep[f] = s->keep + ((size_t)(k - k0) * nk + f) * n;
-        if ((rc = handle_step(h, tab, keep))) return rc;
-      }
-    }
-    for (int k = k1 - 1; k >= k0; --k)
-      if ((rc = adjoint_step(h, k, k - k0, tab))) return rc;
+  return TTI_OK;
+}
+
+// forward steps k0 .. k1-1 from the current state; `record`: what the adjoint
+// needs of each step goes to the kept segment (slot k - k0)
+int forward_steps(tti_handle *h, int k0, int k1, bool record, const SourceTables &tab)
+{
+  GradState *s = h->grad;
+  const int nk = s->nkeep;
+  for (int k = k0; k < k1; ++k) {
+    float *keep[8] = {};
+    if (record)
+      for (int f = 0; f < nk; ++f) keep[f] = s->keep + ((size_t)(k - k0) * nk + f) * h->g.n;
+    const int rc = handle_step(h, tab, record ? keep : nullptr);
+    if (rc) return rc;
   }
+  return TTI_OK;
+}
+
+int adjoint_steps(tti_handle *h, int k0, int k1, const SourceTables &tab)
+{
+  for (int k = k1 - 1; k >= k0; --k) {
+    const int rc = adjoint_step(h, k, k - k0, tab);
+    if (rc) return rc;
+  }
+  return TTI_OK;
+}
+
+int nfull(const tti_handle *h) { return h->cfg.variant == TTI_TENSOR ? 8 : 5; }
+
+int store_state(tti_handle *h, int slot)
+{
+  const size_t n = h->g.n;
+  for (int f = 0; f < nfull(h); ++f)
+    GCK(h, cudaMemcpyAsync(h->grad->ckpt + ((size_t)slot * nfull(h) + f) * n, h->fld[f], n * sizeof(float),
+                           cudaMemcpyDeviceToDevice, h->stream));
+  return TTI_OK;
+}
+
+// the state of step `step` from checkpoint `slot` (slot < 0: the zero state of step 0)
+int restore_state(tti_handle *h, int slot, int step)
+{
+  const size_t n = h->g.n;
+  for (int f = 0; f < nfull(h); ++f) {
+    if (slot < 0) GCK(h, cudaMemsetAsync(h->fld[f], 0, n * sizeof(float), h->stream));
+    else
+      GCK(h, cudaMemcpyAsync(h->fld[f], h->grad->ckpt + ((size_t)slot * nfull(h) + f) * n, n * sizeof(float),
+                             cudaMemcpyDeviceToDevice, h->stream));
+  }
+  h->step_index = step;
+  return TTI_OK;
+}
+
+int grad_finish(tti_handle *h, const double &J, double *misfit)
+{
   GCK(h, cudaEventRecord(h->ev1, h->stream));
   GCK(h, cudaEventSynchronize(h->ev1));
   GCK(h, cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
-  h->step_index = nt;
+  h->step_index = h->cfg.nt;
   if (misfit) *misfit = J;
   return handle_check_flag(h);
+}
+
+}  // namespace
+
+namespace ttifd {
+
+// One step of a gradient run's checkpoint schedule (macro-steps a .. b-1).
+struct Action {
+  enum Kind { ADVANCE, STORE, RESTORE, RECORD, START_ADJOINT, ADJOINT } kind;
+  int a, b, slot;
+};
+
+struct BinomialPlan {
+  int M, S;
+  std::vector<long long> T;  // T(l, c) at [c][l]
+  std::vector<int> D;        // best first split at [c][l]
+  BinomialPlan(int M_, int S_);
+  long long &t(int c, int l) { return T[(size_t)c * (M + 1) + l]; }
+  int &d(int c, int l) { return D[(size_t)c * (M + 1) + l]; }
+  int dd(int c, int l) const { return D[(size_t)c * (M + 1) + l]; }
+  void actions(std::vector<Action> &out) const;
+};
+
+// Binomial checkpointing (Griewank and Walther's Revolve, ACM TOMS 26(1), 2000),
+// stated here as its recursion. M macro-steps are reversed with S checkpoint
+// slots; the state at macro-step a is held (in a slot, or the zero state at
+// a = 0). reverse(a, b, c): if b - a = 1, restore x_a, record the macro-step
+// (forward keeping what its adjoint needs) and run its adjoint; if c = 0,
+// the same for each i = b-1 .. a after advancing from x_a to x_i; otherwise
+// advance to a + d, store that state in a free slot, reverse(a + d, b, c - 1),
+// release the slot and reverse(a, a + d, c). With T(l, c) the macro-steps
+// advanced (recording excluded) to reverse l of them with c free slots,
+//   T(l, 0) = l (l - 1) / 2,   T(1, c) = 0,
+//   T(l, c) = min_d  d + T(l - d, c - 1) + T(d, c),
+// an objective convex in d, so the best split is where its forward difference
+// turns non-negative (a binary search). The table costs O(M S log M) time.
+BinomialPlan::BinomialPlan(int M_, int S_) : M(M_), S(std::max(0, S_))
+{
+  T.assign((size_t)(S + 1) * (M + 1), 0);
+  D.assign((size_t)(S + 1) * (M + 1), 0);
+  for (int l = 1; l <= M; ++l) t(0, l) = (long long)l * (l - 1) / 2;
+  for (int c = 1; c <= S; ++c) {
+    t(c, 1) = 0;
+    for (int l = 2; l <= M; ++l) {
+      auto f = [&](int d) { return d + t(c - 1, l - d) + t(c, d); };
+      int lo = 1, hi = l - 1;  // smallest d with f(d + 1) >= f(d)
+      while (lo < hi) {
+        const int mid = (lo + hi) / 2;
+        if (f(mid + 1) >= f(mid)) hi = mid;
+        else lo = mid + 1;
+      }
+      t(c, l) = f(lo);
+      d(c, l) = lo;
+    }
+  }
+}
+
+void BinomialPlan::actions(std::vector<Action> &out) const
+{
+  struct Rec {
+    const BinomialPlan &p;
+    std::vector<Action> &out;
+    std::vector<char> used;
+    int cur = -1;  // macro-step whose start state is in the wavefields (-1: unknown)
+    bool first = true;
+    void emit(Action::Kind k, int a = 0, int b = 0, int slot = -1) { out.push_back(Action{k, a, b, slot}); }
+    void go(int a, int b, int c, int slot_a)
+    {
+      const int l = b - a;
+      if (l == 1 || c == 0) {
+        for (int i = b - 1; i >= a; --i) {
+          if (cur != i) {
+            if (cur != a) emit(Action::RESTORE, a, 0, slot_a);
+            if (i > a) emit(Action::ADVANCE, a, i);
+          }
+          emit(Action::RECORD, i, i + 1);
+          if (first) {
+            emit(Action::START_ADJOINT);
+            first = false;
+          }
+          emit(Action::ADJOINT, i, i + 1);
+          cur = i + 1;  // the recording left the state of macro-step i + 1
+        }
+        return;
+      }
+      const int m = a + p.dd(c, l);
+      if (cur != a) emit(Action::RESTORE, a, 0, slot_a);
+      emit(Action::ADVANCE, a, m);
+      int k = 0;
+      while (used[k]) ++k;
+      used[k] = 1;
+      emit(Action::STORE, m, 0, k);
+      cur = m;
+      go(m, b, c - 1, k);
+      used[k] = 0;
+      go(a, m, c, slot_a);
+    }
+  } r{*this, out, std::vector<char>(S + 1, 0)};
+  r.cur = 0;  // the run starts from the zero state of step 0
+  if (M > 0) r.go(0, M, S, -1);
+}
+
+}  // namespace ttifd
+
+extern "C" {
+
+long long tti_grad_schedule_cost(int macro_steps, int snapshots)
+{
+  if (macro_steps < 1 || snapshots < 0) return -1;
+  const ttifd::BinomialPlan p(macro_steps, snapshots);
+  std::vector<ttifd::Action> acts;
+  p.actions(acts);
+  long long adv = 0;
+  for (const auto &a : acts)
+    if (a.kind == ttifd::Action::ADVANCE) adv += a.b - a.a;
+  return adv;
+}
+
+int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
+{
+  if (!h || ncheck < 1) return TTI_ERR_ARG;
+  const int nt = h->cfg.nt;
+  ncheck = std::min(ncheck, nt);
+  const int seg = (nt + ncheck - 1) / ncheck, nseg = (nt + seg - 1) / seg;
+  SourceTables tab;
+  int rc = grad_prepare(h, nseg - 1, seg, &tab);
+  if (rc) return rc;
+  // pass 1: forward with a checkpoint at every segment start but the last,
+  // whose states are kept directly (ncheck = 1: all states, no recomputation)
+  if ((rc = tti_reset(h))) return rc;
+  GCK(h, cudaEventRecord(h->ev0, h->stream));
+  for (int q = 0; q < nseg; ++q) {
+    const bool last = q == nseg - 1;
+    if (!last && (rc = store_state(h, q))) return rc;
+    if ((rc = forward_steps(h, q * seg, std::min(nt, (q + 1) * seg), last, tab))) return rc;
+  }
+  double J = 0.0;
+  if ((rc = grad_start_adjoint(h, &J))) return rc;
+  // adjoint, segment by segment from the last
+  for (int q = nseg - 1; q >= 0; --q) {
+    const int k0 = q * seg, k1 = std::min(nt, (q + 1) * seg);
+    if (q < nseg - 1) {  // recompute the segment from its checkpoint
+      if ((rc = restore_state(h, q, k0))) return rc;
+      if ((rc = forward_steps(h, k0, k1, true, tab))) return rc;
+    }
+    if ((rc = adjoint_steps(h, k0, k1, tab))) return rc;
+  }
+  return grad_finish(h, J, misfit);
+}
+
+int tti_grad_run_binomial(tti_handle *h, int snapshots, int keep_steps, double *misfit)
+{
+  if (!h || snapshots < 0 || keep_steps < 1) return TTI_ERR_ARG;
+  const int nt = h->cfg.nt;
+  keep_steps = std::min(keep_steps, nt);
+  const int M = (nt + keep_steps - 1) / keep_steps;
+  snapshots = std::min(snapshots, M - 1);
+  SourceTables tab;
+  int rc = grad_prepare(h, snapshots, keep_steps, &tab);
+  if (rc) return rc;
+  const BinomialPlan plan(M, snapshots);
+  std::vector<Action> acts;
+  plan.actions(acts);
+  auto step_of = [&](int macro) { return std::min(nt, macro * keep_steps); };
+  if ((rc = tti_reset(h))) return rc;
+  GCK(h, cudaEventRecord(h->ev0, h->stream));
+  double J = 0.0;
+  for (const Action &a : acts) {
+    switch (a.kind) {
+    case Action::ADVANCE: rc = forward_steps(h, step_of(a.a), step_of(a.b), false, tab); break;
+    case Action::STORE: rc = store_state(h, a.slot); break;
+    case Action::RESTORE: rc = restore_state(h, a.slot, step_of(a.a)); break;
+    case Action::RECORD: rc = forward_steps(h, step_of(a.a), step_of(a.b), true, tab); break;
+    case Action::START_ADJOINT: rc = grad_start_adjoint(h, &J); break;
+    case Action::ADJOINT: rc = adjoint_steps(h, step_of(a.a), step_of(a.b), tab); break;
+    }
+    if (rc) return rc;
+  }
+  return grad_finish(h, J, misfit);
 }
 
 int tti_grad_fetch(tti_handle *h, int which, float *out)

@@ -104,6 +104,8 @@ _SIGNATURES = {
     "grad_set_observed": (C.c_int, [C.c_void_p, C.c_int, _FP]),
     "grad_zero": (C.c_int, [C.c_void_p]),
     "grad_run": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double)]),
+    "grad_run_binomial": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]),
+    "grad_schedule_cost": (C.c_longlong, [C.c_int, C.c_int]),
     "grad_fetch": (C.c_int, [C.c_void_p, C.c_int, _FP]),
     "grad_fetch_source": (C.c_int, [C.c_void_p, _FP]),
     "grad_accumulators": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t),
@@ -145,6 +147,11 @@ def load(path: str | None = None) -> C.CDLL:
     if path is None:
         _lib = lib
     return lib
+
+
+def schedule_cost(macro_steps: int, snapshots: int) -> int:
+    """Macro-steps advanced by the binomial schedule (tti_grad_schedule_cost; host only)."""
+    return int(load().tti_grad_schedule_cost(macro_steps, snapshots))
 
 
 def _f(a: np.ndarray):
@@ -307,6 +314,12 @@ class Modeling:
         """Adds this shot's gradient to the sums; returns its misfit J."""
         J = C.c_double()
         self._call("grad_run", self._h, ncheck, C.byref(J))
+        return J.value
+
+    def grad_run_binomial(self, snapshots: int, keep_steps: int) -> float:
+        """Binomial (Revolve) checkpointing: `snapshots` state slots, macro-steps of `keep_steps` steps."""
+        J = C.c_double()
+        self._call("grad_run_binomial", self._h, snapshots, keep_steps, C.byref(J))
         return J.value
 
     def grad_fetch(self, name) -> np.ndarray:
