@@ -92,10 +92,20 @@ class _DeviceArray:
 
 
 def gradient_sums(h):
-    """The 7 gradient sums of handle `h` (ttifd.Modeling) as torch views of its device memory."""
+    """The 7 gradient sums of handle `h` as torch views of its memory, without a
+    copy: device arrays for a library handle (ttifd.Modeling), host arrays for
+    a handle whose `device` is "cpu" (a host-memory stand-in with the same
+    grad_accumulators() interface, as the CPU tests use)."""
     import torch
 
     ptrs, n, _ = h.grad_accumulators()
+    if getattr(h, "device", 0) == "cpu":
+        import ctypes
+
+        import numpy as np
+
+        fp = ctypes.POINTER(ctypes.c_float)
+        return [torch.from_numpy(np.ctypeslib.as_array(ctypes.cast(p, fp), shape=(n,))) for p in ptrs]
     return [torch.as_tensor(_DeviceArray(p, n), device=f"cuda:{h.device}") for p in ptrs]
 
 
@@ -106,6 +116,9 @@ def reduce_gradient(group: Group, h) -> None:
         return
     import torch
 
-    torch.cuda.synchronize(h.device)
+    on_gpu = getattr(h, "device", 0) != "cpu"
+    if on_gpu:
+        torch.cuda.synchronize(h.device)
     group.allreduce_(gradient_sums(h))
-    torch.cuda.synchronize(h.device)
+    if on_gpu:
+        torch.cuda.synchronize(h.device)
