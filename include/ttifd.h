@@ -297,6 +297,17 @@ int tti_batch_step(tti_batch *b, int nsteps);
 /* reset + step(max nt): every instance from it = 0 to its own nt. */
 int tti_batch_run(tti_batch *b);
 int tti_batch_elapsed_ms(const tti_batch *b, float *ms);
+/* Gradients of all instances at once: each instance (with its source,
+ * receivers and tti_grad_set_observed traces) runs tti_grad_run_binomial
+ * with the given schedule from its own host thread on its own stream, so the
+ * shots' kernels overlap on the device, and the instances of a model share
+ * its parameter arrays. Afterwards the sums of a model's instances are added
+ * into its first instance (tti_grad_fetch there gives the model's gradient
+ * over those shots) and the other instances' sums are cleared.
+ * tti_batch_elapsed_ms gives the wall time of the whole call. misfits
+ * (may be NULL) receives each instance's J. The reference has no gradient;
+ * this replaces one adjoint run per shot. */
+int tti_batch_grad_run(tti_batch *b, int snapshots, int keep_steps, double *misfits);
 int tti_batch_kernel_launches(const tti_batch *b, long long *n);
 
 #ifdef __cplusplus

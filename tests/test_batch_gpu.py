@@ -134,3 +134,44 @@ def test_batch_autotune_keeps_results(monkeypatch, gpu_lib):
         for i in range(3):
             for c in range(3):
                 assert np.array_equal(b.instances[i].fetch_traces(c).view(np.uint32), ref[i][c].view(np.uint32))
+
+
+@pytest.mark.parametrize("variant", ["coordinate_rotation", "bond_transformation"])
+def test_batch_gradient_equals_sum_of_single_shots(variant, monkeypatch, gpu_lib):
+    """tti_batch_grad_run (the shots' gradients at once, one stream each) against
+    the same shots run one after another on one handle, whose sums accumulate."""
+    import ttifd
+
+    monkeypatch.delenv("TTIFD_EXACT", raising=False)
+    cfg = _model_cfg(120, 160, 140, 1, 1, variant)
+    cfg = dict(cfg, seistype=1)
+    models = _models([cfg])
+    shots = [(30, 2), (80, 2), (130, 3)]
+    gx = np.arange(0, cfg["nx"], 2, dtype=np.int32)
+    w = synthetic.ricker(cfg["nt"], cfg["dt"], cfg["fpeak"])[None, :]
+    dobs = np.zeros((gx.size, (cfg["nt"] - 1) // cfg["mt"] + 1), np.float32)
+    with ttifd.Batch([cfg], [0] * len(shots)) as b:
+        b.upload_model(0, *models[0])
+        for i, (sx, sz) in enumerate(shots):
+            inst = b.instances[i]
+            inst.set_source([sx], [sz], w)
+            for k in (0, 1):
+                inst.set_receivers(k, gx, 4)
+                inst.grad_set_observed(k, dobs)
+        Jb = b.grad_run(4, 10)
+        got = {n: b.instances[0].grad_fetch(n) for n in ("vp", "eps", "delta", "theta")}
+    with ttifd.Modeling(**cfg) as h:
+        h.upload_model(*models[0])
+        h.grad_zero()
+        Js = []
+        for sx, sz in shots:
+            h.set_source([sx], [sz], w)
+            for k in (0, 1):
+                h.set_receivers(k, gx, 4)
+                h.grad_set_observed(k, dobs)
+            Js.append(h.grad_run_binomial(4, 10))
+        ref = {n: h.grad_fetch(n) for n in got}
+    assert Jb == pytest.approx(Js, rel=1e-12)
+    for n in got:
+        err = np.linalg.norm(got[n].astype(np.float64) - ref[n]) / np.linalg.norm(ref[n].astype(np.float64))
+        assert err <= 1e-6, (n, err)

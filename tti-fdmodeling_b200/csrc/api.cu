@@ -322,6 +322,56 @@ int check_flag(tti_handle *h)
   return TTI_OK;
 }
 
+// Copies na host arrays [Nx][Nz] into pitched device arrays [Nx][ldz] on h's
+// stream. Through two page-locked chunks, column blocks at a time: host
+// threads copy block c into one chunk while the DMA engine moves block c - 1
+// from the other (TTIFD_UPLOAD=pageable: straight from the caller's pageable
+// arrays, which the driver stages itself, about 10.5 GB/s on B200 hosts).
+int upload_arrays(tti_handle *h, const float *const *src, float *const *dst, int na)
+{
+  const Grid &g = h->g;
+  const size_t col = (size_t)g.Nz * sizeof(float), dpitch = (size_t)g.ldz * sizeof(float);
+  const char *mode = getenv("TTIFD_UPLOAD");
+  const bool pageable = mode && strcmp(mode, "pageable") == 0;
+  const int per = (int)std::min<size_t>(g.Nx, PIN_CHUNK / g.Nz);  // columns per chunk
+  float *pin[2] = {nullptr, nullptr};
+  if (!pageable && per > 0) {
+    pin[0] = pinned_chunk();
+    pin[1] = pinned_chunk();
+  }
+  for (int b = 0; b < 2 && pin[0] && pin[1]; ++b)
+    if (!h->pev[5 + b] && cudaEventCreateWithFlags(&h->pev[5 + b], cudaEventDisableTiming) != cudaSuccess)
+      pinned_release(pin[b]), pin[b] = nullptr;
+  if (!pin[0] || !pin[1]) {
+    pinned_release(pin[0]);
+    pinned_release(pin[1]);
+    for (int k = 0; k < na; ++k)
+      CK(h, cudaMemcpy2DAsync(dst[k], dpitch, src[k], col, col, g.Nx, cudaMemcpyHostToDevice, h->stream));
+    return TTI_OK;
+  }
+  cudaError_t e = cudaSuccess;
+  bool pending[2] = {false, false};
+  int c = 0;
+  for (int k = 0; k < na && e == cudaSuccess; ++k)
+    for (int x0 = 0; x0 < g.Nx && e == cudaSuccess; x0 += per, ++c) {
+      const int nx = std::min(per, g.Nx - x0), b = c & 1;
+      if (pending[b]) e = cudaEventSynchronize(h->pev[5 + b]);  // chunk b's previous DMA has drained
+      if (e != cudaSuccess) break;
+      parallel_copy(pin[b], src[k] + (size_t)x0 * g.Nz, col * nx);
+      e = cudaMemcpy2DAsync(dst[k] + (size_t)x0 * g.ldz, dpitch, pin[b], col, col, nx, cudaMemcpyHostToDevice,
+                            h->stream);
+      if (e == cudaSuccess) e = cudaEventRecord(h->pev[5 + b], h->stream);
+      pending[b] = true;
+    }
+  // the chunks go back to the shared free list only once their copies are done
+  const cudaError_t es = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess) e = es;
+  pinned_release(pin[0]);
+  pinned_release(pin[1]);
+  CK(h, e);
+  return TTI_OK;
+}
+
 int copy_out_pitched(tti_handle *h, const float *src, float *out)
 {
   const Grid &g = h->g;
@@ -534,9 +584,11 @@ int tti_destroy(tti_handle *h)
   pool_free(h->d_src, fs);
   pool_free(h->d_energy, fs);
   pool_free(h->d_flag, fs);
-  pool_free(h->m_eps, fs);
-  pool_free(h->m_delta, fs);
-  pool_free(h->m_theta, fs);
+  if (!h->owner) {  // a batch instance borrows its model's copies
+    pool_free(h->m_eps, fs);
+    pool_free(h->m_delta, fs);
+    pool_free(h->m_theta, fs);
+  }
   pool_free(h->d_snap, fs);
   pool_free(h->d_stage, fs);
   if (fs) cudaStreamSynchronize(fs);
@@ -588,15 +640,8 @@ int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const floa
     cudaError_t e = pool_alloc(reinterpret_cast<void **>(&raw_block), 6 * g.n * sizeof(float), h->stream);
     if (e != cudaSuccess) rc = set_err(h, TTI_ERR_NOMEM, "device allocation failed: %s", cudaGetErrorString(e));
   }
-  // straight from the caller's pageable arrays: about 10.5 GB/s on B200 hosts;
-  // staging through page-locked chunks with host threads measured no faster
-  // there once the copies into the chunks are counted
-  for (int k = 0; k < 6 && rc == TTI_OK; ++k) {
-    raw[k] = raw_block + (size_t)k * g.n;
-    const cudaError_t e = cudaMemcpy2DAsync(raw[k], (size_t)g.ldz * sizeof(float), src[k], (size_t)g.Nz * sizeof(float),
-                                            (size_t)g.Nz * sizeof(float), g.Nx, cudaMemcpyHostToDevice, h->stream);
-    if (e != cudaSuccess) rc = set_err(h, TTI_ERR_CUDA, "model upload: %s", cudaGetErrorString(e));
-  }
+  for (int k = 0; k < 6; ++k) raw[k] = raw_block + (size_t)k * g.n;
+  if (rc == TTI_OK) rc = upload_arrays(h, src, raw, 6);
   if (rc == TTI_OK) {
     // MEAL scalars evaluated with the host libm, as meal.c:23-29, 62-66 do
     const int nl = g.E;

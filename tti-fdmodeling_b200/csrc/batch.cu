@@ -7,6 +7,8 @@
 // step counter, so the launches of G steps are captured once in a CUDA graph
 // and the graph is replayed for the whole loop.
 #include <algorithm>
+#include <chrono>
+#include <thread>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -73,6 +75,30 @@ int berr(tti_batch *b, int code, const char *fmt, ...)
                   cudaGetErrorString(e_));                                                             \
   } while (0)
 
+// Instances read their model's state: uploaded or not, the undamped-tile flag,
+// and (for the gradient's chain rule) the model's epsilon, delta, theta.
+void sync_instances(tti_batch *b)
+{
+  for (size_t i = 0; i < b->inst.size(); ++i) {
+    tti_handle *h = b->inst[i];
+    const tti_handle *mh = b->models[b->model_of[i]];
+    h->have_model = mh->have_model;
+    h->undamped_ok = mh->undamped_ok;
+    if (h != mh) {
+      h->m_eps = mh->m_eps;
+      h->m_delta = mh->m_delta;
+      h->m_theta = mh->m_theta;
+    }
+  }
+}
+
+// dst[i] += src[i], i < n
+__global__ void k_accumulate(float *dst, const float *src, size_t n)
+{
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] += src[i];
+}
+
 // Fills the device tables from the instances' current sources and receivers.
 int build_tables(tti_batch *b)
 {
@@ -84,11 +110,9 @@ int build_tables(tti_batch *b)
   for (int m = 0; m < nm; ++m) handle_source_tables(b->models[m], &tab[m]);
   std::vector<int> tiles(n);
   bool all_square = true;
+  sync_instances(b);
   for (int i = 0; i < n; ++i) {
     tti_handle *h = b->inst[i];
-    const tti_handle *mh = b->models[b->model_of[i]];
-    h->have_model = mh->have_model;
-    h->undamped_ok = mh->undamped_ok;
     const tti_config &c = h->cfg;
     const StepArgs a = handle_step_args(h);
     const CUtensorMap *tm = static_cast<const CUtensorMap *>(h->tmaps);
@@ -491,6 +515,57 @@ int tti_batch_autotune(tti_batch *b, int nsteps, int *group, int *graph_steps, f
   if (group) *group = bg;
   if (graph_steps) *graph_steps = bs;
   if (ms_per_step) *ms_per_step = best;
+  return TTI_OK;
+}
+
+int tti_batch_grad_run(tti_batch *b, int snapshots, int keep_steps, double *misfits)
+{
+  if (!b || snapshots < 0 || keep_steps < 1) return berr(b, TTI_ERR_ARG, "bad gradient schedule");
+  BCK(b, cudaSetDevice(b->device));
+  for (size_t m = 0; m < b->models.size(); ++m)
+    if (!b->models[m]->have_model) return berr(b, TTI_ERR_STATE, "model %zu not uploaded", m);
+  sync_instances(b);
+  const int n = (int)b->inst.size();
+  std::vector<int> rc(n, TTI_OK);
+  std::vector<double> J(n, 0.0);
+  const auto t0 = std::chrono::steady_clock::now();
+  {
+    // one host thread per instance: each drives its own stream, so the
+    // kernels of different shots overlap on the device
+    std::vector<std::thread> th;
+    th.reserve(n);
+    for (int i = 0; i < n; ++i)
+      th.emplace_back([&, i] {
+        cudaSetDevice(b->device);
+        rc[i] = tti_grad_run_binomial(b->inst[i], snapshots, keep_steps, &J[i]);
+      });
+    for (auto &t : th) t.join();
+  }
+  for (int i = 0; i < n; ++i)
+    if (rc[i]) return berr(b, rc[i], "instance %d: %s", i, tti_last_error(b->inst[i]));
+  // the instances' sums into their model's first instance, the others cleared
+  for (size_t m = 0; m < b->models.size(); ++m) {
+    tti_handle *mh = b->models[m];
+    float *dst[7];
+    size_t cnt = 0;
+    if (tti_grad_accumulators(mh, dst, &cnt, nullptr)) return berr(b, TTI_ERR_STATE, "%s", tti_last_error(mh));
+    for (int i = 0; i < n; ++i) {
+      tti_handle *h = b->inst[i];
+      if (b->model_of[i] != (int)m || h == mh) continue;
+      float *src[7];
+      if (tti_grad_accumulators(h, src, nullptr, nullptr)) return berr(b, TTI_ERR_STATE, "%s", tti_last_error(h));
+      for (int k = 0; k < 7; ++k) {
+        k_accumulate<<<1184, 256, 0, mh->stream>>>(dst[k], src[k], cnt);
+        BCK(b, cudaMemsetAsync(src[k], 0, cnt * sizeof(float), mh->stream));
+      }
+      b->launches += 7;
+    }
+    BCK(b, cudaGetLastError());
+    BCK(b, cudaStreamSynchronize(mh->stream));
+  }
+  b->last_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  if (misfits)
+    for (int i = 0; i < n; ++i) misfits[i] = J[i];
   return TTI_OK;
 }
 

@@ -128,6 +128,7 @@ _BATCH_SIGNATURES = {
     "batch_run": (C.c_int, [C.c_void_p]),
     "batch_elapsed_ms": (C.c_int, [C.c_void_p, _FP]),
     "batch_kernel_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    "batch_grad_run": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]),
 }
 _SIGNATURES.update(_BATCH_SIGNATURES)
 EXPORTS = ["tti_" + k for k in _SIGNATURES]
@@ -446,6 +447,12 @@ class Batch:
 
     def run(self):
         self._call("batch_run", self._b)
+
+    def grad_run(self, snapshots: int, keep_steps: int) -> list:
+        """All instances' gradients at once (tti_batch_grad_run); returns each instance's J."""
+        J = (C.c_double * len(self.instances))()
+        self._call("batch_grad_run", self._b, snapshots, keep_steps, J)
+        return list(J)
 
     @property
     def elapsed_ms(self) -> float:
