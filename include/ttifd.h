@@ -236,6 +236,12 @@ int tti_grad_run_binomial(tti_handle *h, int snapshots, int keep_steps, double *
 /* Macro-steps the binomial schedule advances (recording passes excluded) to
  * reverse `macro_steps` of them with `snapshots` slots; host only, no device. */
 long long tti_grad_schedule_cost(int macro_steps, int snapshots);
+/* Chooses (snapshots, keep_steps) for tti_grad_run_binomial on h so that the
+ * checkpoint slots and kept steps fit in budget_bytes of device memory with
+ * the fewest forward steps (*forward_steps, may be NULL: advances plus one
+ * recording pass). TTI_ERR_NOMEM when not even one kept step fits. Host only. */
+int tti_grad_plan(const tti_handle *h, double budget_bytes, int *snapshots, int *keep_steps,
+                  long long *forward_steps);
 int tti_grad_fetch(tti_handle *h, int which, float *out);
 /* dJ/d(source samples) of the last run, [nsrc][nt]: the stress source
  * (stype 1) reads the adjoint stresses after the residual injection; the

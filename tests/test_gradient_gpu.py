@@ -275,3 +275,29 @@ def test_gradient_sampling_and_components(mt, seistype, variant, gpu_lib):
             err = _rel(h.grad_fetch(name), g_ref[name])
             assert err <= 2e-5, (name, err)
         assert _rel(h.grad_fetch_source(1), gs_ref) <= 5e-5
+
+
+def test_gradient_plan_fits_budget_and_runs(gpu_lib):
+    """tti_grad_plan: the schedule for a memory budget fits it, more memory never
+    costs more forward steps, and the planned run gives the gradient of the
+    schedule that keeps every step."""
+    cfg, pads, true, w, gx = _case(0)
+    dobs = [np.zeros((gx.size, cfg["nt"]), np.float32) for _ in range(3)]
+    h, _ = _device(cfg, pads, w, gx, dobs, 1)
+    with h:
+        ref = [h.grad_fetch(n) for n in NAMES]
+        cell = h.grad_plan(1e15)  # unbounded: every step kept, no recomputation
+        assert cell == {"snapshots": 0, "keep_steps": cfg["nt"], "forward_steps": cfg["nt"]}
+        state = 5 * h.Nx * ((h.Nz + 31) // 32 * 32) * 4.0
+        prev = None
+        for budget in (3 * state, 12 * state, 60 * state):
+            p = h.grad_plan(budget)
+            kept = 8 * state / 5
+            assert p["snapshots"] * state + p["keep_steps"] * kept <= budget
+            if prev is not None:
+                assert p["forward_steps"] <= prev
+            prev = p["forward_steps"]
+            h.grad_zero()
+            h.grad_run_binomial(p["snapshots"], p["keep_steps"])
+            for a, b in zip([h.grad_fetch(n) for n in NAMES], ref):
+                assert np.array_equal(a, b)

@@ -1508,6 +1508,44 @@ long long tti_grad_schedule_cost(int macro_steps, int snapshots)
   return adv;
 }
 
+int tti_grad_plan(const tti_handle *h, double budget_bytes, int *snapshots, int *keep_steps, long long *forward_steps)
+{
+  if (!h || !snapshots || !keep_steps) return TTI_ERR_ARG;
+  const int nt = h->cfg.nt;
+  const double state = (double)(h->cfg.variant == TTI_TENSOR ? 8 : 5) * h->g.n * sizeof(float);
+  const double kept = (double)keep_fields(h) * h->g.n * sizeof(float);
+  // macro-step lengths on a geometric grid; the slots left over for each
+  long long best = -1;
+  int bs = 0, bl = 0;
+  for (int L = 1; L <= nt; L = std::max(L + 1, (int)(L * 1.25))) {
+    const int M = (nt + L - 1) / L;
+    if (M > 4000) continue;  // keeps the cost table small; longer macro-steps come next
+    const double left = budget_bytes - L * kept;
+    if (left < 0) break;  // longer macro-steps need still more memory
+    int s = (int)std::min<double>(M - 1, std::floor(left / state));
+    long long adv;
+    if (s >= M - 1) {
+      adv = M - 1;  // every macro-step start stored in one sweep
+    } else {
+      s = std::min(s, 256);  // beyond that, more slots save little (and the table grows)
+      adv = ttifd::BinomialPlan(M, s).t(s, M);
+    }
+    const long long cost = adv * L + nt;  // advances plus one recording pass
+    if (best < 0 || cost < best) {
+      best = cost;
+      bs = s;
+      bl = L;
+    }
+  }
+  if (best < 0)
+    return gerr(const_cast<tti_handle *>(h), TTI_ERR_NOMEM,
+                "the memory budget holds no kept step: no checkpoint schedule fits");
+  *snapshots = bs;
+  *keep_steps = bl;
+  if (forward_steps) *forward_steps = best;
+  return TTI_OK;
+}
+
 int tti_grad_run(tti_handle *h, int ncheck, double *misfit)
 {
   if (!h || ncheck < 1) return TTI_ERR_ARG;

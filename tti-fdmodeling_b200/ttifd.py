@@ -106,6 +106,7 @@ _SIGNATURES = {
     "grad_run": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double)]),
     "grad_run_binomial": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]),
     "grad_schedule_cost": (C.c_longlong, [C.c_int, C.c_int]),
+    "grad_plan": (C.c_int, [C.c_void_p, C.c_double, _IP, _IP, C.POINTER(C.c_longlong)]),
     "grad_fetch": (C.c_int, [C.c_void_p, C.c_int, _FP]),
     "grad_fetch_source": (C.c_int, [C.c_void_p, _FP]),
     "grad_accumulators": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t),
@@ -322,6 +323,12 @@ class Modeling:
         J = C.c_double()
         self._call("grad_run_binomial", self._h, snapshots, keep_steps, C.byref(J))
         return J.value
+
+    def grad_plan(self, budget_bytes: float) -> dict:
+        """Binomial schedule that fits `budget_bytes` of checkpoints and kept steps (tti_grad_plan)."""
+        s, k, f = C.c_int(), C.c_int(), C.c_longlong()
+        self._call("grad_plan", self._h, float(budget_bytes), C.byref(s), C.byref(k), C.byref(f))
+        return {"snapshots": s.value, "keep_steps": k.value, "forward_steps": f.value}
 
     def grad_fetch(self, name) -> np.ndarray:
         out = np.empty((self.Nx, self.Nz), np.float32)
