@@ -388,6 +388,7 @@ def run_batched_uneven(args, local_rank):
         with ClockSampler(local_rank) as clk:
             b.step(K)
             ms = b.elapsed_ms
+        used = device_memory_in_use(local_rank)
     total = sum(cells)
     per = [c * K / (ms / 1e3) / 1e9 for c in cells]
     return {"workload": f"batched forward, {args.variant}, {M} independent layered models of seeded sizes "
@@ -395,7 +396,18 @@ def run_batched_uneven(args, local_rank):
             "models": M, "steps": K, "cells_total": total, "value": total * K / (ms / 1e3) / 1e9, "unit": "Gcell/s",
             "ms_per_step": ms / K, "per_instance_gcells": {"min": min(per), "median": float(np.median(per)),
                                                             "max": max(per)},
-            "schedule": tuned, "clocks": clk.summary()}
+            "window": f"rates over a window of {K} steps after {W} warm-up steps, not over each instance's whole "
+                      "nt (every instance's nt is at least 1000, so all of them run through the window)",
+            "device_memory_in_use_GB": used, "schedule": tuned, "clocks": clk.summary()}
+
+
+def device_memory_in_use(device: int) -> float:
+    """Device memory in use (total - free, GB) while the batch's buffers are held:
+    the footprint of the run (this process's allocations, no other user)."""
+    import torch
+
+    free, total = torch.cuda.mem_get_info(device)
+    return (total - free) / 1e9
 
 
 # ---------------------------------------------------------------- gradient arm
@@ -459,6 +471,142 @@ def run_gradient(args, local_rank):
             "cost_vs_forward": grad_ms / fwd_ms, "value": cells * K / (grad_ms / 1e3) / 1e9, "unit": "Gcell/s",
             "ncheck30_ms": grad30_ms, "ncheck30_cost_vs_forward": grad30_ms / fwd_ms,
             "misfit": J, "grad_vp_norm": gnorm, "grad_vp_max_abs": gmax}
+
+
+def grad_models():
+    """The gradient workload's true and start models (layered 600 x 1200, seed 3;
+    start = Gaussian blur, sigma 15 cells = 150 m, of vp, epsilon, delta and theta;
+    vs and rho derived from the blurred vp and held fixed)."""
+    from scipy.ndimage import gaussian_filter
+
+    gw = GRAD_WORKLOAD
+    true = synthetic.layered_model(gw["nz"], gw["nx"], seed=3)
+    blur = [gaussian_filter(np.asarray(a, np.float64), 15.0).astype(np.float32)
+            for a in (true.vp, true.epsilon, true.delta, true.theta)]
+    vs = (blur[0] / 1.8).astype(np.float32)
+    rho = (310.0 * blur[0] ** 0.25).astype(np.float32)
+    start = synthetic.Model(blur[0], vs, rho, blur[1], blur[2], blur[3])
+    true = synthetic.Model(true.vp, vs, rho, true.epsilon, true.delta, true.theta)
+    return true, start
+
+
+def run_gradient_shots(args, local_rank):
+    """The gradient configuration as specified: 16 surface shots evenly spaced
+    on the 600 x 1200 layered model, `grad_steps` steps, 30 checkpoints (29
+    full-state slots and a kept segment of steps / 30 steps, the states at the
+    other segment starts recomputed), through tti_batch_grad_run (the shots'
+    gradients at once, one stream each, parameters shared). Its cost is set
+    against the batched forward of the same 16 shots (tti_batch_step,
+    autotuned) and against 16 plain forwards."""
+    import ttifd
+
+    K, S = args.grad_steps, args.grad_shots
+    gw = dict(GRAD_WORKLOAD)
+    true, start = grad_models()
+    cfg = dict(gw, variant="coordinate_rotation", nt=K)
+    wav = synthetic.ricker(K, cfg["dt"], cfg["fpeak"])[None, :]
+    gx = np.arange(gw["nx"], dtype=np.int32)
+    shots = [int(round((i + 0.5) * gw["nx"] / S)) for i in range(S)]
+    # observed traces: the true model's, all shots in one batch
+    with ttifd.Batch([cfg], [0] * S, device=local_rank) as b:
+        b.upload_model(0, *synthetic.padded(true, gw["ealThick"]))
+        for i, sx in enumerate(shots):
+            b.instances[i].set_source([sx], [2], wav)
+            for k in (0, 1):
+                b.instances[i].set_receivers(k, gx, 5)
+        b.run()
+        dobs = [[b.instances[i].fetch_traces(k) for k in (0, 1)] for i in range(S)]
+    seg = -(-K // 30)
+    with ttifd.Batch([cfg], [0] * S, device=local_rank) as b:
+        b.upload_model(0, *synthetic.padded(start, gw["ealThick"]))
+        for i, sx in enumerate(shots):
+            inst = b.instances[i]
+            inst.set_source([sx], [2], wav)
+            for k in (0, 1):
+                inst.set_receivers(k, gx, 5)
+                inst.grad_set_observed(k, dobs[i][k])
+        cells = b.instances[0].Nz * b.instances[0].Nx
+        tuned = b.autotune(min(20, K))
+        b.reset()
+        b.step(K)
+        fwd_ms = b.elapsed_ms
+        b.grad_run(29, seg)  # warm-up: allocations, kernel attributes
+        with ClockSampler(local_rank) as clk:
+            Js = b.grad_run(29, seg)
+            grad_ms = b.elapsed_ms
+        used = device_memory_in_use(local_rank)
+    with ttifd.Modeling(device=local_rank, **cfg) as h:  # one plain shot, for the sequential baseline
+        h.upload_model(*synthetic.padded(start, gw["ealThick"]))
+        h.set_source([shots[0]], [2], wav)
+        h.reset()
+        h.step(K)
+        plain_ms = h.elapsed_ms
+    return {"workload": f"adjoint-state gradient, coordinate_rotation, {S} surface shots on the layered 600x1200 "
+                        f"model, blurred start model, {K} steps, 30 checkpoints (29 slots + a kept segment of "
+                        f"{seg} steps)",
+            "shots": S, "steps": K, "checkpoints": 30, "gradient_ms": grad_ms,
+            "batched_forward_ms": fwd_ms, "cost_vs_batched_forward": grad_ms / fwd_ms,
+            "plain_forward_ms_x_shots": plain_ms * S, "cost_vs_plain_forwards": grad_ms / (plain_ms * S),
+            "value": S * cells * K / (grad_ms / 1e3) / 1e9, "unit": "Gcell/s (forward cell-updates of all shots "
+                                                                   "per second of gradient)",
+            "misfit_sum": float(sum(Js)), "device_memory_in_use_GB": used, "forward_schedule": tuned,
+            "clocks": clk.summary()}
+
+
+def run_gradient_full(args, local_rank):
+    """The batched gradient on the full model: `grad_full_shots` shots 120 m
+    apart around the surface centre of the 1126 x 7872 salt-like model
+    (ealThick 60, free surface, 7872 receivers at z=2, observed traces zero so
+    J = 1/2 |d|^2), `grad_full_steps` steps, checkpoints planned by
+    tti_grad_plan for an equal share per shot of 90 % of the free device
+    memory (less each shot's fixed buffers). The plan for the full nt = 5000
+    under the same budget is reported beside it."""
+    import ttifd
+
+    S, K = args.grad_full_shots, args.grad_full_steps
+    cfg = dict(WORKLOAD, variant="coordinate_rotation", nt=K, seistype=1, wsave=0, energy=0)
+    m = model()
+    pads = synthetic.padded(m, WORKLOAD["ealThick"])
+    wav = synthetic.ricker(K, cfg["dt"], cfg["fpeak"])[None, :]
+    nx = WORKLOAD["nx"]
+    gx = np.arange(nx, dtype=np.int32)
+    shots = [nx // 2 + 12 * (i - S // 2) for i in range(S)]
+    with ttifd.Batch([cfg], [0] * S, device=local_rank) as b:
+        b.upload_model(0, *pads)
+        for i, sx in enumerate(shots):
+            inst = b.instances[i]
+            inst.set_source([sx], [2], wav)
+            for k in (0, 1):
+                inst.set_receivers(k, gx, 2)
+                inst.grad_set_observed(k, np.zeros((nx, inst.nts), np.float32))
+        cells = b.instances[0].Nz * b.instances[0].Nx
+        tuned = b.autotune(min(20, K))
+        b.reset()
+        b.step(K)
+        fwd_ms = b.elapsed_ms
+        import torch
+
+        free0, total = torch.cuda.mem_get_info(local_rank)
+        n = b.instances[0].Nx * ((b.instances[0].Nz + 31) // 32 * 32)
+        fixed = 4.0 * n * 27 + 4.0 * nx * K * 6  # adjoint fields and sums, traces, observed, residuals
+        budget = max(0.0, (0.9 * free0) / S - fixed)
+        plan = b.instances[0].grad_plan(budget)
+        b.grad_run(plan["snapshots"], plan["keep_steps"])
+        grad_ms = b.elapsed_ms
+        used = device_memory_in_use(local_rank)
+    try:
+        with ttifd.Modeling(device=local_rank, **dict(cfg, nt=5000)) as h:
+            plan5000 = h.grad_plan(budget)
+    except ttifd.TTIError as e:
+        plan5000 = {"error": str(e)}
+    return {"workload": f"batched adjoint-state gradient, coordinate_rotation, {S} shots on the full 1126x7872 "
+                        f"salt-like model (padded 1256x8002), {K} steps, checkpoints planned for a "
+                        f"{budget / 1e9:.2f} GB share per shot",
+            "shots": S, "steps": K, "gradient_ms": grad_ms, "batched_forward_ms": fwd_ms,
+            "cost_vs_batched_forward": grad_ms / fwd_ms,
+            "value": S * cells * K / (grad_ms / 1e3) / 1e9, "per_shot_gcells": cells * K / (grad_ms / 1e3) / 1e9,
+            "unit": "Gcell/s", "plan": plan, "plan_nt5000_same_budget": plan5000,
+            "device_memory_in_use_GB": used, "device_memory_total_GB": total / 1e9, "forward_schedule": tuned}
 
 
 # ---------------------------------------------------------------- reference arm
@@ -553,6 +701,9 @@ def main():
     ap.add_argument("--grad-ncheck", type=int, default=1,
                     help="gradient segments (1: every state kept, as the 600x1200 case fits in HBM)")
     ap.add_argument("--no-grad", action="store_true", help="skip the gradient measurement")
+    ap.add_argument("--grad-shots", type=int, default=16)
+    ap.add_argument("--grad-full-shots", type=int, default=32)
+    ap.add_argument("--grad-full-steps", type=int, default=200)
     ap.add_argument("--no-variants", action="store_true",
                     help="skip the other two formulations on the same workload")
     args = ap.parse_args()
@@ -583,6 +734,8 @@ def main():
         line["batched_uneven"] = run_batched_uneven(args, local_rank)
     if not args.no_grad and world == 1:
         line["gradient"] = run_gradient(args, local_rank)
+        line["gradient_shots"] = run_gradient_shots(args, local_rank)
+        line["gradient_batched_full"] = run_gradient_full(args, local_rank)
     if rank == 0:
         if not args.no_cpu_baseline:
             try:

@@ -357,7 +357,7 @@ int upload_arrays(tti_handle *h, const float *const *src, float *const *dst, int
       const int nx = std::min(per, g.Nx - x0), b = c & 1;
       if (pending[b]) e = cudaEventSynchronize(h->pev[5 + b]);  // chunk b's previous DMA has drained
       if (e != cudaSuccess) break;
-      parallel_copy(pin[b], src[k] + (size_t)x0 * g.Nz, col * nx);
+      parallel_copy(pin[b], src[k] + (size_t)x0 * g.Nz, col * nx, 8);
       e = cudaMemcpy2DAsync(dst[k] + (size_t)x0 * g.ldz, dpitch, pin[b], col, col, nx, cudaMemcpyHostToDevice,
                             h->stream);
       if (e == cudaSuccess) e = cudaEventRecord(h->pev[5 + b], h->stream);

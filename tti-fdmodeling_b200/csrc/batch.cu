@@ -368,6 +368,7 @@ int tti_batch_upload_model(tti_batch *b, int m, const float *vp, const float *vs
   if (!b || m < 0 || m >= (int)b->models.size()) return berr(b, TTI_ERR_ARG, "model index out of range");
   const int rc = tti_upload_model(b->models[m], vp, vs, rho, epsilon, delta, theta);
   if (rc) return berr(b, rc, "model %d: %s", m, tti_last_error(b->models[m]));
+  sync_instances(b);  // the model's instances may now take observed traces
   return TTI_OK;
 }
 

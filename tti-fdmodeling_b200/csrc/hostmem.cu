@@ -55,10 +55,11 @@ std::vector<float *> g_pin_free;  // page-locked staging chunks not in use
 
 }  // namespace
 
-void parallel_copy(void *dst, const void *src, size_t bytes)
+void parallel_copy(void *dst, const void *src, size_t bytes, int max_threads)
 {
   const size_t hw = std::max(1u, std::thread::hardware_concurrency());
-  const int nth = (int)std::min<size_t>(std::min<size_t>(16, hw), std::max<size_t>(1, bytes >> 20));
+  const int nth =
+      (int)std::min<size_t>(std::min<size_t>((size_t)std::max(1, max_threads), hw), std::max<size_t>(1, bytes >> 20));
   char *d = static_cast<char *>(dst);
   const char *q = static_cast<const char *>(src);
   split(bytes, nth, [d, q](size_t b, size_t e) { memcpy(d + b, q + b, e - b); });

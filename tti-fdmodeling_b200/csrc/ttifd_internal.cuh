@@ -116,8 +116,10 @@ void pool_free(void *p, cudaStream_t st);
 // floats (NaN entries ignored, as fmaxf does) from several threads.
 void prefault(void *p, size_t bytes);
 float host_max(const float *a, size_t n, float init);
-// memcpy from up to 16 host threads (1 MiB or more each)
-void parallel_copy(void *dst, const void *src, size_t bytes);
+// memcpy from up to max_threads host threads (1 MiB or more each). Into fresh
+// pageable memory 16 threads help (they take the page faults in parallel);
+// from resident memory into page-locked chunks 8 measured faster than 16.
+void parallel_copy(void *dst, const void *src, size_t bytes, int max_threads = 16);
 // Page-locked staging chunks of PIN_CHUNK floats from a process-wide free list
 // (allocated on first need, kept until exit); null when none can be had.
 constexpr size_t PIN_CHUNK = (size_t)4 << 20;
