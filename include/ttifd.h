@@ -157,8 +157,7 @@ int tti_elapsed_ms(const tti_handle *h, float *ms);
 /* Measurement aid (no counterpart in the reference, which only prints the
  * loop wall time, coord:927-930): advances `nsteps` steps like tti_step with
  * CUDA events on the handle's stream around each phase and returns the total
- * device ms per phase: ms[0] the velocity update (with the fused step kernel:
- * the whole step kernel), ms[1] the stress update (0 with the fused kernel),
+ * device ms per phase: ms[0] the velocity update, ms[1] the stress update,
  * ms[2] everything else (sources, free surface, receivers, energy). */
 int tti_profile_steps(tti_handle *h, int nsteps, float ms[3]);
 /* Number of kernels this handle has launched since tti_create. */

@@ -65,8 +65,8 @@ def test_gpu_exact_rounding_mode(name, gpu_lib, monkeypatch):
 
 @pytest.mark.parametrize("name", ["coord_fs", "tensor_basic", "bond_thin_rim", "coord_stype4", "bond_stype7"])
 def test_gpu_one_thread_per_cell_path(name, gpu_lib, monkeypatch):
-    """The per-kernel path (used when the free-surface rows do not fit the
-    fused kernel's first band) against the same golden outputs."""
+    """The one-thread-per-cell path (TTIFD_KERNEL=naive, the cross-check of the
+    tiled kernels) against the same golden outputs."""
     import ttifd
 
     monkeypatch.setenv("TTIFD_KERNEL", "naive")
@@ -75,30 +75,3 @@ def test_gpu_one_thread_per_cell_path(name, gpu_lib, monkeypatch):
     _compare(name, got, helpers.golden_arrays(case), TRACE_RTOL, TRACE_PEAK)
 
 
-@pytest.mark.parametrize("name", ["coord_fs", "tensor_stype6", "bond_fs", "coord_multi_dxdz"])
-def test_gpu_fused_path(name, gpu_lib, monkeypatch):
-    """The single-kernel step against the golden outputs."""
-    import ttifd
-
-    monkeypatch.setenv("TTIFD_KERNEL", "fused")
-    case = helpers.load_golden(name)
-    got = helpers.run_backend(ttifd.Modeling, case)
-    _compare(name, got, helpers.golden_arrays(case), TRACE_RTOL, TRACE_PEAK)
-
-
-@pytest.mark.parametrize("seg", ["16", "23", "40"])
-def test_gpu_fused_segment_lengths(seg, gpu_lib, monkeypatch):
-    """Column-segment boundaries of the fused step must not change results:
-    fused traces at several segment lengths equal the per-kernel path's to
-    the last bit in the exact rounding mode."""
-    import ttifd
-
-    monkeypatch.setenv("TTIFD_EXACT", "1")
-    case = helpers.load_golden("coord_multi_dxdz")
-    monkeypatch.setenv("TTIFD_KERNEL", "naive")
-    ref = helpers.run_backend(ttifd.Modeling, case)
-    monkeypatch.setenv("TTIFD_KERNEL", "fused")
-    monkeypatch.setenv("TTIFD_SEG", seg)
-    got = helpers.run_backend(ttifd.Modeling, case)
-    for k, v in ref.items():
-        assert np.array_equal(np.asarray(got[k]).view(np.uint32), np.asarray(v).view(np.uint32)), k

@@ -73,7 +73,7 @@ constexpr int BZ = 32, BX = 8;
 struct AdjArgs {
   Grid g;
   Params p;
-  fused::Packed pk;  // packed parameters (null on the per-cell path)
+  packed::Packed pk;  // packed parameters (null on the per-cell path)
   float *lam[8];
   float *T[4];
   float *TV[6];
@@ -544,7 +544,7 @@ __global__ void __launch_bounds__(BZ *BX) k_adj_velocity_stencil(AdjArgs a)
 struct alignas(64) AdjTile {
   CUtensorMap map[6];  // velocity pass: T0..T3; stress-node pass: TV0..TV5
   AdjArgs a;
-  fused::Packed pk;
+  packed::Packed pk;
   int z_base;  // first tile row (multiple of 4)
   int *err;    // bit 4: a TMA wait timed out
 };
@@ -903,7 +903,6 @@ int gerr(tti_handle *h, int code, const char *msg) { return handle_error(h, code
 
 int grad_check(tti_handle *h)
 {
-  if (h->use_fused) return gerr(h, TTI_ERR_STATE, "the gradient runs on the tiled or per-cell kernels");
   if (!h->have_model || !h->m_eps) return gerr(h, TTI_ERR_STATE, "model not uploaded");
   return TTI_OK;
 }
@@ -953,7 +952,7 @@ AdjArgs adj_args(tti_handle *h, int slot)
   a.hx = 0.5f * h->invdx;
   a.hz = 0.5f * h->invdz;
   a.dt = h->cfg.dt;
-  a.pk = fused::Packed{h->pk_cf, h->pk_vsc, h->pk_sc, h->pk_c4};
+  a.pk = packed::Packed{h->pk_cf, h->pk_vsc, h->pk_sc, h->pk_c4};
   a.undamped_ok = h->use_tiled && h->undamped_ok;
   a.und_z0 = h->cfg.freesurface ? 0 : h->g.E;
   a.z_lo = h->cfg.freesurface ? std::max(NH, h->g.izStart - NH) : h->g.izStart;
@@ -1168,7 +1167,7 @@ int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
     AdjTile at;
     memset(&at, 0, sizeof at);
     at.a = a;
-    at.pk = fused::Packed{h->pk_cf, h->pk_vsc, h->pk_sc, h->pk_c4};
+    at.pk = packed::Packed{h->pk_cf, h->pk_vsc, h->pk_sc, h->pk_c4};
     at.err = h->d_flag;
     for (int k = 0; k < 4; ++k) at.map[k] = s->maps[k];
     if (c.variant == TTI_COORDINATE)

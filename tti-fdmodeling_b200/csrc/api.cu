@@ -130,54 +130,6 @@ int launch_one_step(tti_handle *h, const SourceTables &tab, cudaEvent_t *ev = nu
   StepArgs a = step_args(h);
   SourceSet s{h->nsrc, h->d_sx, h->d_sz, h->d_src, c.nt};
   const bool vsrc = s.n > 0 && c.stype >= 2, ssrc = s.n > 0 && c.stype == 1;
-  if (h->use_fused && h->nsrc <= fused::MAXSRC) {
-    fused::FusedArgs fa;
-    fa.g = h->g;
-    fa.old = a.f;
-    fa.nw = Fields{h->fld2[0], h->fld2[1], h->fld2[2], h->fld2[3], h->fld2[4], h->fld2[5], h->fld2[6], h->fld2[7]};
-    fa.p = a.p;
-    fa.pk = fused::Packed{h->pk_cf, h->pk_vsc, h->pk_sc, h->pk_c4};
-    fa.invdx = h->invdx;
-    fa.invdz = h->invdz;
-    fa.dt = c.dt;
-    fa.seg = h->seg;
-    fa.bz = h->bz;
-    fa.stype = c.stype;
-    fa.src = s;
-    fa.tab = tab;
-    fa.it = it;
-    fa.freesurface = c.freesurface;
-    fa.undamped_ok = h->undamped_ok;
-    fa.err = h->d_flag;
-    if (ev) CK(h, cudaEventRecord(ev[0], h->stream));
-    CK(h, fused::launch_fused(fa, c.variant, h->exact, h->stream));
-    if (ev) {
-      CK(h, cudaEventRecord(ev[1], h->stream));
-      CK(h, cudaEventRecord(ev[2], h->stream));
-      CK(h, cudaEventRecord(ev[3], h->stream));
-    }
-    h->launches++;
-    std::swap(h->fld, h->fld2);
-    if (c.seistype > 0 && it % c.mt == 0 && h->nrec[0] + h->nrec[1] + h->nrec[2] > 0) {
-      ReceiverSet r;
-      for (int k = 0; k < 3; ++k) {
-        r.n[k] = h->nrec[k];
-        r.x[k] = h->d_rx[k];
-        r.z[k] = h->d_rz[k];
-        r.rec[k] = h->d_rec[k];
-      }
-      launch_receivers(step_args(h), r, c.seistype, it / c.mt, h->d_flag, h->stream);
-      h->launches++;
-    }
-    if (c.energy == 1) {
-      launch_energy(step_args(h), c.nz, c.nx, h->d_energy + 2 * (size_t)it, h->stream);
-      h->launches++;
-    }
-    if (ev) CK(h, cudaEventRecord(ev[4], h->stream));
-    CK(h, cudaGetLastError());
-    h->step_index++;
-    return TTI_OK;
-  }
   tiled::HalfArgs ha{};
   // What the gradient keeps of this step (keep_fields). Tiled kernels: the
   // stress kernel writes the strain rates vxx vxz vzx vzz (keep[0..3]) and for
@@ -191,7 +143,7 @@ int launch_one_step(tti_handle *h, const SourceTables &tab, cudaEvent_t *ev = nu
     ha.g = h->g;
     ha.f = a.f;
     ha.p = a.p;
-    ha.pk = fused::Packed{h->pk_cf, h->pk_vsc, h->pk_sc, h->pk_c4};
+    ha.pk = packed::Packed{h->pk_cf, h->pk_vsc, h->pk_sc, h->pk_c4};
     ha.invdx = h->invdx;
     ha.invdz = h->invdz;
     ha.dt = c.dt;
@@ -316,7 +268,6 @@ int check_flag(tti_handle *h)
   int flag = 0;
   CK(h, cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
-  if (flag & 2) return set_err(h, TTI_ERR_CUDA, "a shared-memory copy wait timed out in the fused step kernel");
   if (flag & 4) return set_err(h, TTI_ERR_CUDA, "a TMA tile wait timed out in a tiled half-step kernel");
   if (flag) return set_err(h, TTI_ERR_NONFINITE, "non-finite value recorded at a receiver (unstable run?)");
   return TTI_OK;
@@ -393,7 +344,6 @@ StepArgs handle_step_args(const tti_handle *h) { return step_args(h); }
 void handle_source_tables(const tti_handle *h, SourceTables *t) { source_tables(h, t); }
 int handle_step(tti_handle *h, const SourceTables &tab, float *const *keep)
 {
-  if (keep && h->use_fused) return set_err(h, TTI_ERR_STATE, "the fused step has no hook between its half-steps");
   return launch_one_step(h, tab, nullptr, keep);
 }
 int handle_check_flag(tti_handle *h) { return check_flag(h); }
@@ -471,20 +421,14 @@ int create_handle(tti_handle **out, const tti_config *cfg, int device, const tti
     return fail(TTI_ERR_CUDA);
   }
   {
+    // default: the tiled half-step kernels; TTIFD_KERNEL=naive selects the
+    // one-thread-per-cell kernels (the cross-check path)
     const char *kern = getenv("TTIFD_KERNEL");
     const bool naive = kern && strcmp(kern, "naive") == 0;
-    const bool fused_req = kern && strcmp(kern, "fused") == 0;
-    const int bands = (g.Nz + fused::BZ - 1) / fused::BZ;
-    h->bz = (g.Nz + bands - 1) / bands;
-    // the fused step needs the free-surface rows E-5 .. E+5 inside the first band
-    // default: the tiled half-step kernels; `fused` selects the single-kernel step
-    h->use_fused = !force_tiled && fused_req && !(cfg->freesurface == 1 && g.E + NH >= h->bz);
-    h->use_tiled = force_tiled || (!naive && !h->use_fused);
+    h->use_tiled = force_tiled || !naive;
   }
-  for (int f = 0; f < nfields(cfg->variant); ++f) {
+  for (int f = 0; f < nfields(cfg->variant); ++f)
     if ((rc = alloc(&h->fld[f]))) return fail(rc);
-    if (h->use_fused && (rc = alloc(&h->fld2[f]))) return fail(rc);
-  }
   if (h->use_tiled) {
     void *mem = nullptr;
     if (posix_memalign(&mem, 64, 5 * sizeof(CUtensorMap)) != 0) {
@@ -506,7 +450,7 @@ int create_handle(tti_handle **out, const tti_config *cfg, int device, const tti
     h->pk_vsc = share->pk_vsc;
     h->pk_sc = share->pk_sc;
     h->pk_c4 = share->pk_c4;
-  } else if (h->use_fused || h->use_tiled) {
+  } else if (h->use_tiled) {
     auto palloc = [&](void *p, size_t bytes) {
       return pool_alloc(static_cast<void **>(p), bytes, h->stream) == cudaSuccess;
     };
@@ -517,22 +461,6 @@ int create_handle(tti_handle **out, const tti_config *cfg, int device, const tti
       set_err(h, TTI_ERR_NOMEM, "device allocation of the packed parameters failed");
       return fail(TTI_ERR_NOMEM);
     }
-    // columns per CTA: one wave of CTAs over the SMs at the kernel's occupancy
-    int sms = 148, dev = device;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    size_t smem_per_sm = 0;
-    int v = 0;
-    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-    smem_per_sm = (size_t)v;
-    const size_t per_cta = fused::smem_bytes(cfg->variant) + 1024;
-    int occ = (int)std::max<size_t>(1, std::min<size_t>(3, smem_per_sm / per_cta));
-    const char *occenv = getenv("TTIFD_CTAS_PER_SM");
-    if (occenv && atoi(occenv) > 0) occ = atoi(occenv);
-    const int bands = (g.Nz + h->bz - 1) / h->bz;
-    int nseg = std::max(1, sms * occ / bands);
-    h->seg = std::max(16, (g.Nx + nseg - 1) / nseg);
-    const char *segenv = getenv("TTIFD_SEG");
-    if (segenv && atoi(segenv) > 0) h->seg = atoi(segenv);
   }
   for (int p = 0; p < TTI_P_COUNT && !share; ++p)
     if (param_used(cfg->variant, p) && (rc = alloc(&h->par[p]))) return fail(rc);
@@ -563,7 +491,6 @@ int tti_destroy(tti_handle *h)
   if (h->stream) cudaStreamSynchronize(h->stream);
   cudaStream_t fs = h->stream;  // pool blocks are released in stream order
   for (auto &p : h->fld) pool_free(p, fs);
-  for (auto &p : h->fld2) pool_free(p, fs);
   if (!h->owner) {
     for (auto &p : h->par) pool_free(p, fs);
     pool_free(h->pk_cf, fs);
@@ -695,20 +622,20 @@ int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const floa
   }
   pool_free(raw_block, h->stream);
   pool_free(d_w, h->stream);
-  if (rc == TTI_OK && (h->use_fused || h->use_tiled)) {
-    fused::launch_pack(g, step_args(h).p, fused::Packed{h->pk_cf, h->pk_vsc, h->pk_sc, h->pk_c4}, c.variant,
+  if (rc == TTI_OK && h->use_tiled) {
+    packed::launch_pack(g, step_args(h).p, packed::Packed{h->pk_cf, h->pk_vsc, h->pk_sc, h->pk_c4}, c.variant,
                        h->stream);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) rc = set_err(h, TTI_ERR_CUDA, "packing parameters: %s", cudaGetErrorString(e));
   }
-  if (rc == TTI_OK && (h->use_fused || h->use_tiled)) {
-    // the fused step skips coef1/coef2 loads where they are exactly 1 and dt;
-    // verify that on the device instead of assuming the MEAL rim geometry
+  if (rc == TTI_OK && h->use_tiled) {
+    // the tiled kernels skip coef1/coef2 loads where they are exactly 1 and
+    // dt; verify that on the device instead of assuming the MEAL rim geometry
     int *cnt = nullptr;
     int bad = -1;
     if (pool_alloc(reinterpret_cast<void **>(&cnt), sizeof(int), h->stream) == cudaSuccess) {
       cudaMemsetAsync(cnt, 0, sizeof(int), h->stream);
-      fused::launch_check_undamped(g, h->par[TTI_P_COEF1], h->par[TTI_P_COEF2], c.dt, c.freesurface ? 0 : g.E, cnt,
+      packed::launch_check_undamped(g, h->par[TTI_P_COEF1], h->par[TTI_P_COEF2], c.dt, c.freesurface ? 0 : g.E, cnt,
                                    h->stream);
       cudaMemcpyAsync(&bad, cnt, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
       pool_free(cnt, h->stream);
@@ -800,7 +727,7 @@ int tti_set_receivers(tti_handle *h, int kind, int ntrace, const int *posx, cons
   CK(h, cudaMemcpyAsync(h->d_rz[kind], z.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice, h->stream));
   CK(h, cudaMemsetAsync(h->d_rec[kind], 0, sizeof(float) * (size_t)ntrace * h->nts, h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
-  // receivers grouped by padded-grid column for the fused step
+  // receivers grouped by padded-grid column for the column pass (k_post)
   {
     const int Nx = h->g.Nx;
     std::vector<int> order(ntrace), colptr(Nx + 1, 0), zs(ntrace), ids(ntrace);
@@ -833,8 +760,6 @@ int tti_reset(tti_handle *h)
   if (!h) return TTI_ERR_ARG;
   CK(h, cudaSetDevice(h->device));
   for (auto p : h->fld)
-    if (p) CK(h, cudaMemsetAsync(p, 0, h->g.n * sizeof(float), h->stream));
-  for (auto p : h->fld2)
     if (p) CK(h, cudaMemsetAsync(p, 0, h->g.n * sizeof(float), h->stream));
   for (int k = 0; k < 3; ++k)
     if (h->d_rec[k]) CK(h, cudaMemsetAsync(h->d_rec[k], 0, sizeof(float) * (size_t)h->nrec[k] * h->nts, h->stream));
@@ -905,14 +830,9 @@ int tti_profile_steps(tti_handle *h, int nsteps, float ms[3])
     CK(h, cudaEventElapsedTime(&t12, h->pev[1], h->pev[2]));
     CK(h, cudaEventElapsedTime(&t23, h->pev[2], h->pev[3]));
     CK(h, cudaEventElapsedTime(&t34, h->pev[3], h->pev[4]));
-    if (h->use_fused) {  // one step kernel: ev[1..3] are recorded back to back
-      ms[0] += t01;
-      ms[2] += t12 + t23 + t34;
-    } else {
-      ms[0] += t01;
-      ms[1] += t23;
-      ms[2] += t12 + t34;
-    }
+    ms[0] += t01;
+    ms[1] += t23;
+    ms[2] += t12 + t34;
   }
   return check_flag(h);
 }

@@ -121,7 +121,7 @@ int build_tables(tti_batch *b)
     ha.g = h->g;
     ha.f = a.f;
     ha.p = a.p;
-    ha.pk = fused::Packed{h->pk_cf, h->pk_vsc, h->pk_sc, h->pk_c4};
+    ha.pk = packed::Packed{h->pk_cf, h->pk_vsc, h->pk_sc, h->pk_c4};
     ha.invdx = h->invdx;
     ha.invdz = h->invdz;
     ha.dt = c.dt;

@@ -4,7 +4,7 @@
 
 #include <cuda.h>
 
-#include "fused.cuh"
+#include "pack.cuh"
 
 namespace ttifd {
 namespace tiled {
@@ -22,7 +22,7 @@ struct alignas(64) HalfArgs {
   Grid g;
   Fields f;
   Params p;
-  fused::Packed pk;
+  packed::Packed pk;
   float invdx, invdz, dt;
   int z_base;  // first tile row (multiple of 4, <= izStart)
   int x_base;  // first tile column (= 5)

@@ -141,20 +141,16 @@ struct tti_handle {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   ttifd::Grid g{};
-  float *fld[8] = {};   // current wavefields
-  float *fld2[8] = {};  // second set: the fused step reads fld and writes fld2, then swaps
-  bool use_fused = false;
+  float *fld[8] = {};      // wavefields, updated in place
   bool use_tiled = false;  // tiled half-step kernels with TMA halo tiles (in place)
   const tti_handle *owner = nullptr;  // set when the parameter arrays belong to another handle (batched shots)
   float *m_eps = nullptr, *m_delta = nullptr;  // epsilon, delta as uploaded (gradient chain rule)
   float *m_theta = nullptr;                    // theta (degrees) as uploaded (Bond gradient chain rule)
   struct GradState *grad = nullptr;            // adjoint-state gradient buffers (adjoint.cu)
   void *tmaps = nullptr;   // host copy of the 5 tensor maps (vx vz sxx szz sxz), 64-byte aligned
-  int seg = 0;          // columns per CTA of the fused step
-  int bz = 0;           // rows per band of the fused step
   int undamped_ok = 0;  // coef1 == 1, coef2 == dt outside the absorbing rims (checked at upload)
   int *d_rcol[3] = {}, *d_rzs[3] = {}, *d_rid[3] = {};  // receivers grouped by column
-  float2 *pk_cf = nullptr, *pk_vsc = nullptr, *pk_sc = nullptr;  // packed parameters (fused step)
+  float2 *pk_cf = nullptr, *pk_vsc = nullptr, *pk_sc = nullptr;  // packed parameters (pack.cuh)
   float4 *pk_c4 = nullptr;
   float *par[TTI_P_COUNT] = {};
   float invdx = 0, invdz = 0, alpha_src = 0;
