@@ -280,10 +280,12 @@ int tti_batch_upload_model(tti_batch *b, int m, const float *vp, const float *vs
  * 1: shot after shot), and the loop replays a CUDA graph of `graph_steps`
  * steps (0: no graph). */
 int tti_batch_set_order(tti_batch *b, int group, int graph_steps);
-/* In-tile schedule of the half-step kernels: 0 = row (one row of cells per
- * thread, every stencil tap a shared-memory load), 1 = walk (each thread walks
- * a diagonal, then an anti-diagonal, of the tile with the stencil taps in a
- * sliding register window). Both give the same bits. */
+/* Schedule of the half-step kernels. Bit 0, the in-tile schedule: 0 = row
+ * (one row of cells per thread, every stencil tap a shared-memory load),
+ * 1 = walk (each thread walks a diagonal, then an anti-diagonal, of the tile
+ * with the stencil taps in a sliding register window). Bit 1: 0 = one CTA per
+ * work item, 1 = persistent (one resident wave of CTAs walks the work table).
+ * All four give the same bits. */
 int tti_batch_set_schedule(tti_batch *b, int tile_schedule);
 /* The schedule in use (any output may be NULL). */
 int tti_batch_get_schedule(const tti_batch *b, int *group, int *graph_steps, int *tile_schedule);

@@ -42,6 +42,7 @@ struct tti_batch {
   int *d_step = nullptr;
   int group = 0;  // work-table order: shots of a model interleaved tile by tile in groups of `group` (0: all)
   bool walk = false;  // in-tile schedule of the half-step kernels: walk (true) or row
+  bool persistent = false;  // one resident wave of CTAs walks the work table (else one CTA per item)
   int graph_steps = 20;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -209,15 +210,20 @@ int build_tables(tti_batch *b)
   return TTI_OK;
 }
 
+// Launch description of a half-step (`vel`: the velocity tables, else the stress ones).
+tiled::BatchLaunch batch_launch(const tti_batch *b, bool vel)
+{
+  return tiled::BatchLaunch{vel ? b->d_vel : b->d_str, b->d_work, b->nwork, b->d_step, b->variant, b->exact,
+                            b->square, b->walk, b->persistent};
+}
+
 // The launches of one time step (all instances).
 int launch_step(tti_batch *b)
 {
   const int n = (int)b->inst.size();
-  BCK(b, tiled::launch_velocity_batch(b->d_vel, b->d_work, b->nwork, b->d_step, b->variant, b->exact, b->square,
-                                      b->walk, b->stream));
+  BCK(b, tiled::launch_velocity_batch(batch_launch(b, true), b->stream));
   if (b->any_vsrc) launch_sources_batch(b->d_src, n, b->d_step, b->stream);
-  BCK(b, tiled::launch_stress_batch(b->d_str, b->d_work, b->nwork, b->d_step, b->variant, b->exact, b->square,
-                                    b->walk, b->stream));
+  BCK(b, tiled::launch_stress_batch(batch_launch(b, false), b->stream));
   launch_post_batch(b->d_post, n, b->max_Nx, b->d_step, b->stream);
   launch_advance(b->d_step, b->stream);
   BCK(b, cudaGetLastError());
@@ -229,7 +235,7 @@ int launches_per_step(const tti_batch *b) { return 4 + (b->any_vsrc ? 1 : 0); }
 int ensure_graph(tti_batch *b)
 {
   if (b->exec || b->graph_steps <= 0) return TTI_OK;
-  BCK(b, tiled::prepare_batch(b->variant, b->exact, b->square, b->walk));
+  BCK(b, tiled::prepare_batch(batch_launch(b, true)));
   BCK(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
   int rc = TTI_OK;
   for (int k = 0; k < b->graph_steps && rc == TTI_OK; ++k) rc = launch_step(b);
@@ -388,13 +394,15 @@ int tti_batch_set_order(tti_batch *b, int group, int graph_steps)
 
 int tti_batch_set_schedule(tti_batch *b, int tile_schedule)
 {
-  if (!b || tile_schedule < 0 || tile_schedule > 1) return berr(b, TTI_ERR_ARG, "tile schedule must be 0 or 1");
-  if ((tile_schedule == 1) != b->walk) {  // the captured launches select the kernels
+  if (!b || tile_schedule < 0 || tile_schedule > 3) return berr(b, TTI_ERR_ARG, "tile schedule must be 0..3");
+  const bool walk = tile_schedule & 1, persistent = tile_schedule & 2;
+  if (walk != b->walk || persistent != b->persistent) {  // the captured launches select the kernels
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     b->exec = nullptr;
     b->graph = nullptr;
-    b->walk = tile_schedule == 1;
+    b->walk = walk;
+    b->persistent = persistent;
   }
   return TTI_OK;
 }
@@ -404,7 +412,7 @@ int tti_batch_get_schedule(const tti_batch *b, int *group, int *graph_steps, int
   if (!b) return TTI_ERR_ARG;
   if (group) *group = b->group;
   if (graph_steps) *graph_steps = b->graph_steps;
-  if (tile_schedule) *tile_schedule = b->walk ? 1 : 0;
+  if (tile_schedule) *tile_schedule = (b->walk ? 1 : 0) | (b->persistent ? 2 : 0);
   return TTI_OK;
 }
 
@@ -468,10 +476,10 @@ int tti_batch_autotune(tti_batch *b, int nsteps, int *group, int *graph_steps, f
   for (size_t m = 0; m < b->models.size(); ++m)
     ninst_max = std::max(ninst_max, (int)std::count(b->model_of.begin(), b->model_of.end(), (int)m));
   std::vector<int> groups = {0};
-  for (int g : {1, 2, 4, 8, 16})
+  for (int g : {1, 4, 16})
     if (g < ninst_max) groups.push_back(g);
   const int graphs[] = {0, 20};
-  const int NS = 2;  // tile schedules: row, walk
+  const int NS = 4;  // tile schedules: row, walk, each with one CTA per tile or a persistent wave
   // Each candidate is timed twice, in two rounds over all of them, and keeps
   // its faster time; a graph candidate is timed over at least one replay of
   // its graph (the step loop only replays it when that many steps remain).

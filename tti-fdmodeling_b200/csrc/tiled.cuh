@@ -62,17 +62,22 @@ bool encode_map(CUtensorMap *map, const Grid &g, float *field);
 dim3 grid(const Grid &g, int *z_base);
 cudaError_t launch_velocity(const HalfArgs &a, int variant, bool exact, cudaStream_t st);
 cudaError_t launch_stress(const HalfArgs &a, int variant, bool exact, cudaStream_t st);
-// Batched: one launch over all instances' tiles. `inst` (device) holds each
-// instance's arguments (z_base set), `work` (device) the CTA -> (instance, tile)
-// table; `step` (device) is the shared step counter.
-// `square`: every instance has square (folded) coefficients (set_square).
-// `walk`: the walk schedule of the tile instead of the row schedule.
-cudaError_t launch_velocity_batch(const HalfArgs *inst, const Work *work, int nwork, const int *step, int variant,
-                                  bool exact, bool square, bool walk, cudaStream_t st);
-cudaError_t launch_stress_batch(const HalfArgs *inst, const Work *work, int nwork, const int *step, int variant,
-                                bool exact, bool square, bool walk, cudaStream_t st);
+// Batched: one launch over all instances' tiles (each instance's arguments
+// with z_base set), driven by the work table.
+struct BatchLaunch {
+  const HalfArgs *inst;  // device: each instance's arguments (velocity or stress maps)
+  const Work *work;      // device: the CTA -> (instance, tile) table
+  int nwork;
+  const int *step;       // device: the shared step counter
+  int variant;
+  bool exact, square;    // square: every instance has folded coefficients (set_square)
+  bool walk;             // the walk schedule of the tile instead of the row schedule
+  bool persistent;       // one resident wave of CTAs walks the table (else one CTA per item)
+};
+cudaError_t launch_velocity_batch(const BatchLaunch &l, cudaStream_t st);
+cudaError_t launch_stress_batch(const BatchLaunch &l, cudaStream_t st);
 // Sets the kernels' shared-memory attributes (call before a stream capture).
-cudaError_t prepare_batch(int variant, bool exact, bool square, bool walk);
+cudaError_t prepare_batch(BatchLaunch l);
 
 // Device side of the TMA halo tiles, shared by the tiled forward and adjoint kernels.
 namespace tma {

@@ -620,28 +620,43 @@ __global__ void __launch_bounds__(NT, K ? 3 : 4) k_stress_tiled(const __grid_con
   stress_tile<V, X, Q, K>(a, a.map, sm, blockIdx.x, blockIdx.y);
 }
 
+// Work items blockIdx.x, blockIdx.x + gridDim.x, ... of the table: one item
+// per CTA when the grid covers the table, several when a persistent grid of
+// one resident wave walks it. The tile's shared memory (boxes, barrier,
+// staged arguments) is reused by the next item only after every thread of
+// the CTA is done with it.
+template <typename F>
+__device__ __forceinline__ void for_work(const HalfArgs *inst, const Work *work, int nwork, const int *step, F f)
+{
+  for (int i = blockIdx.x; i < nwork; i += gridDim.x) {
+    const Work w = work[i];
+    const HalfArgs *src = inst + w.inst;
+    if (*step >= src->nt) continue;  // uniform over the CTA
+    f(src, w);
+    __syncthreads();
+  }
+}
+
 template <int V, bool X, bool Q>
 __global__ void __launch_bounds__(NT, 4) k_velocity_batch(const HalfArgs *__restrict__ inst,
-                                                          const Work *__restrict__ work, const int *step)
+                                                          const Work *__restrict__ work, int nwork, const int *step)
 {
   extern __shared__ __align__(128) float sm[];
-  const Work w = work[blockIdx.x];
-  const HalfArgs *src = inst + w.inst;
-  if (*step >= src->nt) return;
-  const HalfArgs *a = stage_args(src, sm);
-  velocity_tile<V, X, Q>(*a, src->map, sm, w.tile % a->tiles_z, w.tile / a->tiles_z);
+  for_work(inst, work, nwork, step, [&](const HalfArgs *src, const Work &w) {
+    const HalfArgs *a = stage_args(src, sm);
+    velocity_tile<V, X, Q>(*a, src->map, sm, w.tile % a->tiles_z, w.tile / a->tiles_z);
+  });
 }
 
 template <int V, bool X, bool Q>
 __global__ void __launch_bounds__(NT, 4) k_stress_batch(const HalfArgs *__restrict__ inst,
-                                                        const Work *__restrict__ work, const int *step)
+                                                        const Work *__restrict__ work, int nwork, const int *step)
 {
   extern __shared__ __align__(128) float sm[];
-  const Work w = work[blockIdx.x];
-  const HalfArgs *src = inst + w.inst;
-  if (*step >= src->nt) return;
-  const HalfArgs *a = stage_args(src, sm);
-  stress_tile<V, X, Q>(*a, src->map, sm, w.tile % a->tiles_z, w.tile / a->tiles_z);
+  for_work(inst, work, nwork, step, [&](const HalfArgs *src, const Work &w) {
+    const HalfArgs *a = stage_args(src, sm);
+    stress_tile<V, X, Q>(*a, src->map, sm, w.tile % a->tiles_z, w.tile / a->tiles_z);
+  });
 }
 
 // walk schedule of the batched launches: the arguments follow the walk's layout
@@ -653,26 +668,26 @@ constexpr size_t walk_args_off()
 
 template <int V, bool X, bool Q>
 __global__ void __launch_bounds__(walk::NTW, 3) k_velocity_walk_batch(const HalfArgs *__restrict__ inst,
-                                                                      const Work *__restrict__ work, const int *step)
+                                                                      const Work *__restrict__ work, int nwork,
+                                                                      const int *step)
 {
   extern __shared__ __align__(128) float sm[];
-  const Work w = work[blockIdx.x];
-  const HalfArgs *src = inst + w.inst;
-  if (*step >= src->nt) return;
-  const HalfArgs *a = stage_args(src, sm, walk_args_off<3>());
-  walk::velocity_walk<V, X, Q, false>(*a, src->map, sm, w.tile % a->tiles_z, w.tile / a->tiles_z);
+  for_work(inst, work, nwork, step, [&](const HalfArgs *src, const Work &w) {
+    const HalfArgs *a = stage_args(src, sm, walk_args_off<3>());
+    walk::velocity_walk<V, X, Q, false>(*a, src->map, sm, w.tile % a->tiles_z, w.tile / a->tiles_z);
+  });
 }
 
 template <int V, bool X, bool Q>
 __global__ void __launch_bounds__(walk::NTW, 4) k_stress_walk_batch(const HalfArgs *__restrict__ inst,
-                                                                    const Work *__restrict__ work, const int *step)
+                                                                    const Work *__restrict__ work, int nwork,
+                                                                    const int *step)
 {
   extern __shared__ __align__(128) float sm[];
-  const Work w = work[blockIdx.x];
-  const HalfArgs *src = inst + w.inst;
-  if (*step >= src->nt) return;
-  const HalfArgs *a = stage_args(src, sm, walk_args_off<2>());
-  walk::stress_walk<V, X, Q, false>(*a, src->map, sm, w.tile % a->tiles_z, w.tile / a->tiles_z);
+  for_work(inst, work, nwork, step, [&](const HalfArgs *src, const Work &w) {
+    const HalfArgs *a = stage_args(src, sm, walk_args_off<2>());
+    walk::stress_walk<V, X, Q, false>(*a, src->map, sm, w.tile % a->tiles_z, w.tile / a->tiles_z);
+  });
 }
 
 template <typename K>
@@ -807,79 +822,76 @@ cudaError_t launch_stress(const HalfArgs &a, int variant, bool exact, cudaStream
 
 constexpr size_t BATCH_SMEM = (size_t)ARGS_OFF * sizeof(float) + ARGS_BYTES;
 
+// One CTA per work item, or (persistent) one resident wave of CTAs that walks
+// the table: the SM count times the kernel's CTAs per SM at its shared memory.
 template <typename K>
-cudaError_t launch_batch_k(K kernel, const HalfArgs *inst, const Work *work, int nwork, const int *step,
-                           cudaStream_t st, size_t smem = BATCH_SMEM, int threads = NT)
+cudaError_t launch_batch_k(K kernel, const BatchLaunch &l, cudaStream_t st, size_t smem = BATCH_SMEM,
+                           int threads = NT)
 {
   cudaError_t e = set_attr(kernel, smem);
-  if (e != cudaSuccess || nwork == 0) return e;
-  kernel<<<nwork, threads, smem, st>>>(inst, work, step);
+  if (e != cudaSuccess || l.nwork == 0) return e;
+  int grid = l.nwork;
+  if (l.persistent) {
+    int dev = 0, sms = 0, per_sm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem)) != cudaSuccess) return e;
+    grid = std::min(l.nwork, std::max(1, per_sm) * sms);
+  }
+  kernel<<<grid, threads, smem, st>>>(l.inst, l.work, l.nwork, l.step);
   return cudaGetLastError();
 }
 
 template <int NF, typename K>
-cudaError_t launch_walk_batch_k(K kernel, const HalfArgs *inst, const Work *work, int nwork, const int *step,
-                                cudaStream_t st)
+cudaError_t launch_walk_batch_k(K kernel, const BatchLaunch &l, cudaStream_t st)
 {
-  return launch_batch_k(kernel, inst, work, nwork, step, st, walk_args_off<NF>() * sizeof(float) + ARGS_BYTES,
-                        walk::NTW);
+  return launch_batch_k(kernel, l, st, walk_args_off<NF>() * sizeof(float) + ARGS_BYTES, walk::NTW);
 }
 
 template <bool X, bool Q>
-cudaError_t velocity_batch_x(const HalfArgs *inst, const Work *work, int nwork, const int *step, int variant,
-                             bool walk, cudaStream_t st)
+cudaError_t velocity_batch_x(const BatchLaunch &l, cudaStream_t st)
 {
-  if (walk) {
-    if (variant == TTI_COORDINATE)
-      return launch_walk_batch_k<3>(k_velocity_walk_batch<TTI_COORDINATE, X, Q>, inst, work, nwork, step, st);
-    if (variant == TTI_TENSOR)
-      return launch_walk_batch_k<3>(k_velocity_walk_batch<TTI_TENSOR, X, Q>, inst, work, nwork, step, st);
-    return launch_walk_batch_k<3>(k_velocity_walk_batch<TTI_BOND, X, Q>, inst, work, nwork, step, st);
+  if (l.walk) {
+    if (l.variant == TTI_COORDINATE) return launch_walk_batch_k<3>(k_velocity_walk_batch<TTI_COORDINATE, X, Q>, l, st);
+    if (l.variant == TTI_TENSOR) return launch_walk_batch_k<3>(k_velocity_walk_batch<TTI_TENSOR, X, Q>, l, st);
+    return launch_walk_batch_k<3>(k_velocity_walk_batch<TTI_BOND, X, Q>, l, st);
   }
-  if (variant == TTI_COORDINATE)
-    return launch_batch_k(k_velocity_batch<TTI_COORDINATE, X, Q>, inst, work, nwork, step, st);
-  if (variant == TTI_TENSOR) return launch_batch_k(k_velocity_batch<TTI_TENSOR, X, Q>, inst, work, nwork, step, st);
-  return launch_batch_k(k_velocity_batch<TTI_BOND, X, Q>, inst, work, nwork, step, st);
+  if (l.variant == TTI_COORDINATE) return launch_batch_k(k_velocity_batch<TTI_COORDINATE, X, Q>, l, st);
+  if (l.variant == TTI_TENSOR) return launch_batch_k(k_velocity_batch<TTI_TENSOR, X, Q>, l, st);
+  return launch_batch_k(k_velocity_batch<TTI_BOND, X, Q>, l, st);
 }
 
 template <bool X, bool Q>
-cudaError_t stress_batch_x(const HalfArgs *inst, const Work *work, int nwork, const int *step, int variant,
-                           bool walk, cudaStream_t st)
+cudaError_t stress_batch_x(const BatchLaunch &l, cudaStream_t st)
 {
-  if (walk) {
-    if (variant == TTI_COORDINATE)
-      return launch_walk_batch_k<2>(k_stress_walk_batch<TTI_COORDINATE, X, Q>, inst, work, nwork, step, st);
-    if (variant == TTI_TENSOR)
-      return launch_walk_batch_k<2>(k_stress_walk_batch<TTI_TENSOR, X, Q>, inst, work, nwork, step, st);
-    return launch_walk_batch_k<2>(k_stress_walk_batch<TTI_BOND, X, Q>, inst, work, nwork, step, st);
+  if (l.walk) {
+    if (l.variant == TTI_COORDINATE) return launch_walk_batch_k<2>(k_stress_walk_batch<TTI_COORDINATE, X, Q>, l, st);
+    if (l.variant == TTI_TENSOR) return launch_walk_batch_k<2>(k_stress_walk_batch<TTI_TENSOR, X, Q>, l, st);
+    return launch_walk_batch_k<2>(k_stress_walk_batch<TTI_BOND, X, Q>, l, st);
   }
-  if (variant == TTI_COORDINATE)
-    return launch_batch_k(k_stress_batch<TTI_COORDINATE, X, Q>, inst, work, nwork, step, st);
-  if (variant == TTI_TENSOR) return launch_batch_k(k_stress_batch<TTI_TENSOR, X, Q>, inst, work, nwork, step, st);
-  return launch_batch_k(k_stress_batch<TTI_BOND, X, Q>, inst, work, nwork, step, st);
+  if (l.variant == TTI_COORDINATE) return launch_batch_k(k_stress_batch<TTI_COORDINATE, X, Q>, l, st);
+  if (l.variant == TTI_TENSOR) return launch_batch_k(k_stress_batch<TTI_TENSOR, X, Q>, l, st);
+  return launch_batch_k(k_stress_batch<TTI_BOND, X, Q>, l, st);
 }
 
-cudaError_t launch_velocity_batch(const HalfArgs *inst, const Work *work, int nwork, const int *step, int variant,
-                                  bool exact, bool square, bool walk, cudaStream_t st)
+cudaError_t launch_velocity_batch(const BatchLaunch &l, cudaStream_t st)
 {
-  if (exact) return velocity_batch_x<true, false>(inst, work, nwork, step, variant, walk, st);
-  return square ? velocity_batch_x<false, true>(inst, work, nwork, step, variant, walk, st)
-                : velocity_batch_x<false, false>(inst, work, nwork, step, variant, walk, st);
+  if (l.exact) return velocity_batch_x<true, false>(l, st);
+  return l.square ? velocity_batch_x<false, true>(l, st) : velocity_batch_x<false, false>(l, st);
 }
 
-cudaError_t launch_stress_batch(const HalfArgs *inst, const Work *work, int nwork, const int *step, int variant,
-                                bool exact, bool square, bool walk, cudaStream_t st)
+cudaError_t launch_stress_batch(const BatchLaunch &l, cudaStream_t st)
 {
-  if (exact) return stress_batch_x<true, false>(inst, work, nwork, step, variant, walk, st);
-  return square ? stress_batch_x<false, true>(inst, work, nwork, step, variant, walk, st)
-                : stress_batch_x<false, false>(inst, work, nwork, step, variant, walk, st);
+  if (l.exact) return stress_batch_x<true, false>(l, st);
+  return l.square ? stress_batch_x<false, true>(l, st) : stress_batch_x<false, false>(l, st);
 }
 
-cudaError_t prepare_batch(int variant, bool exact, bool square, bool walk)
+cudaError_t prepare_batch(BatchLaunch l)
 {
   // a launch over zero CTAs only sets the attributes
-  cudaError_t e = launch_velocity_batch(nullptr, nullptr, 0, nullptr, variant, exact, square, walk, nullptr);
-  if (e == cudaSuccess) e = launch_stress_batch(nullptr, nullptr, 0, nullptr, variant, exact, square, walk, nullptr);
+  l.nwork = 0;
+  cudaError_t e = launch_velocity_batch(l, nullptr);
+  if (e == cudaSuccess) e = launch_stress_batch(l, nullptr);
   return e;
 }
 

@@ -430,15 +430,17 @@ class Batch:
         """Shots interleaved per tile in groups of `group` (0: all); graph of `graph_steps` steps (0: none)."""
         self._call("batch_set_order", self._b, group, graph_steps)
 
+    TILE_SCHEDULES = ["row", "walk", "row+persistent", "walk+persistent"]
+
     def set_schedule(self, tile_schedule):
-        """In-tile schedule of the half-step kernels: "row" (0) or "walk" (1)."""
-        ts = {"row": 0, "walk": 1}.get(tile_schedule, tile_schedule)
+        """Schedule of the half-step kernels: one of TILE_SCHEDULES (or its index)."""
+        ts = self.TILE_SCHEDULES.index(tile_schedule) if isinstance(tile_schedule, str) else tile_schedule
         self._call("batch_set_schedule", self._b, ts)
 
     def schedule(self) -> dict:
         g, gs, ts = C.c_int(), C.c_int(), C.c_int()
         self._call("batch_get_schedule", self._b, C.byref(g), C.byref(gs), C.byref(ts))
-        return {"group": g.value, "graph_steps": gs.value, "tile_schedule": ["row", "walk"][ts.value]}
+        return {"group": g.value, "graph_steps": gs.value, "tile_schedule": self.TILE_SCHEDULES[ts.value]}
 
     def autotune(self, nsteps: int) -> dict:
         """Times the schedules on nsteps steps, keeps the fastest, resets the batch."""
