@@ -488,12 +488,25 @@ __device__ __forceinline__ void velocity_walk(const HalfArgs &a, const CUtensorM
     const float *base[3];
 #pragma unroll
     for (int f = 0; f < 3; ++f) base[f] = fld + f * FIELD + 4 * BZ + l + 9;
-    walk_line<3, 4, BZ - 1, X, Q>(a, base, [&](int s, const float (&d2)[3]) {
+    // cell s of the walk: in the tile and updated by the reference
+    auto on = [&](int s) {
       const int row = l - s, z = z0 + row, x = x0 + s;
-      if ((unsigned)row < (unsigned)TZ && z >= g.izStart && z < g.Nz - NH && x < g.Nx - NH) {
-        const size_t gi = (size_t)x * g.ldz + z;
-        VCell p;
-        load_vcell(a, und, gi, p);
+      return (unsigned)row < (unsigned)TZ && z >= g.izStart && z < g.Nz - NH && x < g.Nx - NH;
+    };
+    auto at = [&](int s) { return (size_t)(x0 + s) * g.ldz + (z0 + l - s); };
+    // per-cell inputs loaded two cells ahead of their use along the walk (each
+    // cell is read and written by this thread alone, so the early loads see
+    // the values the update starts from)
+    VCell ring[2];
+#pragma unroll
+    for (int s = 0; s < 2; ++s)
+      if (on(s)) load_vcell(a, und, at(s), ring[s]);
+    walk_line<3, 4, BZ - 1, X, Q>(a, base, [&](int s, const float (&d2)[3]) {
+      const VCell p = ring[s & 1];
+      if (s + 2 < TX && on(s + 2)) load_vcell(a, und, at(s + 2), ring[s & 1]);
+      const int row = l - s;
+      if (on(s)) {
+        const size_t gi = at(s);
         float d[3][2];
 #pragma unroll
         for (int f = 0; f < 3; ++f) {
@@ -548,12 +561,22 @@ __device__ __forceinline__ void stress_walk(const HalfArgs &a, const CUtensorMap
     const float *base[2];
 #pragma unroll
     for (int f = 0; f < 2; ++f) base[f] = fld + f * FIELD + 5 * BZ + l + 7;
-    walk_line<2, 5, BZ - 1, X, Q>(a, base, [&](int s, const float (&d2)[2]) {
+    auto on = [&](int s) {
       const int row = l - s, z = z0 + row, x = x0 + s;
-      if ((unsigned)row < (unsigned)TZ && z >= g.izStart && z < g.Nz - NH && x < g.Nx - NH) {
-        const size_t gi = (size_t)x * g.ldz + z;
-        SCell p;
-        load_scell<V>(a, und, gi, p);
+      return (unsigned)row < (unsigned)TZ && z >= g.izStart && z < g.Nz - NH && x < g.Nx - NH;
+    };
+    auto at = [&](int s) { return (size_t)(x0 + s) * g.ldz + (z0 + l - s); };
+    // per-cell inputs two cells ahead, as in the velocity walk
+    SCell ring[2];
+#pragma unroll
+    for (int s = 0; s < 2; ++s)
+      if (on(s)) load_scell<V>(a, und, at(s), ring[s]);
+    walk_line<2, 5, BZ - 1, X, Q>(a, base, [&](int s, const float (&d2)[2]) {
+      const SCell p = ring[s & 1];
+      if (s + 2 < TX && on(s + 2)) load_scell<V>(a, und, at(s + 2), ring[s & 1]);
+      const int row = l - s;
+      if (on(s)) {
+        const size_t gi = at(s);
         float d[2][2];
 #pragma unroll
         for (int f = 0; f < 2; ++f) {
