@@ -83,7 +83,7 @@ def test_walk_schedule_gradient_equals_row_schedule(variant, fs, monkeypatch, gp
     grid of several tiles the gradient must be the row schedule's, bit for bit."""
     J0, g0 = _gradient("row", monkeypatch, variant, fs)
     J1, g1 = _gradient("walk", monkeypatch, variant, fs)
-    assert J1 == J0
+    assert J1 == pytest.approx(J0, rel=1e-12)  # J is a double atomic sum: order-dependent last bit
     for n in g0:
         assert np.array_equal(g1[n].view(np.uint32), g0[n].view(np.uint32)), n
         assert np.abs(g0[n]).max() > 0

@@ -893,12 +893,16 @@ __global__ void k_chain(Grid g, Params p, const float *vp, const float *vs, cons
 
 int gerr(tti_handle *h, int code, const char *msg) { return handle_error(h, code, msg); }
 
+// On failure the runtime's last error is cleared as well: a refused
+// allocation must not be found again by a later launch check.
 #define GCK(h, call)                                                                    \
   do {                                                                                  \
     cudaError_t e_ = (call);                                                            \
-    if (e_ != cudaSuccess)                                                              \
+    if (e_ != cudaSuccess) {                                                            \
+      cudaGetLastError();                                                               \
       return gerr((h), e_ == cudaErrorMemoryAllocation ? TTI_ERR_NOMEM : TTI_ERR_CUDA, \
                   cudaGetErrorString(e_));                                              \
+    }                                                                                   \
   } while (0)
 
 int grad_check(tti_handle *h)
@@ -924,7 +928,10 @@ int grad_alloc(tti_handle *h)
   for (auto &p : s->acc) ok = ok && al(&p);
   for (auto &p : s->out) ok = ok && al(&p);
   ok = ok && cudaMalloc(&s->d_J, sizeof(double)) == cudaSuccess;
-  if (!ok) return gerr(h, TTI_ERR_NOMEM, "device allocation of the gradient buffers failed");
+  if (!ok) {
+    cudaGetLastError();
+    return gerr(h, TTI_ERR_NOMEM, "device allocation of the gradient buffers failed");
+  }
   if (h->use_tiled) {
     void *mem = nullptr;
     if (posix_memalign(&mem, 64, 10 * sizeof(CUtensorMap)) != 0)
@@ -1283,6 +1290,7 @@ int grad_prepare(tti_handle *h, int slots, int seg, SourceTables *tab)
     s->ckpt = s->keep = nullptr;
     if (cudaMalloc(&s->ckpt, sizeof(float) * nf * n * std::max(1, slots)) != cudaSuccess ||
         cudaMalloc(&s->keep, sizeof(float) * nk * n * seg) != cudaSuccess) {
+      cudaGetLastError();
       cudaFree(s->ckpt);  // nothing half-allocated stays behind; the handle stays usable
       cudaFree(s->keep);
       s->ckpt = s->keep = nullptr;
@@ -1516,7 +1524,8 @@ int tti_grad_plan(const tti_handle *h, double budget_bytes, int *snapshots, int 
   // macro-step lengths on a geometric grid; the slots left over for each
   long long best = -1;
   int bs = 0, bl = 0;
-  for (int L = 1; L <= nt; L = std::max(L + 1, (int)(L * 1.25))) {
+  // (the last candidate is nt itself: one macro-step, every step kept)
+  for (int L = 1; L <= nt; L = L == nt ? nt + 1 : std::min(nt, std::max(L + 1, (int)(L * 1.25)))) {
     const int M = (nt + L - 1) / L;
     if (M > 4000) continue;  // keeps the cost table small; longer macro-steps come next
     const double left = budget_bytes - L * kept;

@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <future>
 #include <vector>
 
 #include <algorithm>
@@ -30,12 +31,16 @@ int set_err(tti_handle *h, int code, const char *fmt, ...)
   return code;
 }
 
+// On failure the runtime's last error is cleared too, so that a refused
+// allocation is not found again by a later launch check.
 #define CK(h, call)                                                                                     \
   do {                                                                                                  \
     cudaError_t e_ = (call);                                                                            \
-    if (e_ != cudaSuccess)                                                                              \
+    if (e_ != cudaSuccess) {                                                                            \
+      cudaGetLastError();                                                                               \
       return set_err((h), e_ == cudaErrorMemoryAllocation ? TTI_ERR_NOMEM : TTI_ERR_CUDA, "%s: %s (%s:%d)", \
                      #call, cudaGetErrorString(e_), __FILE__, __LINE__);                                \
+    }                                                                                                   \
   } while (0)
 
 // Arrays each formulation needs on the device (beyond D/Beta/coef/vp/vs/rho
@@ -230,6 +235,52 @@ int snapshot_kinds(int wsave, int *kinds)
   }
 }
 
+// Copies `bytes` from device memory into a host buffer whose pages are
+// resident, ordered after the work already on h's stream; returns once the
+// data are in place. Above one chunk, through two page-locked chunks: the DMA
+// of chunk c runs while host threads copy chunk c - 1 out (the driver's own
+// staging of a pageable destination is slower); otherwise directly.
+int download(tti_handle *h, void *dst, const void *src, size_t bytes)
+{
+  constexpr size_t CH = PIN_CHUNK * sizeof(float);
+  float *pin[2] = {nullptr, nullptr};
+  if (bytes > CH) {
+    pin[0] = pinned_chunk();
+    pin[1] = pinned_chunk();
+  }
+  for (int b = 0; b < 2 && pin[0] && pin[1]; ++b)
+    if (!h->pev[5 + b] && cudaEventCreateWithFlags(&h->pev[5 + b], cudaEventDisableTiming) != cudaSuccess)
+      pinned_release(pin[b]), pin[b] = nullptr;
+  if (!pin[0] || !pin[1]) {
+    pinned_release(pin[0]);
+    pinned_release(pin[1]);
+    CK(h, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    return TTI_OK;
+  }
+  const size_t nchunk = (bytes + CH - 1) / CH;
+  cudaError_t e = cudaSuccess;
+  for (size_t c = 0; c <= nchunk && e == cudaSuccess; ++c) {
+    if (c < nchunk) {
+      const size_t off = c * CH, nb = std::min(CH, bytes - off);
+      e = cudaMemcpyAsync(pin[c & 1], static_cast<const char *>(src) + off, nb, cudaMemcpyDeviceToHost, h->stream);
+      if (e == cudaSuccess) e = cudaEventRecord(h->pev[5 + (c & 1)], h->stream);
+    }
+    if (c > 0 && e == cudaSuccess) {
+      const size_t p = c - 1, off = p * CH, nb = std::min(CH, bytes - off);
+      e = cudaEventSynchronize(h->pev[5 + (p & 1)]);
+      if (e == cudaSuccess) parallel_copy(static_cast<char *>(dst) + off, pin[p & 1], nb, 8);
+    }
+  }
+  // wait on the error path too before the chunks go back to the shared list
+  const cudaError_t es = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess) e = es;
+  pinned_release(pin[0]);
+  pinned_release(pin[1]);
+  CK(h, e);
+  return TTI_OK;
+}
+
 int do_snapshot(tti_handle *h, tti_snapshot_fn fn, void *user, int it)
 {
   const Grid &g = h->g;
@@ -254,9 +305,8 @@ int do_snapshot(tti_handle *h, tti_snapshot_fn fn, void *user, int it)
   for (int q = 0; q < nk; ++q) {
     launch_snapshot(a, kinds[q], h->cfg.savew, h->d_snap, h->stream);
     h->launches++;
-    // pageable destination whose pages are resident: the driver's staged copy
-    CK(h, cudaMemcpyAsync(h->h_snap, h->d_snap, n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
-    CK(h, cudaStreamSynchronize(h->stream));
+    const int rc = download(h, h->h_snap, h->d_snap, n * sizeof(float));
+    if (rc) return rc;
     if (fn(user, it, kinds[q], h->h_snap, nzo, nxo) != 0)
       return set_err(h, TTI_ERR_CALLBACK, "snapshot callback aborted the run at it=%d", it);
   }
@@ -549,15 +599,10 @@ int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const floa
   const tti_config &c = h->cfg;
   const Grid &g = h->g;
   const size_t np = (size_t)g.Nz * g.Nx;
-  // stability check on the unscaled padded vp (stable.c:217-246)
-  {
-    const double vmax = host_max(vp, np, FLT_MIN);
-    const double csum = (double)rsg(0) + (double)rsg(2) + (double)rsg(4);
-    const double dtmax = 1.0f / (vmax * sqrt((1.0 / (c.dx * c.dx) + 1.0 / (c.dz * c.dz)) * csum));
-    if (c.dt > dtmax)
-      return set_err(h, TTI_ERR_UNSTABLE,
-                     "the finite differenct scheme is unstable! the time step size must smaller than %5.5f!", dtmax);
-  }
+  // Stability check on the unscaled padded vp (stable.c:217-246). Its host
+  // maximum runs on other threads while the arrays travel to the device;
+  // nothing is computed from them on the device before it has passed.
+  auto vmax_f = std::async(std::launch::async, [vp, np] { return host_max(vp, np, FLT_MIN); });
   // raw model on the device (pitched, one block of six arrays), freed after the precompute
   float *raw[6] = {};
   const float *src[6] = {vp, vs, rho, epsilon, delta, theta};
@@ -569,6 +614,17 @@ int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const floa
   }
   for (int k = 0; k < 6; ++k) raw[k] = raw_block + (size_t)k * g.n;
   if (rc == TTI_OK) rc = upload_arrays(h, src, raw, 6);
+  {
+    const double vmax = vmax_f.get();
+    const double csum = (double)rsg(0) + (double)rsg(2) + (double)rsg(4);
+    const double dtmax = 1.0f / (vmax * sqrt((1.0 / (c.dx * c.dx) + 1.0 / (c.dz * c.dz)) * csum));
+    if (rc == TTI_OK && c.dt > dtmax) {
+      cudaStreamSynchronize(h->stream);
+      pool_free(raw_block, h->stream);
+      return set_err(h, TTI_ERR_UNSTABLE,
+                     "the finite differenct scheme is unstable! the time step size must smaller than %5.5f!", dtmax);
+    }
+  }
   if (rc == TTI_OK) {
     // MEAL scalars evaluated with the host libm, as meal.c:23-29, 62-66 do
     const int nl = g.E;

@@ -71,9 +71,11 @@ int berr(tti_batch *b, int code, const char *fmt, ...)
 #define BCK(b, call)                                                                                   \
   do {                                                                                                 \
     cudaError_t e_ = (call);                                                                           \
-    if (e_ != cudaSuccess)                                                                             \
+    if (e_ != cudaSuccess) {                                                                           \
+      cudaGetLastError();                                                                              \
       return berr((b), e_ == cudaErrorMemoryAllocation ? TTI_ERR_NOMEM : TTI_ERR_CUDA, "%s: %s", #call, \
                   cudaGetErrorString(e_));                                                             \
+    }                                                                                                  \
   } while (0)
 
 // Instances read their model's state: uploaded or not, the undamped-tile flag,
@@ -357,7 +359,10 @@ int tti_batch_create(tti_batch **out, int nmodels, const tti_config *cfg, int ni
                   cudaMalloc(&b->d_tab, sizeof(SourceTables) * nmodels) == cudaSuccess &&
                   cudaMalloc(&b->d_work, sizeof(tiled::Work) * (size_t)std::max(1, b->nwork)) == cudaSuccess &&
                   cudaMalloc(&b->d_step, sizeof(int)) == cudaSuccess;
-  if (!ok) return fail(TTI_ERR_NOMEM, "device allocation of the batch tables failed");
+  if (!ok) {
+    cudaGetLastError();
+    return fail(TTI_ERR_NOMEM, "device allocation of the batch tables failed");
+  }
   *out = b;
   return TTI_OK;
 }

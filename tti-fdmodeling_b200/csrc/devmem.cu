@@ -54,7 +54,11 @@ cudaError_t pool_alloc(void **p, size_t bytes, cudaStream_t st)
   cudaMemPool_t pool = nullptr;
   cudaError_t e = pool_of(&pool);
   if (e != cudaSuccess) return e;
-  return cudaMallocFromPoolAsync(p, bytes, pool, st);
+  e = cudaMallocFromPoolAsync(p, bytes, pool, st);
+  // a refused request is reported here; it must not linger as the runtime's
+  // last error, where a later launch check would find it
+  if (e != cudaSuccess) cudaGetLastError();
+  return e;
 }
 
 void pool_free(void *p, cudaStream_t st)
