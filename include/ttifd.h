@@ -280,20 +280,17 @@ int tti_batch_upload_model(tti_batch *b, int m, const float *vp, const float *vs
  * 1: shot after shot), and the loop replays a CUDA graph of `graph_steps`
  * steps (0: no graph). */
 int tti_batch_set_order(tti_batch *b, int group, int graph_steps);
-/* Schedule of the half-step kernels. Bit 0, the in-tile schedule: 0 = row
- * (one row of cells per thread, every stencil tap a shared-memory load),
- * 1 = walk (each thread walks a diagonal, then an anti-diagonal, of the tile
- * with the stencil taps in a sliding register window). Bit 1: 0 = one CTA per
+/* Grid of the batched half-step launches: 0 = one CTA per (instance, tile)
  * work item, 1 = persistent (one resident wave of CTAs walks the work table).
- * All four give the same bits. */
-int tti_batch_set_schedule(tti_batch *b, int tile_schedule);
+ * Both give the same bits. */
+int tti_batch_set_schedule(tti_batch *b, int persistent);
 /* The schedule in use (any output may be NULL). */
-int tti_batch_get_schedule(const tti_batch *b, int *group, int *graph_steps, int *tile_schedule);
-/* Times every group size in {all, 1, 2, 4, 8, 16} (those below the shot
- * count) with and without a graph of 20 steps, under both tile schedules,
- * each over nsteps steps (at least one graph replay, at most the longest
- * instance's nt) in two rounds, keeps the fastest and resets the batch.
- * Outputs (may be NULL): the choice and its ms per step; the tile schedule
+int tti_batch_get_schedule(const tti_batch *b, int *group, int *graph_steps, int *persistent);
+/* Times every group size in {all, 1, 4, 16} (those below the shot count)
+ * with and without a graph of 20 steps, with one CTA per work item and with a
+ * persistent grid, each over nsteps steps (at least one graph replay, at most
+ * the longest instance's nt) in two rounds, keeps the fastest and resets the
+ * batch. Outputs (may be NULL): the choice and its ms per step; the grid
  * chosen is read with tti_batch_get_schedule. */
 int tti_batch_autotune(tti_batch *b, int nsteps, int *group, int *graph_steps, float *ms_per_step);
 /* Zeroes every instance and rebuilds the launch tables from the current

@@ -65,7 +65,7 @@ CASES = {
     "coord_tiles": ("coordinate_rotation", dict(nz=280, nx=180, nt=400, seistype=3, wsave=2, snap_sample=399),
                     "salt", [(43, 113)], (1, 113)),
     "tensor_tiles_fs": ("tensor_rotation", dict(nz=280, nx=180, nt=400, freesurface=1, seistype=3, wsave=2,
-                                                snap_sample=399), "salt", [(43, 2)], (1, 98)),
+                                                snap_sample=399), "salt", [(43, 108)], (1, 112)),
     "bond_tiles": ("bond_transformation", dict(nz=280, nx=180, nt=400, seistype=3, wsave=2, snap_sample=399),
                    "salt", [(59, 113)], (2, 112)),
 }

@@ -42,7 +42,7 @@ def _single(cfg, model, k):
         return [h.fetch_traces(c) for c in (0, 1, 2)]
 
 
-def _batch(cfgs, models, model_of, group=0, graph_steps=20, tile_schedule="row"):
+def _batch(cfgs, models, model_of, group=0, graph_steps=20, grid="per-tile"):
     import ttifd
 
     out = []
@@ -50,7 +50,7 @@ def _batch(cfgs, models, model_of, group=0, graph_steps=20, tile_schedule="row")
         for m, model in enumerate(models):
             b.upload_model(m, *model)
         b.set_order(group, graph_steps)
-        b.set_schedule(tile_schedule)
+        b.set_schedule(grid)
         for i, m in enumerate(model_of):
             sx, sz, w, gx, gz = _geometry(cfgs[m], i)
             inst = b.instances[i]
@@ -101,24 +101,23 @@ def test_batch_schedules_agree(group, graph_steps, monkeypatch, gpu_lib):
             assert np.array_equal(got[i][c].view(np.uint32), ref[i][c].view(np.uint32))
 
 
-@pytest.mark.parametrize("tile_schedule", ["walk", "row+persistent", "walk+persistent"])
-def test_batch_tile_schedules_agree(tile_schedule, monkeypatch, gpu_lib):
-    """The walk schedule and the persistent grid (one wave of CTAs walking the
-    work table) give the row schedule's traces bit for bit, with uneven models,
-    mode 2 and a graph."""
+@pytest.mark.parametrize("graph_steps", [0, 20])
+def test_batch_persistent_grid_agrees(graph_steps, monkeypatch, gpu_lib):
+    """The persistent grid (one wave of CTAs walking the work table) gives the
+    per-tile grid's traces bit for bit, with uneven models and mode 2."""
     monkeypatch.delenv("TTIFD_EXACT", raising=False)
     cfgs = [_model_cfg(130, 200, 100, 1, 1), _model_cfg(100, 160, 70, 1, 8, mode=2)]
     models = _models(cfgs)
     model_of = [0, 0, 1, 0, 1]
-    ref, _ = _batch(cfgs, models, model_of, group=0, graph_steps=20)
-    got, _ = _batch(cfgs, models, model_of, group=0, graph_steps=20, tile_schedule=tile_schedule)
+    ref, _ = _batch(cfgs, models, model_of, group=0, graph_steps=graph_steps)
+    got, _ = _batch(cfgs, models, model_of, group=0, graph_steps=graph_steps, grid="persistent")
     for i in range(len(model_of)):
         for c in range(3):
-            assert np.array_equal(got[i][c].view(np.uint32), ref[i][c].view(np.uint32)), (tile_schedule, i, c)
+            assert np.array_equal(got[i][c].view(np.uint32), ref[i][c].view(np.uint32)), (graph_steps, i, c)
 
 
 def test_batch_fma_mode_matches_single_shot(monkeypatch, gpu_lib):
-    monkeypatch.delenv("TTIFD_EXACT", raising=False)
+    monkeypatch.setenv("TTIFD_EXACT", "0")  # the FMA opt-in
     monkeypatch.delenv("TTIFD_KERNEL", raising=False)
     cfgs = [_model_cfg(140, 220, 150, 1, 1)]
     models = _models(cfgs)

@@ -41,13 +41,14 @@ def _compare(name, got, gold, rtol, peak):
     assert compared >= 3
 
 
-@pytest.mark.parametrize("schedule", ["row", "walk"])
+@pytest.mark.parametrize("arith", ["reference", "fma"])
 @pytest.mark.parametrize("name", helpers.golden_names())
-def test_gpu_matches_reference_build(name, schedule, gpu_lib, monkeypatch):
-    """The default (FMA) arithmetic with either in-tile schedule of the tiled kernels."""
+def test_gpu_matches_reference_build(name, arith, gpu_lib, monkeypatch):
+    """The default arithmetic (the reference's rounding) and the FMA opt-in
+    (TTIFD_EXACT=0) against the reference build's outputs."""
     import ttifd
 
-    monkeypatch.setenv("TTIFD_SCHEDULE", schedule)
+    monkeypatch.setenv("TTIFD_EXACT", "1" if arith == "reference" else "0")
     case = helpers.load_golden(name)
     got = helpers.run_backend(ttifd.Modeling, case)
     _compare(name, got, helpers.golden_arrays(case), TRACE_RTOL, TRACE_PEAK)

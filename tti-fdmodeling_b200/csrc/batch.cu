@@ -41,7 +41,6 @@ struct tti_batch {
   SourceTables *d_tab = nullptr;
   int *d_step = nullptr;
   int group = 0;  // work-table order: shots of a model interleaved tile by tile in groups of `group` (0: all)
-  bool walk = false;  // in-tile schedule of the half-step kernels: walk (true) or row
   bool persistent = false;  // one resident wave of CTAs walks the work table (else one CTA per item)
   int graph_steps = 20;
   cudaGraph_t graph = nullptr;
@@ -216,7 +215,7 @@ int build_tables(tti_batch *b)
 tiled::BatchLaunch batch_launch(const tti_batch *b, bool vel)
 {
   return tiled::BatchLaunch{vel ? b->d_vel : b->d_str, b->d_work, b->nwork, b->d_step, b->variant, b->exact,
-                            b->square, b->walk, b->persistent};
+                            b->square, b->persistent};
 }
 
 // The launches of one time step (all instances).
@@ -314,12 +313,10 @@ int tti_batch_create(tti_batch **out, int nmodels, const tti_config *cfg, int ni
   tti_batch *b = new tti_batch();
   b->device = device;
   b->variant = cfg[0].variant;
-  const char *ex = getenv("TTIFD_EXACT");
-  b->exact = ex && ex[0] == '1';
+  const char *ex = getenv("TTIFD_EXACT");  // the handles' default: the reference's rounding
+  b->exact = !(ex && ex[0] == '0');
   const char *gs = getenv("TTIFD_GRAPH_STEPS");
   if (gs) b->graph_steps = atoi(gs);
-  const char *sched = getenv("TTIFD_SCHEDULE");
-  b->walk = sched && strcmp(sched, "walk") == 0;
   auto fail = [&](int rc, const std::string &msg) {
     tti_batch_destroy(b);
     return berr(nullptr, rc, "%s", msg.c_str());
@@ -397,27 +394,25 @@ int tti_batch_set_order(tti_batch *b, int group, int graph_steps)
   return TTI_OK;
 }
 
-int tti_batch_set_schedule(tti_batch *b, int tile_schedule)
+int tti_batch_set_schedule(tti_batch *b, int persistent)
 {
-  if (!b || tile_schedule < 0 || tile_schedule > 3) return berr(b, TTI_ERR_ARG, "tile schedule must be 0..3");
-  const bool walk = tile_schedule & 1, persistent = tile_schedule & 2;
-  if (walk != b->walk || persistent != b->persistent) {  // the captured launches select the kernels
+  if (!b || persistent < 0 || persistent > 1) return berr(b, TTI_ERR_ARG, "grid schedule must be 0 or 1");
+  if ((persistent == 1) != b->persistent) {  // the captured launches set the grid sizes
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     b->exec = nullptr;
     b->graph = nullptr;
-    b->walk = walk;
-    b->persistent = persistent;
+    b->persistent = persistent == 1;
   }
   return TTI_OK;
 }
 
-int tti_batch_get_schedule(const tti_batch *b, int *group, int *graph_steps, int *tile_schedule)
+int tti_batch_get_schedule(const tti_batch *b, int *group, int *graph_steps, int *persistent)
 {
   if (!b) return TTI_ERR_ARG;
   if (group) *group = b->group;
   if (graph_steps) *graph_steps = b->graph_steps;
-  if (tile_schedule) *tile_schedule = (b->walk ? 1 : 0) | (b->persistent ? 2 : 0);
+  if (persistent) *persistent = b->persistent ? 1 : 0;
   return TTI_OK;
 }
 
@@ -484,7 +479,7 @@ int tti_batch_autotune(tti_batch *b, int nsteps, int *group, int *graph_steps, f
   for (int g : {1, 4, 16})
     if (g < ninst_max) groups.push_back(g);
   const int graphs[] = {0, 20};
-  const int NS = 4;  // tile schedules: row, walk, each with one CTA per tile or a persistent wave
+  const int NS = 2;  // grids: one CTA per tile, or a persistent wave
   // Each candidate is timed twice, in two rounds over all of them, and keeps
   // its faster time; a graph candidate is timed over at least one replay of
   // its graph (the step loop only replays it when that many steps remain).

@@ -32,7 +32,6 @@ struct alignas(64) HalfArgs {
   int nt;      // batched launches: time steps of this instance (its CTAs idle once the step counter reaches it)
   int tiles_z; // batched launches: tile rows of this instance's grid
   int square;  // FMA mode with dx == dz: stencil coefficients hc fold in h = 0.5 / dx
-  int walk;    // the walk schedule of the tile (register windows along the diagonals)
   unsigned wait_limit;  // polls of the first TMA wait before it gives up (tma::WAIT_LIMIT)
   float hc[5]; // h * C_k
   // Gradient forward pass (null: nothing kept). Velocity update, coordinate
@@ -71,7 +70,6 @@ struct BatchLaunch {
   const int *step;       // device: the shared step counter
   int variant;
   bool exact, square;    // square: every instance has folded coefficients (set_square)
-  bool walk;             // the walk schedule of the tile instead of the row schedule
   bool persistent;       // one resident wave of CTAs walks the table (else one CTA per item)
 };
 cudaError_t launch_velocity_batch(const BatchLaunch &l, cudaStream_t st);

@@ -361,252 +361,6 @@ __device__ __forceinline__ void stress_tile(const HalfArgs &a, const CUtensorMap
   }
 }
 
-// ---------------------------------------------------------------------------
-// Walk schedule of the same tiles. The d1 sum of a cell reads one field along
-// its diagonal (x + i, z + i) and the d2 sum along an anti-diagonal
-// (x + i, z + c - i), ten taps each. Instead of one shared-memory load per
-// tap, a thread walks one diagonal of the tile across its TX columns keeping
-// the ten taps of the current cell in registers (a sliding window: one new
-// load per cell), and a second pass walks the anti-diagonals the same way:
-//   phase A  thread l walks diagonal z - x = z0 - x0 + l - (TX - 1) and writes
-//            d1 of every field at each tile cell it crosses into a shared
-//            buffer [field][column][row];
-//   phase B  thread l walks anti-diagonal x + z = x0 + z0 + l, forms d2 of
-//            every field, reads the cell's d1 back and finishes the update.
-// Per cell and field that is about (TX + 9) / TX loads per phase plus one
-// store and one load of d1, against 20 loads in the row schedule above. In
-// both phases the lanes of a warp sit on 32 consecutive rows of one column, so
-// shared accesses are conflict-free and global accesses coalesced.
-// The sums are formed in the order of the row schedule (k = 1 first), so both
-// schedules give the same bits.
-namespace walk {
-
-constexpr int LANES = TZ + TX - 1;            // diagonals crossing a tile
-constexpr int NTW = (LANES + 31) / 32 * 32;   // threads per CTA
-constexpr int GUARD = 32;                     // floats before the first field
-constexpr int DB = TX * TZ;                   // floats of one field's d1 buffer
-// The windows of lanes whose walk leaves the tile rows reach past the box: down
-// to TX - 4 floats before a field's region and up to TX - 5 after its last box
-// element (the stress walk one less after). Those values feed only cells
-// outside the tile, which are never stored; the guard and the region's slack
-// keep the addresses inside the CTA's shared memory.
-static_assert(GUARD >= TX - 4 && FIELD - BX * BZ >= TX - 5, "walk windows must stay inside shared memory");
-
-constexpr size_t smem_floats(int nf) { return GUARD + (size_t)nf * (FIELD + DB) + 4; }
-
-// sum_k C_k (w[4 + k] - w[5 - k]), k = 1 .. 5 in order (the row schedule's order)
-template <bool X, bool Q>
-__device__ __forceinline__ float window_sum(const HalfArgs &a, const float (&w)[10])
-{
-  using A = Ar<X>;
-  float s = A::mul(coef<Q>(a, 0), A::sub(w[5], w[4]));
-#pragma unroll
-  for (int k = 2; k <= NH; ++k) s = A::add(s, A::mul(coef<Q>(a, k - 1), A::sub(w[4 + k], w[5 - k])));
-  return s;
-}
-
-// Walks NF fields from base[f] + (i * step) for i = -H .. TX - 1 + 9 - H:
-// window of cell s is the values at i = s - H .. s + 9 - H. fn(s, sums).
-template <int NF, int H, int STEP, bool X, bool Q, typename F>
-__device__ __forceinline__ void walk_line(const HalfArgs &a, const float *const (&base)[NF], F fn)
-{
-  float w[NF][10];
-#pragma unroll
-  for (int f = 0; f < NF; ++f)
-#pragma unroll
-    for (int j = 0; j < 9; ++j) w[f][j] = base[f][(j - H) * STEP];
-#pragma unroll
-  for (int s = 0; s < TX; ++s) {
-    float sum[NF];
-#pragma unroll
-    for (int f = 0; f < NF; ++f) {
-      w[f][9] = base[f][(s + 9 - H) * STEP];
-      sum[f] = window_sum<X, Q>(a, w[f]);
-#pragma unroll
-      for (int j = 0; j < 9; ++j) w[f][j] = w[f][j + 1];
-    }
-    fn(s, sum);
-  }
-}
-
-// L2 prefetch of the tile's per-cell lines while the halo boxes are in flight:
-// `nl` 128-byte lines per 32 rows of a column, line q of column x at line(q, gi).
-template <typename L>
-__device__ __forceinline__ void prefetch_tile(const HalfArgs &a, int x0, int z0, int nl, L line)
-{
-  const int per_col = nl * (TZ / 32);
-  for (int q = threadIdx.x; q < TX * per_col; q += blockDim.x) {
-    const int col = q / per_col, r = q % per_col, x = x0 + col, z = z0 + 32 * (r % (TZ / 32));
-    if (x >= a.g.Nx - NH || z >= a.g.Nz - NH) continue;
-    const void *p = line(r / (TZ / 32), (size_t)x * a.g.ldz + z);
-    if (p) asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
-  }
-}
-
-template <int V, bool X, bool Q, bool K>
-__device__ __forceinline__ void velocity_walk(const HalfArgs &a, const CUtensorMap *map, float *sm, int tz, int tx)
-{
-  float *fld = sm + GUARD;
-  float *db = fld + 3 * FIELD;
-  unsigned long long *bar = reinterpret_cast<unsigned long long *>(db + 3 * DB);
-  const Grid &g = a.g;
-  const int z0 = a.z_base + tz * TZ, x0 = a.x_base + tx * TX;
-  tma::issue_tiles(map, fld, bar, 3, z0, x0, 4);
-  const Cells c{x0, z0, x0, z0};
-  const bool und = tile_undamped(a, c);
-  prefetch_tile(a, x0, z0, V == TTI_COORDINATE ? 7 : 5, [&](int k, size_t gi) -> const void * {
-    switch (k) {
-    case 0: return a.f.vx + gi;
-    case 1: return a.f.vz + gi;
-    case 2: return a.p.invrho + gi;
-    case 3: return und ? nullptr : (const void *)(a.pk.cf + gi);
-    case 4: return und ? nullptr : (const void *)(a.pk.cf + gi + 16);
-    case 5: return a.pk.vsc + gi;
-    default: return a.pk.vsc + gi + 16;
-    }
-  });
-  if (!tma::wait_tiles(a.err, bar, a.wait_limit)) return;
-  const int l = threadIdx.x;
-  // box element (column x0 - 4 + i, row z0 - 8 + r) of field f: fld[f * FIELD + i * BZ + r]
-  if (l < LANES) {
-    // phase A: d1 along diagonal row - col = l - (TX - 1); cell s at (x0 + s, z0 + l - (TX - 1) + s)
-    const int c0 = l - (TX - 1);
-    const float *base[3];
-#pragma unroll
-    for (int f = 0; f < 3; ++f) base[f] = fld + f * FIELD + 4 * BZ + c0 + 8;
-    walk_line<3, 4, BZ + 1, X, Q>(a, base, [&](int s, const float (&d1)[3]) {
-      const int row = c0 + s;
-      if ((unsigned)row < (unsigned)TZ)
-#pragma unroll
-        for (int f = 0; f < 3; ++f) db[f * DB + s * TZ + row] = d1[f];
-    });
-  }
-  __syncthreads();
-  if (l < LANES) {
-    // phase B: d2 along anti-diagonal row + col = l; cell s at (x0 + s, z0 + l - s); its taps
-    // are (x + i, z + 1 - i), i.e. the line (x0 + j, z0 + l + 1 - j)
-    const float *base[3];
-#pragma unroll
-    for (int f = 0; f < 3; ++f) base[f] = fld + f * FIELD + 4 * BZ + l + 9;
-    // cell s of the walk: in the tile and updated by the reference
-    auto on = [&](int s) {
-      const int row = l - s, z = z0 + row, x = x0 + s;
-      return (unsigned)row < (unsigned)TZ && z >= g.izStart && z < g.Nz - NH && x < g.Nx - NH;
-    };
-    auto at = [&](int s) { return (size_t)(x0 + s) * g.ldz + (z0 + l - s); };
-    // per-cell inputs loaded two cells ahead of their use along the walk (each
-    // cell is read and written by this thread alone, so the early loads see
-    // the values the update starts from)
-    VCell ring[2];
-#pragma unroll
-    for (int s = 0; s < 2; ++s)
-      if (on(s)) load_vcell(a, und, at(s), ring[s]);
-    walk_line<3, 4, BZ - 1, X, Q>(a, base, [&](int s, const float (&d2)[3]) {
-      const VCell p = ring[s & 1];
-      if (s + 2 < TX && on(s + 2)) load_vcell(a, und, at(s + 2), ring[s & 1]);
-      const int row = l - s;
-      if (on(s)) {
-        const size_t gi = at(s);
-        float d[3][2];
-#pragma unroll
-        for (int f = 0; f < 3; ++f) {
-          d[f][0] = db[f * DB + s * TZ + row];
-          d[f][1] = d2[f];
-        }
-        velocity_store<V, X, Q, K>(a, gi, d, p);
-      }
-    });
-  }
-}
-
-template <int V, bool X, bool Q, bool K>
-__device__ __forceinline__ void stress_walk(const HalfArgs &a, const CUtensorMap *map, float *sm, int tz, int tx)
-{
-  float *fld = sm + GUARD;
-  float *db = fld + 2 * FIELD;
-  unsigned long long *bar = reinterpret_cast<unsigned long long *>(db + 2 * DB);
-  const Grid &g = a.g;
-  const int z0 = a.z_base + tz * TZ, x0 = a.x_base + tx * TX;
-  tma::issue_tiles(map, fld, bar, 2, z0, x0, 5);
-  const Cells c{x0, z0, x0, z0};
-  const bool und = tile_undamped(a, c);
-  prefetch_tile(a, x0, z0, V == TTI_TENSOR ? 12 : 11, [&](int k, size_t gi) -> const void * {
-    if (k < 3)
-      return (V == TTI_TENSOR ? (k == 0 ? a.f.txx : k == 1 ? a.f.tzz : a.f.txz)
-                              : (k == 0 ? a.f.sxx : k == 1 ? a.f.szz : a.f.sxz)) + gi;
-    if (k < 5) return und ? nullptr : (const void *)(a.pk.cf + gi + 16 * (k - 3));
-    if (k < 9) return a.pk.c4 + gi + 8 * (k - 5);
-    if (k < 11) return a.pk.sc + gi + 16 * (k - 9);
-    return a.p.s2t + gi;
-  });
-  if (!tma::wait_tiles(a.err, bar, a.wait_limit)) return;
-  const int l = threadIdx.x;
-  // box element (column x0 - 5 + i, row z0 - 8 + r) of field f: fld[f * FIELD + i * BZ + r]
-  if (l < LANES) {
-    // phase A: d1 taps (x + k - 1, z + k - 1) and (x - k, z - k) on the cell's diagonal
-    const int c0 = l - (TX - 1);
-    const float *base[2];
-#pragma unroll
-    for (int f = 0; f < 2; ++f) base[f] = fld + f * FIELD + 5 * BZ + c0 + 8;
-    walk_line<2, 5, BZ + 1, X, Q>(a, base, [&](int s, const float (&d1)[2]) {
-      const int row = c0 + s;
-      if ((unsigned)row < (unsigned)TZ)
-#pragma unroll
-        for (int f = 0; f < 2; ++f) db[f * DB + s * TZ + row] = d1[f];
-    });
-  }
-  __syncthreads();
-  if (l < LANES) {
-    // phase B: d2 taps (x + k - 1, z - k) and (x - k, z + k - 1): the line (x0 + j, z0 + l - 1 - j)
-    const float *base[2];
-#pragma unroll
-    for (int f = 0; f < 2; ++f) base[f] = fld + f * FIELD + 5 * BZ + l + 7;
-    auto on = [&](int s) {
-      const int row = l - s, z = z0 + row, x = x0 + s;
-      return (unsigned)row < (unsigned)TZ && z >= g.izStart && z < g.Nz - NH && x < g.Nx - NH;
-    };
-    auto at = [&](int s) { return (size_t)(x0 + s) * g.ldz + (z0 + l - s); };
-    // per-cell inputs two cells ahead, as in the velocity walk
-    SCell ring[2];
-#pragma unroll
-    for (int s = 0; s < 2; ++s)
-      if (on(s)) load_scell<V>(a, und, at(s), ring[s]);
-    walk_line<2, 5, BZ - 1, X, Q>(a, base, [&](int s, const float (&d2)[2]) {
-      const SCell p = ring[s & 1];
-      if (s + 2 < TX && on(s + 2)) load_scell<V>(a, und, at(s + 2), ring[s & 1]);
-      const int row = l - s;
-      if (on(s)) {
-        const size_t gi = at(s);
-        float d[2][2];
-#pragma unroll
-        for (int f = 0; f < 2; ++f) {
-          d[f][0] = db[f * DB + s * TZ + row];
-          d[f][1] = d2[f];
-        }
-        stress_finish<V, X, Q, K>(a, gi, d, p);
-      }
-    });
-  }
-}
-
-}  // namespace walk
-
-template <int V, bool X, bool Q, bool K = false>
-__global__ void __launch_bounds__(walk::NTW, 3) k_velocity_walk(const __grid_constant__ HalfArgs a)
-{
-  extern __shared__ __align__(128) float sm[];
-  pdl_sync();
-  walk::velocity_walk<V, X, Q, K>(a, a.map, sm, blockIdx.x, blockIdx.y);
-}
-
-template <int V, bool X, bool Q, bool K = false>
-__global__ void __launch_bounds__(walk::NTW, 4) k_stress_walk(const __grid_constant__ HalfArgs a)
-{
-  extern __shared__ __align__(128) float sm[];
-  pdl_sync();
-  walk::stress_walk<V, X, Q, K>(a, a.map, sm, blockIdx.x, blockIdx.y);
-}
-
 // Batched launches copy the instance's arguments (less the tensor maps, which
 // TMA reads from global memory) into shared memory once per CTA: the fields are
 // then uniform shared loads that the in-place global stores cannot alias.
@@ -682,37 +436,6 @@ __global__ void __launch_bounds__(NT, 4) k_stress_batch(const HalfArgs *__restri
   });
 }
 
-// walk schedule of the batched launches: the arguments follow the walk's layout
-template <int NF>
-constexpr size_t walk_args_off()
-{
-  return (walk::smem_floats(NF) + 3) / 4 * 4;
-}
-
-template <int V, bool X, bool Q>
-__global__ void __launch_bounds__(walk::NTW, 3) k_velocity_walk_batch(const HalfArgs *__restrict__ inst,
-                                                                      const Work *__restrict__ work, int nwork,
-                                                                      const int *step)
-{
-  extern __shared__ __align__(128) float sm[];
-  for_work(inst, work, nwork, step, [&](const HalfArgs *src, const Work &w) {
-    const HalfArgs *a = stage_args(src, sm, walk_args_off<3>());
-    walk::velocity_walk<V, X, Q, false>(*a, src->map, sm, w.tile % a->tiles_z, w.tile / a->tiles_z);
-  });
-}
-
-template <int V, bool X, bool Q>
-__global__ void __launch_bounds__(walk::NTW, 4) k_stress_walk_batch(const HalfArgs *__restrict__ inst,
-                                                                    const Work *__restrict__ work, int nwork,
-                                                                    const int *step)
-{
-  extern __shared__ __align__(128) float sm[];
-  for_work(inst, work, nwork, step, [&](const HalfArgs *src, const Work &w) {
-    const HalfArgs *a = stage_args(src, sm, walk_args_off<2>());
-    walk::stress_walk<V, X, Q, false>(*a, src->map, sm, w.tile % a->tiles_z, w.tile / a->tiles_z);
-  });
-}
-
 template <typename K>
 cudaError_t set_attr(K kernel, size_t bytes)
 {
@@ -745,18 +468,6 @@ cudaError_t launch_k(K kernel, const HalfArgs &a, int nfields, cudaStream_t st)
   const dim3 gr = grid(a.g, &b.z_base);
   if (gr.x == 0 || gr.y == 0) return cudaSuccess;
   return launch_pdl(kernel, gr, dim3(NT), bytes, st, b);
-}
-
-template <typename K>
-cudaError_t launch_w(K kernel, const HalfArgs &a, int nfields, cudaStream_t st)
-{
-  const size_t bytes = walk::smem_floats(nfields) * sizeof(float);
-  cudaError_t e = set_attr(kernel, bytes);
-  if (e != cudaSuccess) return e;
-  HalfArgs b = a;
-  const dim3 gr = grid(a.g, &b.z_base);
-  if (gr.x == 0 || gr.y == 0) return cudaSuccess;
-  return launch_pdl(kernel, gr, dim3(walk::NTW), bytes, st, b);
 }
 
 }  // namespace
@@ -795,13 +506,6 @@ bool encode_map(CUtensorMap *map, const Grid &g, float *field)
 template <bool X, bool Q>
 cudaError_t velocity_xq(const HalfArgs &a, int variant, cudaStream_t st)
 {
-  if (a.walk) {
-    if (variant == TTI_COORDINATE && a.kd[0])
-      return launch_w(k_velocity_walk<TTI_COORDINATE, X, Q, true>, a, 3, st);
-    if (variant == TTI_COORDINATE) return launch_w(k_velocity_walk<TTI_COORDINATE, X, Q>, a, 3, st);
-    if (variant == TTI_TENSOR) return launch_w(k_velocity_walk<TTI_TENSOR, X, Q>, a, 3, st);
-    return launch_w(k_velocity_walk<TTI_BOND, X, Q>, a, 3, st);
-  }
   if (variant == TTI_COORDINATE && a.kd[0]) return launch_k(k_velocity_tiled<TTI_COORDINATE, X, Q, true>, a, 3, st);
   if (variant == TTI_COORDINATE) return launch_k(k_velocity_tiled<TTI_COORDINATE, X, Q>, a, 3, st);
   if (variant == TTI_TENSOR) return launch_k(k_velocity_tiled<TTI_TENSOR, X, Q>, a, 3, st);
@@ -812,16 +516,6 @@ template <bool X, bool Q>
 cudaError_t stress_xq(const HalfArgs &a, int variant, cudaStream_t st)
 {
   const bool k = a.kd[0] != nullptr;
-  if (a.walk) {
-    if (variant == TTI_COORDINATE)
-      return k ? launch_w(k_stress_walk<TTI_COORDINATE, X, Q, true>, a, 2, st)
-               : launch_w(k_stress_walk<TTI_COORDINATE, X, Q>, a, 2, st);
-    if (variant == TTI_TENSOR)
-      return k ? launch_w(k_stress_walk<TTI_TENSOR, X, Q, true>, a, 2, st)
-               : launch_w(k_stress_walk<TTI_TENSOR, X, Q>, a, 2, st);
-    return k ? launch_w(k_stress_walk<TTI_BOND, X, Q, true>, a, 2, st)
-             : launch_w(k_stress_walk<TTI_BOND, X, Q>, a, 2, st);
-  }
   if (variant == TTI_COORDINATE)
     return k ? launch_k(k_stress_tiled<TTI_COORDINATE, X, Q, true>, a, 2, st)
              : launch_k(k_stress_tiled<TTI_COORDINATE, X, Q>, a, 2, st);
@@ -865,20 +559,9 @@ cudaError_t launch_batch_k(K kernel, const BatchLaunch &l, cudaStream_t st, size
   return cudaGetLastError();
 }
 
-template <int NF, typename K>
-cudaError_t launch_walk_batch_k(K kernel, const BatchLaunch &l, cudaStream_t st)
-{
-  return launch_batch_k(kernel, l, st, walk_args_off<NF>() * sizeof(float) + ARGS_BYTES, walk::NTW);
-}
-
 template <bool X, bool Q>
 cudaError_t velocity_batch_x(const BatchLaunch &l, cudaStream_t st)
 {
-  if (l.walk) {
-    if (l.variant == TTI_COORDINATE) return launch_walk_batch_k<3>(k_velocity_walk_batch<TTI_COORDINATE, X, Q>, l, st);
-    if (l.variant == TTI_TENSOR) return launch_walk_batch_k<3>(k_velocity_walk_batch<TTI_TENSOR, X, Q>, l, st);
-    return launch_walk_batch_k<3>(k_velocity_walk_batch<TTI_BOND, X, Q>, l, st);
-  }
   if (l.variant == TTI_COORDINATE) return launch_batch_k(k_velocity_batch<TTI_COORDINATE, X, Q>, l, st);
   if (l.variant == TTI_TENSOR) return launch_batch_k(k_velocity_batch<TTI_TENSOR, X, Q>, l, st);
   return launch_batch_k(k_velocity_batch<TTI_BOND, X, Q>, l, st);
@@ -887,11 +570,6 @@ cudaError_t velocity_batch_x(const BatchLaunch &l, cudaStream_t st)
 template <bool X, bool Q>
 cudaError_t stress_batch_x(const BatchLaunch &l, cudaStream_t st)
 {
-  if (l.walk) {
-    if (l.variant == TTI_COORDINATE) return launch_walk_batch_k<2>(k_stress_walk_batch<TTI_COORDINATE, X, Q>, l, st);
-    if (l.variant == TTI_TENSOR) return launch_walk_batch_k<2>(k_stress_walk_batch<TTI_TENSOR, X, Q>, l, st);
-    return launch_walk_batch_k<2>(k_stress_walk_batch<TTI_BOND, X, Q>, l, st);
-  }
   if (l.variant == TTI_COORDINATE) return launch_batch_k(k_stress_batch<TTI_COORDINATE, X, Q>, l, st);
   if (l.variant == TTI_TENSOR) return launch_batch_k(k_stress_batch<TTI_TENSOR, X, Q>, l, st);
   return launch_batch_k(k_stress_batch<TTI_BOND, X, Q>, l, st);

@@ -174,7 +174,6 @@ struct tti_handle {
   long long launches = 0;
   cudaEvent_t pev[8] = {};  // phase events for tti_profile_steps
   bool exact = false;
-  bool walk = false;  // walk schedule of the tiled half-step kernels (TTIFD_SCHEDULE=walk at tti_create)
   unsigned wait_limit = 0;  // polls of the tiled kernels' first TMA wait
   std::string err;
 };

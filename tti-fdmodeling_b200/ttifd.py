@@ -430,17 +430,16 @@ class Batch:
         """Shots interleaved per tile in groups of `group` (0: all); graph of `graph_steps` steps (0: none)."""
         self._call("batch_set_order", self._b, group, graph_steps)
 
-    TILE_SCHEDULES = ["row", "walk", "row+persistent", "walk+persistent"]
+    GRIDS = ["per-tile", "persistent"]
 
-    def set_schedule(self, tile_schedule):
-        """Schedule of the half-step kernels: one of TILE_SCHEDULES (or its index)."""
-        ts = self.TILE_SCHEDULES.index(tile_schedule) if isinstance(tile_schedule, str) else tile_schedule
-        self._call("batch_set_schedule", self._b, ts)
+    def set_schedule(self, grid):
+        """Grid of the half-step launches: "per-tile" (0) or "persistent" (1)."""
+        self._call("batch_set_schedule", self._b, self.GRIDS.index(grid) if isinstance(grid, str) else grid)
 
     def schedule(self) -> dict:
-        g, gs, ts = C.c_int(), C.c_int(), C.c_int()
-        self._call("batch_get_schedule", self._b, C.byref(g), C.byref(gs), C.byref(ts))
-        return {"group": g.value, "graph_steps": gs.value, "tile_schedule": self.TILE_SCHEDULES[ts.value]}
+        g, gs, p = C.c_int(), C.c_int(), C.c_int()
+        self._call("batch_get_schedule", self._b, C.byref(g), C.byref(gs), C.byref(p))
+        return {"group": g.value, "graph_steps": gs.value, "grid": self.GRIDS[p.value]}
 
     def autotune(self, nsteps: int) -> dict:
         """Times the schedules on nsteps steps, keeps the fastest, resets the batch."""
