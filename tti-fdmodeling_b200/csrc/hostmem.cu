@@ -17,7 +17,9 @@
 #include <sys/mman.h>
 
 #include <algorithm>
+#include <condition_variable>
 #include <cstring>
+#include <functional>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -53,16 +55,98 @@ void split(size_t n, int nth, F f)
 std::mutex g_pin_mu;
 std::vector<float *> g_pin_free;  // page-locked staging chunks not in use
 
+// Persistent copy workers for parallel_copy: a staged transfer calls it once
+// per 16 MB chunk, and starting fresh threads for every chunk (18 chunks x 8
+// threads for a 1126 x 7872 model) cost several milliseconds of the upload.
+// One job at a time (callers queue on job_mu); the caller takes a share too.
+class CopyPool {
+ public:
+  static CopyPool &get()
+  {
+    static CopyPool *p = new CopyPool();  // never destroyed: workers may outlive static destructors
+    return *p;
+  }
+  // f(i) for i in [0, n), on up to n threads (the caller's included)
+  void run(int n, const std::function<void(int)> &f)
+  {
+    std::lock_guard<std::mutex> job(job_mu_);
+    {
+      std::lock_guard<std::mutex> lock(mu_);
+      f_ = &f;
+      n_ = n;
+      next_ = 1;  // item 0 is the caller's
+      left_ = n - 1;
+      ++gen_;
+    }
+    cv_.notify_all();
+    f(0);
+    std::unique_lock<std::mutex> lock(mu_);
+    for (;;) {  // the caller helps with items no worker has taken yet
+      if (next_ < n_) {
+        const int i = next_++;
+        lock.unlock();
+        f(i);
+        lock.lock();
+        --left_;
+        continue;
+      }
+      if (left_ == 0) break;
+      done_.wait(lock);
+    }
+    f_ = nullptr;
+  }
+  int size() const { return (int)th_.size() + 1; }
+
+ private:
+  CopyPool()
+  {
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    for (int t = 0; t < std::min(15, hw - 1); ++t) th_.emplace_back([this] { loop(); });
+    for (auto &x : th_) x.detach();
+  }
+  void loop()
+  {
+    unsigned long long seen = 0;
+    std::unique_lock<std::mutex> lock(mu_);
+    for (;;) {
+      cv_.wait(lock, [&] { return gen_ != seen && f_ && next_ < n_; });
+      seen = gen_;
+      while (f_ && next_ < n_) {
+        const int i = next_++;
+        const std::function<void(int)> *f = f_;
+        lock.unlock();
+        (*f)(i);
+        lock.lock();
+        if (--left_ == 0) done_.notify_all();
+      }
+    }
+  }
+  std::mutex job_mu_, mu_;
+  std::condition_variable cv_, done_;
+  const std::function<void(int)> *f_ = nullptr;
+  int n_ = 0, next_ = 0, left_ = 0;
+  unsigned long long gen_ = 0;
+  std::vector<std::thread> th_;
+};
+
 }  // namespace
 
 void parallel_copy(void *dst, const void *src, size_t bytes, int max_threads)
 {
-  const size_t hw = std::max(1u, std::thread::hardware_concurrency());
-  const int nth =
-      (int)std::min<size_t>(std::min<size_t>((size_t)std::max(1, max_threads), hw), std::max<size_t>(1, bytes >> 20));
+  CopyPool &pool = CopyPool::get();
+  const int nth = (int)std::min<size_t>(std::min<size_t>((size_t)std::max(1, max_threads), (size_t)pool.size()),
+                                        std::max<size_t>(1, bytes >> 20));
   char *d = static_cast<char *>(dst);
   const char *q = static_cast<const char *>(src);
-  split(bytes, nth, [d, q](size_t b, size_t e) { memcpy(d + b, q + b, e - b); });
+  if (nth <= 1) {
+    memcpy(d, q, bytes);
+    return;
+  }
+  const size_t per = (bytes + nth - 1) / nth;
+  pool.run(nth, [&](int i) {
+    const size_t b = (size_t)i * per, e = std::min(bytes, b + per);
+    if (b < e) memcpy(d + b, q + b, e - b);
+  });
 }
 
 float *pinned_chunk()
