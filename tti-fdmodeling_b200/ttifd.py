@@ -236,14 +236,17 @@ class Modeling:
         self._call("set_receivers", self._h, kind, x.size, _i(x), _i(z))
         self._nrec[kind] = x.size
 
-    def run(self, snapshot=None):
-        """snapshot(it, kind, array[nx_out, nz_out]) -> None, or None."""
+    def run(self, snapshot=None, copy=True):
+        """snapshot(it, kind, array[nx_out, nz_out]) -> None, or None. With
+        copy=False the array is a view of the library's host buffer, valid only
+        during the call (as for a C callback: write it out or copy it there)."""
         if snapshot is None:
             cb = SNAP_FN()
         else:
             def _cb(user, it, kind, data, nzo, nxo):
                 try:
-                    arr = _copy(np.ctypeslib.as_array(data, shape=(nxo, nzo)))
+                    view = np.ctypeslib.as_array(data, shape=(nxo, nzo))
+                    arr = _copy(view) if copy else view
                     snapshot(it, kind, arr)
                     return 0
                 except Exception:  # abort the run
