@@ -7,7 +7,8 @@ namespace ttifd {
 
 // ---------------- setup ----------------
 struct SetupIn {
-  const float *vp, *vs, *rho, *eps, *delta, *theta;  // padded raw model
+  const float *vp, *vs, *rho, *eps, *delta, *theta;  // padded raw model, [Nx][pitch]
+  int pitch;                                         // floats per column (Nz: as uploaded)
 };
 struct SetupOut {
   float *D, *Beta, *coef1, *coef2, *vp, *vs, *rho, *invrho;

@@ -35,9 +35,10 @@ __global__ void k_setup_cell(Grid g, SetupIn in, SetupOut out, MealConst mc, int
   const int iz = blockIdx.x * blockDim.x + threadIdx.x;
   const int ix = blockIdx.y;
   if (iz >= g.Nz || ix >= g.Nx) return;
-  const size_t i = (size_t)ix * g.ldz + iz;
+  const size_t i = (size_t)ix * g.ldz + iz;       // outputs
+  const size_t ri = (size_t)ix * in.pitch + iz;  // the raw model
   const int nl = g.E;
-  float vp = in.vp[i], vs = in.vs[i], rho = in.rho[i];
+  float vp = in.vp[ri], vs = in.vs[ri], rho = in.rho[ri];
 
   // ---- MEAL profile
   const float Vs = vs == 0.0f ? fd(vp, mc.sqrt3) : vs;
@@ -83,13 +84,13 @@ __global__ void k_setup_cell(Grid g, SetupIn in, SetupOut out, MealConst mc, int
   const float q = fd(vs, vp);
   const double f = ds(1.0, dm((double)q, (double)q));
   const float rvv = fm(fm(rho, vp), vp);
-  const double C11 = dm((double)rvv, da(1.0, dm(2.0, (double)in.eps[i])));
+  const double C11 = dm((double)rvv, da(1.0, dm(2.0, (double)in.eps[ri])));
   const double C13 =
-      dm((double)rho, ds(dm((double)fm(vp, vp), __dsqrt_rn(dm(f, da(f, dm(2.0, (double)in.delta[i]))))),
+      dm((double)rho, ds(dm((double)fm(vp, vp), __dsqrt_rn(dm(f, da(f, dm(2.0, (double)in.delta[ri]))))),
                          (double)fm(vs, vs)));
   const float c33f = rvv;
   const float c55f = fm(fm(rho, vs), vs);
-  const float th = f2(dm(dd((double)fm(scalar, in.theta[i]), 180.0), kPi));
+  const float th = f2(dm(dd((double)fm(scalar, in.theta[ri]), 180.0), kPi));
   const double thd = (double)th;
   if (variant == TTI_BOND) {
     const double C33 = (double)c33f, C55 = (double)c55f;
