@@ -231,44 +231,70 @@ def measure_plain(variant, K, W, nprof, rank, world, local_rank, clock_window_s=
             "launches": launches, "roofline": roof, "clocks": clk.summary()}
 
 
-def measure_e2e(variant, K, rank, world, local_rank):
+SNAP_KINDS = {0: 0, 1: 2, 2: 1, 3: 3, 4: 2, 5: 2}  # wsave -> snapshot kinds per snapshot step
+
+
+def measure_e2e(variant, K, rank, world, local_rank, reps=3):
     """The whole public-API sequence from host buffers: create, upload +
     device precompute, geometry, K steps with snapshots delivered to the host,
-    traces fetched, destroy (wall clock, max over ranks)."""
+    traces fetched, destroy (wall clock, max over ranks). The model, trace and
+    snapshot buffers are page-locked host arrays (tti_host_alloc), allocated
+    and filled once outside the timed region, as a service that models shot
+    after shot keeps them; every copy between them and the device is inside
+    it. One untimed pass, then `reps` timed passes; the median pass is
+    reported (all walls listed)."""
     import ttifd
 
     m = model()
     pads = synthetic.padded(m, WORKLOAD["ealThick"])
+    pinned = [ttifd.host_empty(a.shape) for a in pads]
+    for d, a in zip(pinned, pads):
+        d[...] = a
     sx, sz, gx, gz = geometry(rank)
     cfg_e = dict(WORKLOAD, variant=variant, nt=K)
     wav_e = synthetic.ricker(K, cfg_e["dt"], cfg_e["fpeak"])
-    dist_barrier()
-    phases = {}
-    t0 = time.perf_counter()
-    with ttifd.Modeling(device=local_rank, **cfg_e) as he:
-        phases["create"] = time.perf_counter() - t0
-        he.upload_model(*pads)
-        phases["upload"] = time.perf_counter() - t0 - sum(phases.values())
-        he.set_source([sx], [sz], wav_e[None, :])
-        for k in (0, 1, 2):
-            he.set_receivers(k, gx, gz)
-        phases["geometry"] = time.perf_counter() - t0 - sum(phases.values())
+    nts = (K - 1) // cfg_e["mt"] + 1
+    trace_out = [ttifd.host_empty((gx.size, nts)) for _ in range(3)]
+    pad = 0 if WORKLOAD["savew"] == 0 else 2 * (WORKLOAD["ealThick"] + 5)  # savew = 0: the physical area
+    nk = SNAP_KINDS[WORKLOAD["wsave"]]
+    snap_buf = ttifd.host_empty(nk * (WORKLOAD["nz"] + pad) * (WORKLOAD["nx"] + pad)) if nk else None
+
+    def one():
+        dist_barrier()
+        phases = {}
         snaps = []
-        # the snapshot reaches host memory; the callback sees the library's buffer
-        # (as a C caller's callback does) and takes its size
-        he.run(lambda it, kind, a: snaps.append(a.nbytes), copy=False)
-        phases["run"] = time.perf_counter() - t0 - sum(phases.values())
-        trs = [he.fetch_traces(k) for k in (0, 1, 2)]
-        phases["fetch"] = time.perf_counter() - t0 - sum(phases.values())
-        cells = he.Nz * he.Nx
-    t_e2e = dist_max(time.perf_counter() - t0)
-    phases["destroy"] = t_e2e - sum(phases.values())
+        t0 = time.perf_counter()
+        with ttifd.Modeling(device=local_rank, **cfg_e) as he:
+            phases["create"] = time.perf_counter() - t0
+            he.upload_model(*pinned)
+            phases["upload"] = time.perf_counter() - t0 - sum(phases.values())
+            he.set_source([sx], [sz], wav_e[None, :])
+            for k in (0, 1, 2):
+                he.set_receivers(k, gx, gz)
+            if snap_buf is not None:
+                he.set_snapshot_buffer(snap_buf)
+            phases["geometry"] = time.perf_counter() - t0 - sum(phases.values())
+            # the snapshot reaches host memory; the callback sees it in place
+            # (as a C caller's callback does) and takes its size
+            he.run(lambda it, kind, a: snaps.append(a.nbytes), copy=False)
+            phases["run"] = time.perf_counter() - t0 - sum(phases.values())
+            trs = [he.fetch_traces(k, out=trace_out[k]) for k in (0, 1, 2)]
+            phases["fetch"] = time.perf_counter() - t0 - sum(phases.values())
+            cells = he.Nz * he.Nx
+        t = dist_max(time.perf_counter() - t0)
+        phases["destroy"] = t - sum(phases.values())
+        d2h = sum(snaps) + sum(x.nbytes for x in trs)
+        return t, phases, cells, d2h
+
+    one()  # untimed: first use of the snapshot and transpose kernels in the process
+    runs = sorted((one() for _ in range(reps)), key=lambda r: r[0])
+    t_e2e, phases, cells, d2h = runs[len(runs) // 2]
     h2d = sum(a.nbytes for a in pads) + wav_e.nbytes + 3 * 2 * gx.nbytes
-    d2h = sum(snaps) + sum(t.nbytes for t in trs)
     return {"value": cells * K * world / t_e2e / 1e9, "unit": "Gcell/s", "h2d_bytes_per_step": h2d / K,
-            "d2h_bytes_per_step": d2h / K, "wall_s": t_e2e, "phases_s": phases,
+            "d2h_bytes_per_step": d2h / K, "wall_s": t_e2e, "walls_s": [r[0] for r in runs], "phases_s": phases,
+            "host_buffers": "page-locked (tti_host_alloc), allocated once outside the timed region",
             "includes": "tti_create..tti_destroy: model upload + device precompute, geometry, K steps, "
-                        "snapshots to host, traces"}
+                        "snapshots to host, traces; median of %d passes after one untimed pass" % reps}
 
 
 def run_ours(args, rank, world, local_rank):

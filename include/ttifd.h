@@ -148,6 +148,28 @@ int tti_set_receivers(tti_handle *h, int kind, int ntrace, const int *posx, cons
 /* Runs the whole time loop (coord:611-926): zero wavefields, nt steps,
  * snapshots through `snap` (may be NULL), receivers, energy. */
 int tti_run(tti_handle *h, tti_snapshot_fn snap, void *user);
+/* Page-locked host memory for the caller's arrays (no counterpart in the
+ * reference, which keeps everything in host memory). tti_upload_model from
+ * six such arrays, tti_fetch_traces into one and tti_run's snapshots into a
+ * buffer given to tti_set_snapshot_buffer move in one copy each at the host
+ * link's rate; with pageable arrays the library stages those copies through
+ * its own page-locked chunks. Page-locking is slow (about 0.4 ms per MB): take
+ * the buffers once and reuse them shot after shot. tti_host_free releases a
+ * buffer of tti_host_alloc (TTI_ERR_ARG for any other pointer). */
+int tti_host_alloc(size_t bytes, void **ptr);
+int tti_host_free(void *ptr);
+/* Host buffer of `floats` floats into which tti_run delivers its snapshots
+ * (NULL: the library's own buffer), kind q of a snapshot step at q x nz_out x
+ * nx_out, so it needs (kinds of wsave) x nz_out x nx_out floats (TTI_ERR_ARG
+ * when smaller, TTI_ERR_STATE when wsave writes none). When it is page-locked
+ * (tti_host_alloc) the copy of a snapshot to the host runs on a second stream
+ * while the time steps go on, and the callbacks of a snapshot step run later:
+ * at the next snapshot step or at the end of tti_run, in step order, with
+ * `data` pointing into this buffer (valid until the callback returns). A
+ * nonzero return still ends the run with TTI_ERR_CALLBACK. With a pageable
+ * buffer snapshots are delivered at their step, as without one. The buffer
+ * must outlive every tti_run of h that uses it. */
+int tti_set_snapshot_buffer(tti_handle *h, float *host, size_t floats);
 /* Lower-level stepping: zero the wavefields / advance `nsteps` steps from the
  * current step index without snapshots. tti_run = reset + all steps. */
 int tti_reset(tti_handle *h);

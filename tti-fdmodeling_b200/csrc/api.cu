@@ -280,35 +280,111 @@ int download(tti_handle *h, void *dst, const void *src, size_t bytes)
   return TTI_OK;
 }
 
-int do_snapshot(tti_handle *h, tti_snapshot_fn fn, void *user, int it)
+// Output size of one snapshot kind (savew = 0: the physical area).
+void snapshot_dims(const tti_handle *h, int *nzo, int *nxo)
 {
   const Grid &g = h->g;
-  const int nzo = h->cfg.savew == 0 ? g.Nz - 2 * g.E : g.Nz;
-  const int nxo = h->cfg.savew == 0 ? g.Nx - 2 * g.E : g.Nx;
+  *nzo = h->cfg.savew == 0 ? g.Nz - 2 * g.E : g.Nz;
+  *nxo = h->cfg.savew == 0 ? g.Nx - 2 * g.E : g.Nx;
+}
+
+// The snapshot of step h->snap_it whose copy into the caller's page-locked
+// buffer is in flight on copy_stream: waits for the copy, then (deliver) runs
+// the callbacks of its kinds in order. Error paths drop it once the copy is
+// done, so that no transfer into the caller's buffer outlives tti_run.
+int finish_snapshot(tti_handle *h, bool deliver)
+{
+  if (!h->snap_pending) return TTI_OK;
+  h->snap_pending = false;
+  const cudaError_t e = cudaEventSynchronize(h->snap_done);
+  if (!deliver) return TTI_OK;
+  CK(h, e);
+  int nzo, nxo, kinds[3];
+  snapshot_dims(h, &nzo, &nxo);
   const size_t n = (size_t)nzo * nxo;
-  if (h->snap_cap < n) {
+  const int nk = snapshot_kinds(h->cfg.wsave, kinds);
+  for (int q = 0; q < nk; ++q)
+    if (h->snap_fn(h->snap_arg, h->snap_it, kinds[q], h->snap_user + q * n, nzo, nxo) != 0)
+      return set_err(h, TTI_ERR_CALLBACK, "snapshot callback aborted the run at it=%d", h->snap_it);
+  return TTI_OK;
+}
+
+int do_snapshot(tti_handle *h, tti_snapshot_fn fn, void *user, int it)
+{
+  int nzo, nxo, kinds[3];
+  snapshot_dims(h, &nzo, &nxo);
+  const size_t n = (size_t)nzo * nxo;
+  const int nk = snapshot_kinds(h->cfg.wsave, kinds);
+  // Into the caller's page-locked buffer: every kind packed on the device, one
+  // copy on copy_stream that overlaps the next time steps on h->stream.
+  const bool overlap = h->snap_user && h->snap_user_pinned;
+  const size_t dev = overlap ? nk * n : n;
+  if (overlap) {
+    const int rc = finish_snapshot(h, true);  // the previous one, and d_snap is free again
+    if (rc) return rc;
+  }
+  if (h->snap_cap < dev) {
     pool_free(h->d_snap, h->stream);
-    free(h->h_snap);
     h->d_snap = nullptr;
-    h->h_snap = nullptr;
     h->snap_cap = 0;
-    CK(h, pool_alloc(reinterpret_cast<void **>(&h->d_snap), n * sizeof(float), h->stream));
+    CK(h, pool_alloc(reinterpret_cast<void **>(&h->d_snap), dev * sizeof(float), h->stream));
+    h->snap_cap = dev;
+  }
+  StepArgs a = step_args(h);
+  if (overlap) {
+    if (!h->copy_stream) CK(h, cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+    if (!h->snap_packed) CK(h, cudaEventCreateWithFlags(&h->snap_packed, cudaEventDisableTiming));
+    if (!h->snap_done) CK(h, cudaEventCreateWithFlags(&h->snap_done, cudaEventDisableTiming));
+    for (int q = 0; q < nk; ++q) {
+      launch_snapshot(a, kinds[q], h->cfg.savew, h->d_snap + q * n, h->stream);
+      h->launches++;
+    }
+    CK(h, cudaEventRecord(h->snap_packed, h->stream));
+    CK(h, cudaStreamWaitEvent(h->copy_stream, h->snap_packed, 0));
+    CK(h, cudaMemcpyAsync(h->snap_user, h->d_snap, nk * n * sizeof(float), cudaMemcpyDeviceToHost, h->copy_stream));
+    CK(h, cudaEventRecord(h->snap_done, h->copy_stream));
+    h->snap_pending = true;
+    h->snap_it = it;
+    h->snap_fn = fn;
+    h->snap_arg = user;
+    return TTI_OK;
+  }
+  float *host = h->snap_user;  // a pageable caller's buffer: kind q at q * n
+  if (!host && h->h_snap_cap < n) {
+    free(h->h_snap);
+    h->h_snap_cap = 0;
     h->h_snap = static_cast<float *>(malloc(n * sizeof(float)));
     if (!h->h_snap) return set_err(h, TTI_ERR_NOMEM, "host allocation of the snapshot buffer failed");
     prefault(h->h_snap, n * sizeof(float));
-    h->snap_cap = n;
+    h->h_snap_cap = n;
   }
-  int kinds[3];
-  const int nk = snapshot_kinds(h->cfg.wsave, kinds);
-  StepArgs a = step_args(h);
   for (int q = 0; q < nk; ++q) {
+    float *dst = host ? host + q * n : h->h_snap;
     launch_snapshot(a, kinds[q], h->cfg.savew, h->d_snap, h->stream);
     h->launches++;
-    const int rc = download(h, h->h_snap, h->d_snap, n * sizeof(float));
+    const int rc = download(h, dst, h->d_snap, n * sizeof(float));
     if (rc) return rc;
-    if (fn(user, it, kinds[q], h->h_snap, nzo, nxo) != 0)
+    if (fn(user, it, kinds[q], dst, nzo, nxo) != 0)
       return set_err(h, TTI_ERR_CALLBACK, "snapshot callback aborted the run at it=%d", it);
   }
+  return TTI_OK;
+}
+
+// The time loop of tti_run after the reset; device time between events
+// ev0 and ev1. A snapshot of the last snapshot step may still be in flight.
+int run_steps(tti_handle *h, const SourceTables &tab, tti_snapshot_fn snap, void *user)
+{
+  const tti_config &c = h->cfg;
+  CK(h, cudaEventRecord(h->ev0, h->stream));
+  for (int n = 0; n < c.nt; ++n) {
+    const int it = current_it(h);
+    int rc = launch_one_step(h, tab);
+    if (rc == TTI_OK && snap && c.wsave > 0 && it % c.snap_sample == 0) rc = do_snapshot(h, snap, user, it);
+    if (rc) return rc;
+  }
+  CK(h, cudaEventRecord(h->ev1, h->stream));
+  CK(h, cudaEventSynchronize(h->ev1));
+  CK(h, cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
   return TTI_OK;
 }
 
@@ -325,7 +401,8 @@ int check_flag(tti_handle *h)
 // Copies na host arrays [Nx][Nz] into dense device arrays [Nx][Nz] on h's
 // stream (dense, not pitched: a contiguous host-to-device copy runs about 1.5x
 // faster than a pitched one of the same bytes; the setup kernel re-pitches).
-// Through two page-locked chunks, column blocks at a time: host threads copy
+// From page-locked arrays (tti_host_alloc) one copy each, at the link's rate.
+// Otherwise through two page-locked chunks, column blocks at a time: host threads copy
 // block c into one chunk while the DMA engine moves block c - 1 from the other
 // (TTIFD_UPLOAD=pageable: straight from the caller's pageable arrays, which
 // the driver stages itself, about 10.5 GB/s on B200 hosts).
@@ -333,6 +410,13 @@ int upload_arrays(tti_handle *h, const float *const *src, float *const *dst, int
 {
   const Grid &g = h->g;
   const size_t col = (size_t)g.Nz * sizeof(float);
+  bool pinned = true;  // all from page-locked memory: straight to the device
+  for (int k = 0; k < na; ++k) pinned = pinned && is_pinned(src[k]);
+  if (pinned) {
+    for (int k = 0; k < na; ++k)
+      CK(h, cudaMemcpyAsync(dst[k], src[k], col * g.Nx, cudaMemcpyHostToDevice, h->stream));
+    return TTI_OK;
+  }
   const char *mode = getenv("TTIFD_UPLOAD");
   const bool pageable = mode && strcmp(mode, "pageable") == 0;
   const int per = (int)std::min<size_t>(g.Nx, PIN_CHUNK / g.Nz);  // columns per chunk
@@ -578,6 +662,9 @@ int tti_destroy(tti_handle *h)
   free(h->tmaps);
   for (auto e : h->pev)
     if (e) cudaEventDestroy(e);
+  if (h->snap_packed) cudaEventDestroy(h->snap_packed);
+  if (h->snap_done) cudaEventDestroy(h->snap_done);
+  if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return TTI_OK;
@@ -848,6 +935,23 @@ int tti_step(tti_handle *h, int nsteps)
   return check_flag(h);
 }
 
+int tti_set_snapshot_buffer(tti_handle *h, float *host, size_t floats)
+{
+  if (!h) return TTI_ERR_ARG;
+  if (host) {
+    int nzo, nxo, kinds[3];
+    snapshot_dims(h, &nzo, &nxo);
+    const size_t need = (size_t)snapshot_kinds(h->cfg.wsave, kinds) * nzo * nxo;
+    if (need == 0) return set_err(h, TTI_ERR_STATE, "wsave = %d writes no snapshots", h->cfg.wsave);
+    if (floats < need)
+      return set_err(h, TTI_ERR_ARG, "snapshot buffer of %zu floats, wsave = %d needs %zu", floats, h->cfg.wsave,
+                     need);
+  }
+  h->snap_user = host;
+  h->snap_user_pinned = host && is_pinned(host);
+  return TTI_OK;
+}
+
 int tti_run(tti_handle *h, tti_snapshot_fn snap, void *user)
 {
   if (!h) return TTI_ERR_ARG;
@@ -856,17 +960,12 @@ int tti_run(tti_handle *h, tti_snapshot_fn snap, void *user)
   if (rc) return rc;
   SourceTables tab;
   source_tables(h, &tab);
-  const tti_config &c = h->cfg;
-  CK(h, cudaEventRecord(h->ev0, h->stream));
-  for (int n = 0; n < c.nt; ++n) {
-    const int it = current_it(h);
-    if ((rc = launch_one_step(h, tab))) return rc;
-    if (snap && c.wsave > 0 && it % c.snap_sample == 0)
-      if ((rc = do_snapshot(h, snap, user, it))) return rc;
+  rc = run_steps(h, tab, snap, user);
+  if (rc) {
+    finish_snapshot(h, false);
+    return rc;
   }
-  CK(h, cudaEventRecord(h->ev1, h->stream));
-  CK(h, cudaEventSynchronize(h->ev1));
-  CK(h, cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
+  if ((rc = finish_snapshot(h, true))) return rc;
   return check_flag(h);
 }
 
@@ -932,6 +1031,19 @@ int tti_fetch_traces(tti_handle *h, int kind, float *out)
     return set_err(h, TTI_ERR_ARG, "trace of %d samples is longer than the fetch supports", nts);
   const int per = (int)std::max<size_t>(1, STAGE / (size_t)nts);  // receivers per chunk
   const int nchunk = (n + per - 1) / per;
+  if (is_pinned(out)) {
+    // page-locked destination: each chunk's copy runs asynchronously, and the
+    // next transpose into the staging buffer waits for it in stream order
+    for (int r0 = 0; r0 < n; r0 += per) {
+      const int nr = std::min(per, n - r0);
+      launch_transpose(h->d_rec[kind], h->d_stage, nts, n, r0, nr, h->stream);
+      h->launches++;
+      CK(h, cudaMemcpyAsync(out + (size_t)r0 * nts, h->d_stage, sizeof(float) * (size_t)nr * nts,
+                            cudaMemcpyDeviceToHost, h->stream));
+    }
+    CK(h, cudaStreamSynchronize(h->stream));
+    return TTI_OK;
+  }
   // A fetch of one chunk goes straight to the caller's block: staging would
   // not overlap anything, and the first staged fetch of a process pays for
   // page-locking the chunks (about 13 ms for two).

@@ -173,6 +173,16 @@ void pinned_release(float *p)
   g_pin_free.push_back(p);
 }
 
+bool is_pinned(const void *p)
+{
+  cudaPointerAttributes at;
+  if (!p || cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();  // a failed query leaves nothing behind
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost;
+}
+
 void prefault(void *p, size_t bytes)
 {
   if (!p || bytes == 0) return;
@@ -212,3 +222,32 @@ float host_max(const float *a, size_t n, float init)
 }
 
 }  // namespace ttifd
+
+extern "C" {
+
+int tti_host_alloc(size_t bytes, void **ptr)
+{
+  if (!ptr) return TTI_ERR_ARG;
+  *ptr = nullptr;
+  if (bytes == 0) return TTI_ERR_ARG;
+  // portable: the buffer serves handles on any device of the process
+  if (cudaHostAlloc(ptr, bytes, cudaHostAllocPortable) != cudaSuccess) {
+    cudaGetLastError();
+    *ptr = nullptr;
+    return TTI_ERR_NOMEM;
+  }
+  return TTI_OK;
+}
+
+int tti_host_free(void *ptr)
+{
+  if (!ptr) return TTI_OK;
+  if (!ttifd::is_pinned(ptr)) return TTI_ERR_ARG;
+  if (cudaFreeHost(ptr) != cudaSuccess) {
+    cudaGetLastError();
+    return TTI_ERR_CUDA;
+  }
+  return TTI_OK;
+}
+
+}  // extern "C"

@@ -115,6 +115,8 @@ void pool_free(void *p, cudaStream_t st);
 // several threads before a pageable device-to-host copy; the maximum of n
 // floats (NaN entries ignored, as fmaxf does) from several threads.
 void prefault(void *p, size_t bytes);
+// true for page-locked host memory known to CUDA (cudaHostAlloc, cudaHostRegister)
+bool is_pinned(const void *p);
 float host_max(const float *a, size_t n, float init);
 // memcpy from up to max_threads host threads (1 MiB or more each). Into fresh
 // pageable memory 16 threads help (they take the page faults in parallel);
@@ -164,10 +166,21 @@ struct tti_handle {
   int nts = 0;
   double *d_energy = nullptr;  // [nt][2]
   int *d_flag = nullptr;       // nonfinite watchdog
-  float *d_snap = nullptr;
-  float *h_snap = nullptr;     // snapshot handed to the callback (pageable, faulted in once)
-  float *d_stage = nullptr;    // trace fetch: device chunk of transposed traces
-  size_t snap_cap = 0;
+  float *d_snap = nullptr;      // packed snapshot kinds of one step, snap_cap floats
+  float *h_snap = nullptr;      // snapshot handed to the callback (pageable, faulted in once), h_snap_cap floats
+  float *d_stage = nullptr;     // trace fetch: device chunk of transposed traces
+  size_t snap_cap = 0, h_snap_cap = 0;
+  // caller's snapshot buffer (tti_set_snapshot_buffer); when page-locked the
+  // copy runs on copy_stream and the callbacks of snapshot step snap_it follow
+  // at the next snapshot step or at the end of tti_run
+  float *snap_user = nullptr;
+  bool snap_user_pinned = false;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t snap_packed = nullptr, snap_done = nullptr;
+  bool snap_pending = false;
+  int snap_it = 0;
+  tti_snapshot_fn snap_fn = nullptr;
+  void *snap_arg = nullptr;
   bool have_model = false;
   int step_index = 0;
   float last_ms = 0.0f;
