@@ -684,19 +684,40 @@ __global__ void __launch_bounds__(tiled::NT, 3) k_adj_velocity_tiled(const __gri
   }
 }
 
+// TMA boxes of the TV pair p (components sxx, szz, sxz) into shared buffers
+// 2b, 2b + 1, completing on barrier p; called by one thread.
+__device__ __forceinline__ void issue_tv_pair(const AdjTile &at, float *sm, unsigned long long *bar, int p, int b,
+                                              const TileCells &c)
+{
+  constexpr unsigned BOX_BYTES = tiled::BX * tiled::BZ * 4;
+  tiled::tma::mbar_arrive_expect_tx(bar + p, 2 * BOX_BYTES);
+  for (int k = 0; k < 2; ++k)
+    tiled::tma::tma_load_2d(sm + (2 * b + k) * tiled::FIELD, at.map + 2 * p + k, c.z0 - 8, c.x0 - 5, bar + p);
+}
+
 // transposed velocity stencils into lambda_sigma (maps: TV0..TV5), rows from
-// z_lo. The boxes arrive in three pairs (sxx: TV0 TV1, szz: TV2 TV3, sxz: TV4
-// TV5), each component computed as soon as its pair has landed.
-__global__ void __launch_bounds__(tiled::NT, 2) k_adj_vstencil_tiled(const __grid_constant__ AdjTile at)
+// z_lo. The boxes come in three pairs (sxx: TV0 TV1, szz: TV2 TV3, sxz: TV4
+// TV5) through two pair buffers: pairs 0 and 1 are in flight from the start,
+// and pair 2 goes into pair 0's buffer once every thread is done with it. Four
+// boxes (58 KB) instead of six let three CTAs share an SM.
+__global__ void __launch_bounds__(tiled::NT, 3) k_adj_vstencil_tiled(const __grid_constant__ AdjTile at)
 {
   pdl_sync();
   constexpr int F = tiled::FIELD, B = tiled::BZ;
   extern __shared__ __align__(128) float sm[];
-  unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm + 6 * F);
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm + 4 * F);
   const AdjArgs &a = at.a;
   const Grid &g = a.g;
   const TileCells c = tile_cells(at.z_base);
-  tiled::tma::issue_groups(at.map, sm, bar, 3, 2, c.z0, c.x0, 5);
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < 3; ++q) tiled::tma::mbar_init(bar + q, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    issue_tv_pair(at, sm, bar, 0, 0, c);
+    issue_tv_pair(at, sm, bar, 1, 1, c);
+  }
   const int z = c.z;
   const bool zin = z >= a.z_lo && z < g.Nz - NH;
   // this row's lambda_sigma, loaded while the halo boxes are in flight
@@ -713,15 +734,25 @@ __global__ void __launch_bounds__(tiled::NT, 2) k_adj_vstencil_tiled(const __gri
   }
 #pragma unroll
   for (int q = 0; q < 3; ++q) {
-    if (!tiled::tma::wait_group(at.err, bar, q, 3)) return;
-    if (!zin) continue;
+    if (q == 1) {
+      // every thread is done with pair 0's buffer: pair 2 goes there while pair 1 is used
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        issue_tv_pair(at, sm, bar, 2, 0, c);
+      }
+    }
+    // on a timeout the pairs still in flight get a bounded drain: q .. 1 before pair 2 is issued, q .. 2 after
+    if (!tiled::tma::wait_group(at.err, bar, q, q == 0 ? 2 : 3)) return;
+    if (zin) {
 #pragma unroll
-    for (int j = 0; j < NJ; ++j) {
-      const float *p = sm + (c.xc + j - c.x0 + 5) * B + (z - c.z0 + 8) + 2 * q * F;
-      float d1, d2, u;
-      spair(p, d1, u);
-      spair(p + F, u, d2);
-      l[j][q] -= d1 + d2;
+      for (int j = 0; j < NJ; ++j) {
+        const float *p = sm + (c.xc + j - c.x0 + 5) * B + (z - c.z0 + 8) + 2 * (q & 1) * F;
+        float d1, d2, u;
+        spair(p, d1, u);
+        spair(p + F, u, d2);
+        l[j][q] -= d1 + d2;
+      }
     }
   }
   if (!zin) return;
@@ -1182,7 +1213,7 @@ int adjoint_step(tti_handle *h, int n, int slot, const SourceTables &tab)
     else  // tensor and Bond: no rotation at the velocity node
       GCK(h, launch_adj_tile(k_adj_velocity_tiled<TTI_BOND>, at, 4, g.izStart, g, h->stream));
     for (int k = 0; k < 6; ++k) at.map[k] = s->maps[4 + k];
-    GCK(h, launch_adj_tile(k_adj_vstencil_tiled, at, 6, a.z_lo, g, h->stream));
+    GCK(h, launch_adj_tile(k_adj_vstencil_tiled, at, 4, a.z_lo, g, h->stream));
     return TTI_OK;
   }
   const dim3 blk(BZ, BX), grd((g.Nz + BZ - 1) / BZ, (g.Nx + BX - 1) / BX);
