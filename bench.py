@@ -762,8 +762,10 @@ def main():
         line["batched_uneven"] = run_batched_uneven(args, local_rank)
     if not args.no_grad and world == 1:
         line["gradient"] = run_gradient(args, local_rank)
-        line["gradient_shots"] = run_gradient_shots(args, local_rank)
-        line["gradient_batched_full"] = run_gradient_full(args, local_rank)
+        if args.grad_shots > 0:
+            line["gradient_shots"] = run_gradient_shots(args, local_rank)
+        if args.grad_full_shots > 0:
+            line["gradient_batched_full"] = run_gradient_full(args, local_rank)
     if rank == 0:
         if not args.no_cpu_baseline:
             try:

@@ -635,12 +635,8 @@ int tti_destroy(tti_handle *h)
     pool_free(h->pk_c4, fs);
   }
   for (int k = 0; k < 3; ++k) {
-    pool_free(h->d_rx[k], fs);
-    pool_free(h->d_rz[k], fs);
+    pool_free(h->d_rz[k], fs);  // with d_rzs, d_rid, d_rcol (one block)
     pool_free(h->d_rec[k], fs);
-    pool_free(h->d_rcol[k], fs);
-    pool_free(h->d_rzs[k], fs);
-    pool_free(h->d_rid[k], fs);
   }
   pool_free(h->d_sx, fs);
   pool_free(h->d_sz, fs);
@@ -854,50 +850,42 @@ int tti_set_receivers(tti_handle *h, int kind, int ntrace, const int *posx, cons
                      posx[i], c.nx);
   }
   CK(h, cudaSetDevice(h->device));
-  pool_free(h->d_rx[kind], h->stream);
+  // One device block per component holds its receiver rows in the caller's
+  // order (d_rz, owner of the block), then, grouped by padded-grid column for
+  // the column pass (k_post), the rows (d_rzs), the receiver ids (d_rid) and
+  // the column offsets (d_rcol): one copy and one synchronisation per call.
   pool_free(h->d_rz[kind], h->stream);
   pool_free(h->d_rec[kind], h->stream);
-  h->d_rx[kind] = h->d_rz[kind] = nullptr;
+  h->d_rz[kind] = h->d_rzs[kind] = h->d_rid[kind] = h->d_rcol[kind] = nullptr;
   h->d_rec[kind] = nullptr;
   h->nrec[kind] = 0;
   if (ntrace == 0) return TTI_OK;
-  std::vector<int> x(ntrace), z(ntrace);
+  const int Nx = h->g.Nx;
+  std::vector<int> blk(3 * (size_t)ntrace + Nx + 1, 0), x(ntrace), order(ntrace);
+  int *z = blk.data(), *zs = z + ntrace, *ids = zs + ntrace, *colptr = ids + ntrace;
   for (int i = 0; i < ntrace; ++i) {
     x[i] = posx[i] + h->g.E;
     z[i] = posz[i] + h->g.E;
   }
-  CK(h, pool_alloc(reinterpret_cast<void **>(&h->d_rx[kind]), sizeof(int) * ntrace, h->stream));
-  CK(h, pool_alloc(reinterpret_cast<void **>(&h->d_rz[kind]), sizeof(int) * ntrace, h->stream));
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return x[a] < x[b]; });
+  for (int i = 0; i < ntrace; ++i) colptr[x[i] + 1]++;
+  for (int c = 0; c < Nx; ++c) colptr[c + 1] += colptr[c];
+  for (int i = 0; i < ntrace; ++i) {
+    zs[i] = z[order[i]];
+    ids[i] = order[i];
+  }
+  int *d = nullptr;
+  CK(h, pool_alloc(reinterpret_cast<void **>(&d), sizeof(int) * blk.size(), h->stream));
+  h->d_rz[kind] = d;
+  h->d_rzs[kind] = d + ntrace;
+  h->d_rid[kind] = d + 2 * (size_t)ntrace;
+  h->d_rcol[kind] = d + 3 * (size_t)ntrace;
   // the traces (ntrace x nts floats, the largest of these) from the handle's pool
   CK(h, pool_alloc(reinterpret_cast<void **>(&h->d_rec[kind]), sizeof(float) * (size_t)ntrace * h->nts, h->stream));
-  CK(h, cudaMemcpyAsync(h->d_rx[kind], x.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice, h->stream));
-  CK(h, cudaMemcpyAsync(h->d_rz[kind], z.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemcpyAsync(d, blk.data(), sizeof(int) * blk.size(), cudaMemcpyHostToDevice, h->stream));
   CK(h, cudaMemsetAsync(h->d_rec[kind], 0, sizeof(float) * (size_t)ntrace * h->nts, h->stream));
-  CK(h, cudaStreamSynchronize(h->stream));
-  // receivers grouped by padded-grid column for the column pass (k_post)
-  {
-    const int Nx = h->g.Nx;
-    std::vector<int> order(ntrace), colptr(Nx + 1, 0), zs(ntrace), ids(ntrace);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return x[a] < x[b]; });
-    for (int i = 0; i < ntrace; ++i) colptr[x[i] + 1]++;
-    for (int c = 0; c < Nx; ++c) colptr[c + 1] += colptr[c];
-    for (int i = 0; i < ntrace; ++i) {
-      zs[i] = z[order[i]];
-      ids[i] = order[i];
-    }
-    pool_free(h->d_rcol[kind], h->stream);
-    pool_free(h->d_rzs[kind], h->stream);
-    pool_free(h->d_rid[kind], h->stream);
-    h->d_rcol[kind] = h->d_rzs[kind] = h->d_rid[kind] = nullptr;
-    CK(h, pool_alloc(reinterpret_cast<void **>(&h->d_rcol[kind]), sizeof(int) * (Nx + 1), h->stream));
-    CK(h, pool_alloc(reinterpret_cast<void **>(&h->d_rzs[kind]), sizeof(int) * ntrace, h->stream));
-    CK(h, pool_alloc(reinterpret_cast<void **>(&h->d_rid[kind]), sizeof(int) * ntrace, h->stream));
-    CK(h, cudaMemcpyAsync(h->d_rcol[kind], colptr.data(), sizeof(int) * (Nx + 1), cudaMemcpyHostToDevice, h->stream));
-    CK(h, cudaMemcpyAsync(h->d_rzs[kind], zs.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice, h->stream));
-    CK(h, cudaMemcpyAsync(h->d_rid[kind], ids.data(), sizeof(int) * ntrace, cudaMemcpyHostToDevice, h->stream));
-    CK(h, cudaStreamSynchronize(h->stream));  // the host vectors go out of scope
-  }
+  CK(h, cudaStreamSynchronize(h->stream));  // the host block goes out of scope
   h->nrec[kind] = ntrace;
   return TTI_OK;
 }

@@ -161,7 +161,7 @@ struct tti_handle {
   int *d_sx = nullptr, *d_sz = nullptr;
   float *d_src = nullptr;
   int nrec[3] = {0, 0, 0};
-  int *d_rx[3] = {}, *d_rz[3] = {};
+  int *d_rz[3] = {};  // receiver rows in the caller's order; owns the block d_rzs, d_rid, d_rcol point into
   float *d_rec[3] = {};
   int nts = 0;
   double *d_energy = nullptr;  // [nt][2]
