@@ -129,17 +129,21 @@ __device__ __forceinline__ void tma_load_2d(float *dst, const CUtensorMap *map, 
 static_assert((BZ * 4) % 16 == 0, "TMA inner box extent must be a multiple of 16 bytes");
 
 // Issues the TMA copies of the halo boxes of `n` fields (origin row z0 - 8,
-// column x0 - xoff); waited for by wait_tiles.
+// column x0 - xoff); waited for by wait_tiles. With ph < 0 the barrier is
+// initialised here (a CTA that loads one tile); with ph >= 0 it is a barrier
+// the CTA initialised once, whose phase ph these copies complete (a CTA that
+// loads tile after tile: an mbarrier must not be initialised again while it
+// is valid).
 __device__ __forceinline__ void issue_tiles(const CUtensorMap *map, float *sm, unsigned long long *bar, int n, int z0,
-                                            int x0, int xoff)
+                                            int x0, int xoff, int ph = -1)
 {
   constexpr unsigned BOX_BYTES = BX * BZ * 4;
   const int t = threadIdx.x;
-  if (t == 0) {
+  if (t == 0 && ph < 0) {
     mbar_init(bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  __syncthreads();
+  __syncthreads();  // also: every thread is done with the boxes these copies replace
   if (t == 0) {
     mbar_arrive_expect_tx(bar, n * BOX_BYTES);
     for (int f = 0; f < n; ++f) tma_load_2d(sm + f * FIELD, map + f, z0 - 8, x0 - xoff, bar);
@@ -147,13 +151,14 @@ __device__ __forceinline__ void issue_tiles(const CUtensorMap *map, float *sm, u
 }
 
 // returns false (all threads) after a timed-out wait
-__device__ __forceinline__ bool wait_tiles(int *err, unsigned long long *bar, unsigned limit = WAIT_LIMIT)
+__device__ __forceinline__ bool wait_tiles(int *err, unsigned long long *bar, unsigned limit = WAIT_LIMIT,
+                                           unsigned parity = 0)
 {
-  const bool ok = mbar_wait(bar, 0, limit);
+  const bool ok = mbar_wait(bar, parity, limit);
   if (__syncthreads_or(!ok)) {
     if (threadIdx.x == 0) {
       atomicOr(err, 4);
-      mbar_wait(bar, 0, 1u << 16);  // give the copies in flight a bounded time
+      mbar_wait(bar, parity, 1u << 16);  // give the copies in flight a bounded time
     }
     return false;
   }

@@ -142,20 +142,24 @@ __device__ __forceinline__ void velocity_store(const HalfArgs &a, size_t gi, con
   a.f.vz[gi] = A::add(A::mul(p.c1, p.vz0), A::mul(br, fz));
 }
 
-template <int V, bool X, bool Q, bool K = false>
-__device__ __forceinline__ void velocity_tile(const HalfArgs &a, const CUtensorMap *map, float *sm, int tz, int tx)
+// PB (a CTA that runs tile after tile): the boxes complete phase ph of the
+// CTA's barrier pbar, initialised once; otherwise the tile initialises its own
+// barrier after the boxes.
+template <int V, bool X, bool Q, bool K = false, bool PB = false>
+__device__ __forceinline__ void velocity_tile(const HalfArgs &a, const CUtensorMap *map, float *sm, int tz, int tx,
+                                              unsigned long long *pbar = nullptr, int ph = 0)
 {
   using A = Ar<X>;
-  unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm + 3 * FIELD);
+  unsigned long long *bar = PB ? pbar : reinterpret_cast<unsigned long long *>(sm + 3 * FIELD);
   const Grid &g = a.g;
   const Cells c = cells_of(a, tz, tx);
-  tma::issue_tiles(map, sm, bar, 3, c.z0, c.x0, 4);
+  tma::issue_tiles(map, sm, bar, 3, c.z0, c.x0, 4, PB ? ph : -1);
   const int L = g.ldz;
   const bool und = tile_undamped(a, c);
   const int z = c.zr;
   const bool zin = z >= g.izStart && z < g.Nz - NH;
   prefetch_cells<V == TTI_COORDINATE>(a, c, und);
-  if (!tma::wait_tiles(a.err, bar, a.wait_limit)) return;
+  if (!tma::wait_tiles(a.err, bar, a.wait_limit, PB ? (unsigned)ph : 0u)) return;
   if (!zin) return;
 #pragma unroll
   for (int i = 0; i < TX / 4; ++i) {
@@ -319,19 +323,20 @@ __device__ __forceinline__ void prefetch_scells(const HalfArgs &a, const Cells &
   }
 }
 
-template <int V, bool X, bool Q, bool K = false>
-__device__ __forceinline__ void stress_tile(const HalfArgs &a, const CUtensorMap *map, float *sm, int tz, int tx)
+template <int V, bool X, bool Q, bool K = false, bool PB = false>
+__device__ __forceinline__ void stress_tile(const HalfArgs &a, const CUtensorMap *map, float *sm, int tz, int tx,
+                                            unsigned long long *pbar = nullptr, int ph = 0)
 {
   using A = Ar<X>;
-  unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm + 2 * FIELD);
+  unsigned long long *bar = PB ? pbar : reinterpret_cast<unsigned long long *>(sm + 2 * FIELD);
   const Grid &g = a.g;
   const Cells c = cells_of(a, tz, tx);
-  tma::issue_tiles(map, sm, bar, 2, c.z0, c.x0, 5);
+  tma::issue_tiles(map, sm, bar, 2, c.z0, c.x0, 5, PB ? ph : -1);
   const bool und = tile_undamped(a, c);
   const int z = c.zr;
   const bool zin = z >= g.izStart && z < g.Nz - NH;
   prefetch_scells<V>(a, c, und);
-  if (!tma::wait_tiles(a.err, bar, a.wait_limit)) return;
+  if (!tma::wait_tiles(a.err, bar, a.wait_limit, PB ? (unsigned)ph : 0u)) return;
   if (!zin) return;
 #pragma unroll
   for (int i = 0; i < TX / 4; ++i) {
@@ -419,9 +424,16 @@ __global__ void __launch_bounds__(NT, 4) k_velocity_batch(const HalfArgs *__rest
                                                           const Work *__restrict__ work, int nwork, const int *step)
 {
   extern __shared__ __align__(128) float sm[];
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm + 3 * FIELD);
+  if (threadIdx.x == 0) {  // one barrier for all the CTA's tiles (ordered by stage_args' barrier)
+    tma::mbar_init(bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  int ph = 0;
   for_work(inst, work, nwork, step, [&](const HalfArgs *src, const Work &w) {
     const HalfArgs *a = stage_args(src, sm);
-    velocity_tile<V, X, Q>(*a, src->map, sm, w.tile % a->tiles_z, w.tile / a->tiles_z);
+    velocity_tile<V, X, Q, false, true>(*a, src->map, sm, w.tile % a->tiles_z, w.tile / a->tiles_z, bar, ph);
+    ph ^= 1;
   });
 }
 
@@ -430,9 +442,16 @@ __global__ void __launch_bounds__(NT, 4) k_stress_batch(const HalfArgs *__restri
                                                         const Work *__restrict__ work, int nwork, const int *step)
 {
   extern __shared__ __align__(128) float sm[];
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm + 2 * FIELD);
+  if (threadIdx.x == 0) {  // one barrier for all the CTA's tiles (ordered by stage_args' barrier)
+    tma::mbar_init(bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  int ph = 0;
   for_work(inst, work, nwork, step, [&](const HalfArgs *src, const Work &w) {
     const HalfArgs *a = stage_args(src, sm);
-    stress_tile<V, X, Q>(*a, src->map, sm, w.tile % a->tiles_z, w.tile / a->tiles_z);
+    stress_tile<V, X, Q, false, true>(*a, src->map, sm, w.tile % a->tiles_z, w.tile / a->tiles_z, bar, ph);
+    ph ^= 1;
   });
 }
 
