@@ -306,6 +306,9 @@ def run_ours(args, rank, world, local_rank):
             "warmup": W, "ms_per_step": p["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": workload_config(variant, world),
             "roofline": p["roofline"], "e2e": e2e, "gpu_launches": p["launches"], "clocks": p["clocks"]}
+    # the same rate over the physical grid (nz * nx, without the absorbing rims)
+    phys = WORKLOAD["nz"] * WORKLOAD["nx"] / p["cells"]
+    line["value_physical"] = p["value"] * phys
     if not args.no_variants:
         # the other two formulations on the same workload (BASELINE config: all three)
         line["variants"] = {}
@@ -315,6 +318,7 @@ def run_ours(args, rank, world, local_rank):
             q = measure_plain(v, K, W, args.profile_steps, rank, world, local_rank, clock_window_s=0.5)
             q["e2e"] = measure_e2e(v, K, rank, world, local_rank)
             q["config"] = workload_config(v, world)
+            q["value_physical"] = q["value"] * phys
             line["variants"][v] = q
     return line
 
