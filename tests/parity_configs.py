@@ -180,16 +180,119 @@ def run_config(name, nt=None, variants=None, threads=None, log=print):
     return out
 
 
+BATCHED = ("config2", "config4")
+
+
+def batched_setup(name, nt=None):
+    """The instances of a batched configuration: (list of batch model configs,
+    model_of, per model: the physical model, per instance: (model, sx, sz,
+    nt, receiver x positions))."""
+    if name == "config2":
+        # 64 shots 120 m apart on the nx=3000 crop (columns 2436..5435) of config 1's model
+        nt = nt or 4000
+        m = synthetic.crop(synthetic.salt_model(1126, 7872, seed=1), 2436, 3000)
+        cfg = dict(variant="coordinate_rotation", nz=1126, nx=3000, nt=nt, dx=10.0, dz=10.0, dt=0.0008, fpeak=10.0,
+                   ealThick=50, freesurface=1, stype=1, seistype=1, mt=1)
+        inst = [(0, 1122 + 12 * i, 2, nt, np.arange(3000)) for i in range(64)]
+        return [cfg], [0] * 64, [m], inst
+    # config4: 48 layered models of seeded sizes, one centred shot each (as bench.py's uneven batch)
+    rng = np.random.default_rng(4)
+    sizes = [(int(rng.integers(256, 1127)), int(rng.integers(256, 4097)), int(rng.integers(1000, 4001)))
+             for _ in range(48)]
+    cfgs = [dict(variant="coordinate_rotation", nz=nz, nx=nx, nt=nt or t, dx=10.0, dz=10.0, dt=0.0008, fpeak=15.0,
+                 ealThick=40, freesurface=0, stype=1, seistype=1, mt=1) for nz, nx, t in sizes]
+    models = [synthetic.layered_model(nz, nx, seed=100 + k) for k, (nz, nx, _) in enumerate(sizes)]
+    inst = [(k, c["nx"] // 2, 2, c["nt"], np.arange(c["nx"])) for k, c in enumerate(cfgs)]
+    return cfgs, list(range(48)), models, inst
+
+
+def run_batched(name, pick=None, nt=None, threads=None, log=print):
+    """Every instance of a batched configuration in one batch on the GPU
+    (ttifd.Batch: one launch per half-step for all of them), against the
+    reference program run alone for the instances `pick` (default: config2
+    shots 0, 31, 63; config4 the three smallest models); vx and vz traces
+    compared with the bounds of the plain runs."""
+    import ttifd
+
+    cfgs, model_of, models, inst = batched_setup(name, nt)
+    if pick is None:
+        pick = [0, 31, 63] if name == "config2" else sorted(
+            range(len(inst)), key=lambda i: cfgs[model_of[i]]["nz"] * cfgs[model_of[i]]["nx"])[:3]
+    t0 = time.perf_counter()
+    ours = {}
+    with ttifd.Batch(cfgs, model_of) as b:
+        for k, m in enumerate(models):
+            b.upload_model(k, *synthetic.padded(m, cfgs[k]["ealThick"]))
+        for i, (k, sx, sz, t, gx) in enumerate(inst):
+            c = cfgs[k]
+            h = b.instances[i]
+            h.set_source([sx], [sz], synthetic.ricker(t, c["dt"], c["fpeak"])[None, :])
+            for comp in (0, 1):
+                h.set_receivers(comp, gx, 2)
+        b.run()
+        for i in pick:
+            ours[i] = [b.instances[i].fetch_traces(comp) for comp in (0, 1)]
+    ours_wall = time.perf_counter() - t0
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads or os.cpu_count() or 1), OMP_PROC_BIND="close",
+               OMP_PLACES="cores", SUSHIM_QUIET="1")
+    out = []
+    for i in pick:
+        k, sx, sz, t, gx = inst[i]
+        c = cfgs[k]
+        work = tempfile.mkdtemp(prefix=f"parity_{name}_{i}_")
+        try:
+            files = synthetic.write_model(work, models[k])
+            synthetic.write_su_source(os.path.join(work, "src.su"), synthetic.ricker(t, c["dt"], c["fpeak"])[None, :],
+                                      [sx], [sz], c["dt"])
+            synthetic.write_su_receivers(os.path.join(work, "rec.su"), gx, np.full(gx.size, 2))
+            p = dict(nz=c["nz"], nx=c["nx"], nt=t, dx=c["dx"], dz=c["dz"], dt=c["dt"], fpeak=c["fpeak"],
+                     ealThick=c["ealThick"], freesurface=c["freesurface"], stype=1, seistype=1, mt=1, wsave=0,
+                     savew=0, shotID=1, snap_sample=1)
+            args = [f"{a}={v}" for a, v in p.items()]
+            args += [f"{a}file={files[a]}" for a in ("vp", "vs", "rho", "epsilon", "delta", "theta")]
+            args += [f"sourcefile={work}/src.su", f"recposfile={work}/rec.su", "trace_prefix=traces"]
+            r = subprocess.run([os.path.join(REF, "sufdmod2dTTIelastic_coordinate_rotation")] + args, cwd=work,
+                               env=env, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"reference instance {i} failed ({r.returncode}): {r.stderr[-800:]}")
+            rec = {"config": name, "instance": i, "nz": c["nz"], "nx": c["nx"], "nt": t, "sx": sx, "files": []}
+            for line in r.stdout.splitlines():
+                if "Finite difference modeling takes" in line:
+                    rec["reference_loop_s"] = float(line.split("takes")[1].split()[0])
+            for comp, tag in ((0, "vx"), (1, "vz")):
+                fn = [f for f in os.listdir(work) if f.startswith(f"traces_{tag}_") and f.endswith(".su")]
+                _, dr = _su(os.path.join(work, fn[0]))
+                do = ours[i][comp]
+                rel, mx = _metrics(do, dr) if do.shape == dr.shape else (np.inf, np.inf)
+                rec["files"].append({"file": fn[0], "kind": "traces", "rel_l2": rel, "max_over_peak": mx,
+                                     "ok": rel <= TRACE_RTOL and mx <= TRACE_PEAK})
+            rec["ok"] = all(f["ok"] for f in rec["files"])
+            out.append(rec)
+            log(f"{name} instance {i} ({c['nz']}x{c['nx']}, nt {t}, sx {sx}): {'ok' if rec['ok'] else 'FAIL'}; "
+                f"worst rel-L2 {max(f['rel_l2'] for f in rec['files']):.2e}; reference loop "
+                f"{rec.get('reference_loop_s')} s")
+        finally:
+            shutil.rmtree(work, ignore_errors=True)
+    for rec in out:
+        rec["batch_wall_s"] = ours_wall  # the whole batch, every instance, upload to fetch
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("config", choices=sorted(CONFIGS))
+    ap.add_argument("config", choices=sorted(CONFIGS) + list(BATCHED))
     ap.add_argument("--nt", type=int, default=None)
     ap.add_argument("--variants", nargs="*", default=None)
+    ap.add_argument("--instances", type=int, nargs="*", default=None, help="batched configs: instances to check")
     ap.add_argument("--json", default=None)
     a = ap.parse_args()
     if not available():
         sys.exit("build oracle/_ref (make -C oracle REF=...) and the drop-in programs first")
-    recs = run_config(a.config, nt=a.nt, variants=a.variants, log=lambda *x: print(*x, file=sys.stderr, flush=True))
+    lg = lambda *x: print(*x, file=sys.stderr, flush=True)  # noqa: E731
+    if a.config in BATCHED:
+        recs = run_batched(a.config, pick=a.instances, nt=a.nt, log=lg)
+    else:
+        recs = run_config(a.config, nt=a.nt, variants=a.variants, log=lg)
     s = json.dumps({"cores": os.cpu_count(), "runs": recs}, indent=1)
     if a.json:
         open(a.json, "w").write(s)

@@ -1,12 +1,17 @@
-"""Parity at the benchmark configurations with the default (FMA) arithmetic,
-after the full number of steps: traces and snapshots within rel-L2 <= 1e-5
-and max |diff| <= 1e-4 of the peak, SU headers byte-identical.
+"""Parity at the benchmark configurations with the default arithmetic, after
+the full number of steps: traces and snapshots within rel-L2 <= 1e-5 and
+max |diff| <= 1e-4 of the peak, SU headers byte-identical.
 
 * program against program (tests/parity_configs.py): the reference's own
   OpenMP build and this library's drop-in programs on the same files, config0
   in full (nt=1501, both runs) and config1 (1126 x 7872, all three
   formulations) over its first 301 steps. The full config1 (nt=5001) runs
   through the same script; its record is kept with the profiles.
+* batched against the reference program: the 64-shot batch of config2 and
+  the 48-model uneven batch of config4 in one batch each on the GPU, over
+  their first 301 steps, with two instances of each run alone through the
+  reference build. The full-length record (nt 4000 and 1000-4000) is kept
+  with the profiles.
 * library against the CPU restatement (the oracle, itself bit-identical to the
   reference build on every golden case): config0's second run through the C
   ABI, so the check stands where the reference build is not at hand.
@@ -77,3 +82,12 @@ def test_config0_library_against_restatement(gpu_lib, monkeypatch):
     for a, b in [(tg, to)] + [(sg[k], so[k]) for k in (750, 1500)]:
         rel, mx = parity_configs._metrics(a, b)
         assert rel <= parity_configs.TRACE_RTOL and mx <= parity_configs.TRACE_PEAK, (rel, mx)
+
+
+@need_programs
+@pytest.mark.parametrize("name,pick", [("config2", [0, 63]), ("config4", [5, 17])])
+def test_batched_configs_first_steps(name, pick, gpu_lib):
+    recs = parity_configs.run_batched(name, pick=pick, nt=301)
+    assert [r["instance"] for r in recs] == pick
+    for r in recs:
+        assert r["ok"], r
