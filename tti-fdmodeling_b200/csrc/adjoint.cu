@@ -655,20 +655,33 @@ __global__ void __launch_bounds__(tiled::NT, 3) k_adj_velocity_tiled(const __gri
     const int x = c.xc + j;
     if (x >= g.Nx - NH) break;
     const size_t i = (size_t)x * g.ldz + z;
-    const float *q = sm + (x - c.x0 + 4) * B + (z - c.z0 + 8);
-    const float lx = l[j][0] - (vdiag1(q) + vdiag2(q + F));
-    const float lz = l[j][1] - (vdiag1(q + 2 * F) + vdiag2(q + 3 * F));
+    // the cell's inputs are requested before its stencil (the kept fields are
+    // read-only here, so their loads need not wait behind the previous
+    // column's stores)
     const float2 cf = cell_undamped(a, x, z) ? make_float2(1.0f, a.dt) : __ldg(at.pk.cf + i);
-    const float br = cf.y * __ldg(a.p.invrho + i);
-    const float Fx = br * lx, Fz = br * lz;
+    const float ir = __ldg(a.p.invrho + i);
     float sv = 0.0f, cv = 1.0f;  // tensor and Bond: fx = sxx_x + sxz_z, fz = sxz_x + szz_z
+    float kp = 0.0f, kq = 0.0f, kr = 0.0f, ks = 0.0f, a5 = 0.0f, a6 = 0.0f;
     if (V == TTI_COORDINATE) {
       const float2 vsc = __ldg(at.pk.vsc + i);
       sv = vsc.x;
       cv = vsc.y;
+      kp = __ldg(a.keep[4] + i);
+      kq = __ldg(a.keep[5] + i);
+      kr = __ldg(a.keep[6] + i);
+      ks = __ldg(a.keep[7] + i);
+      a5 = a.acc[5][i];
+      a6 = a.acc[6][i];
+    }
+    const float *q = sm + (x - c.x0 + 4) * B + (z - c.z0 + 8);
+    const float lx = l[j][0] - (vdiag1(q) + vdiag2(q + F));
+    const float lz = l[j][1] - (vdiag1(q + 2 * F) + vdiag2(q + 3 * F));
+    const float br = cf.y * ir;
+    const float Fx = br * lx, Fz = br * lz;
+    if (V == TTI_COORDINATE) {
       // P = sxz_x - sxx_z, Q = szz_x - sxz_z, R = sxx_x + sxz_z, S = sxz_x + szz_z
-      a.acc[5][i] += Fx * a.keep[4][i] + Fz * a.keep[5][i];
-      a.acc[6][i] += Fx * a.keep[6][i] + Fz * a.keep[7][i];
+      a.acc[5][i] = a5 + (Fx * kp + Fz * kq);
+      a.acc[6][i] = a6 + (Fx * kr + Fz * ks);
     }
     const float Axx_x = cv * Fx, Axx_z = -sv * Fx;
     const float Axz_x = sv * Fx + cv * Fz, Axz_z = cv * Fx - sv * Fz;
