@@ -310,7 +310,7 @@ def run_ours(args, rank, world, local_rank):
     phys = WORKLOAD["nz"] * WORKLOAD["nx"] / p["cells"]
     line["value_physical"] = p["value"] * phys
     if not args.no_variants:
-        # the other two formulations on the same workload (BASELINE config: all three)
+        # the other two formulations on the same workload, so the line carries all three
         line["variants"] = {}
         for v in ALG_BYTES_STEP:
             if v == variant:

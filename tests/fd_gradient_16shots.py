@@ -1,4 +1,4 @@
-"""The device gradient of the gradient configuration at its full size against
+"""The device gradient of the 16-shot gradient workload at its full size against
 central finite differences of the device's own misfit (a record, like
 parity_configs.py; the -m gpu test test_gradient_fd_gpu.py does the same on a
 reduced grid).
@@ -23,7 +23,7 @@ At each parameter's worst centre the difference is then taken again with h
 halved, doubled and quadrupled: an error that falls as h grows is the FP32
 forward's rounding noise in J+ - J-, one that grows as h^2 is truncation.
 
-    python tests/fd_config3.py [--json out.json] [--nt 3000] [--centres 50]
+    python tests/fd_gradient_16shots.py [--json out.json] [--nt 3000] [--centres 50]
 """
 from __future__ import annotations
 

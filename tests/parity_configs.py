@@ -12,24 +12,29 @@ input files, and every output file is compared:
 Configurations (seeded synthetic inputs with the benchmark's shapes; the
 reference's demo files are not available):
 
-  config0   coordinate rotation, nz=200 nx=400 dx=dz=10 m, nt=1501, dt=0.8 ms,
-            5 flat layers (seed 0), vs = vp/1.8, rho = 310 vp^0.25, one 15 Hz
-            Ricker at (z=20, x=200), 400 receivers on z=5, ealThick=40, no free
-            surface. Two runs: seistype=1 (vx, vz); seistype=2 with wsave=2 and
-            snap_sample=750 (p snapshots at 0, 600 and 1200 ms).
-  config1   the three formulations on the salt-like 1126 x 7872 model (seed 1),
-            nt=5001, dt=0.8 ms, one 12 Hz Ricker at the surface centre (sdepth
-            2, sx 3936), 7872 receivers on z=2, ealThick=60, free surface,
-            seistype=3, wsave=2, snap_sample=1250 (p at 0, 1000, ..., 4000 ms).
+  layered_200x400
+      coordinate rotation, nz=200 nx=400 dx=dz=10 m, nt=1501, dt=0.8 ms, 5
+      flat layers (seed 0), vs = vp/1.8, rho = 310 vp^0.25, one 15 Hz Ricker
+      at (z=20, x=200), 400 receivers on z=5, ealThick=40, no free surface.
+      Two runs: seistype=1 (vx, vz); seistype=2 with wsave=2 and
+      snap_sample=750 (p snapshots at 0, 600 and 1200 ms).
+  salt_1126x7872
+      the three formulations on the salt-like 1126 x 7872 model (seed 1),
+      nt=5001, dt=0.8 ms, one 12 Hz Ricker at the surface centre (sdepth 2,
+      sx 3936), 7872 receivers on z=2, ealThick=60, free surface, seistype=3,
+      wsave=2, snap_sample=1250 (p at 0, 1000, ..., 4000 ms).
+  shots64_1126x3000, models48_uneven
+      batched (run_batched below): 64 shots on a 1126 x 3000 crop of the
+      salt-like model, and 48 layered models of seeded sizes.
 
 Usage (from the repository root, after `make -C oracle REF=...` built
 oracle/_ref and `make -C tti-fdmodeling_b200` the programs):
 
-    python tests/parity_configs.py config0 [--json out.json]
-    python tests/parity_configs.py config1 [--nt 5001] [--variants coordinate_rotation ...]
+    python tests/parity_configs.py layered_200x400 [--json out.json]
+    python tests/parity_configs.py salt_1126x7872 [--nt 5001] [--variants coordinate_rotation ...]
 
-The -m gpu tests call run_config at full size for config0 and with a short nt
-for config1.
+The -m gpu tests call run_config at full size for layered_200x400 and with a
+short nt for salt_1126x7872.
 """
 from __future__ import annotations
 
@@ -55,10 +60,10 @@ TRACE_RTOL, TRACE_PEAK = 1e-5, 1e-4
 DUMPS = ("D_", "Beta_", "coef1_", "coef2_", "invrho_", "c11_", "c13_", "c15_", "c33_", "c35_", "c55_")
 
 CONFIGS = {
-    "config0": dict(model=("layered", 200, 400, 0), nt=1501, dx=10, dz=10, dt=0.0008, fpeak=15, ealThick=40,
+    "layered_200x400": dict(model=("layered", 200, 400, 0), nt=1501, dx=10, dz=10, dt=0.0008, fpeak=15, ealThick=40,
                     freesurface=0, source=(200, 20), rec_z=5, variants=("coordinate_rotation",),
                     runs=[dict(seistype=1, wsave=0), dict(seistype=2, wsave=2, snap_sample=750)]),
-    "config1": dict(model=("salt", 1126, 7872, 1), nt=5001, dx=10, dz=10, dt=0.0008, fpeak=12, ealThick=60,
+    "salt_1126x7872": dict(model=("salt", 1126, 7872, 1), nt=5001, dx=10, dz=10, dt=0.0008, fpeak=12, ealThick=60,
                     freesurface=1, source=(3936, 2), rec_z=2, variants=VARIANTS,
                     runs=[dict(seistype=3, wsave=2, snap_sample=1250)]),
 }
@@ -180,22 +185,22 @@ def run_config(name, nt=None, variants=None, threads=None, log=print):
     return out
 
 
-BATCHED = ("config2", "config4")
+BATCHED = ("shots64_1126x3000", "models48_uneven")
 
 
 def batched_setup(name, nt=None):
     """The instances of a batched configuration: (list of batch model configs,
     model_of, per model: the physical model, per instance: (model, sx, sz,
     nt, receiver x positions))."""
-    if name == "config2":
-        # 64 shots 120 m apart on the nx=3000 crop (columns 2436..5435) of config 1's model
+    if name == "shots64_1126x3000":
+        # 64 shots 120 m apart on the nx=3000 crop (columns 2436..5435) of the salt-like 1126 x 7872 model
         nt = nt or 4000
         m = synthetic.crop(synthetic.salt_model(1126, 7872, seed=1), 2436, 3000)
         cfg = dict(variant="coordinate_rotation", nz=1126, nx=3000, nt=nt, dx=10.0, dz=10.0, dt=0.0008, fpeak=10.0,
                    ealThick=50, freesurface=1, stype=1, seistype=1, mt=1)
         inst = [(0, 1122 + 12 * i, 2, nt, np.arange(3000)) for i in range(64)]
         return [cfg], [0] * 64, [m], inst
-    # config4: 48 layered models of seeded sizes, one centred shot each (as bench.py's uneven batch)
+    # models48_uneven: 48 layered models of seeded sizes, one centred shot each (as bench.py's uneven batch)
     rng = np.random.default_rng(4)
     sizes = [(int(rng.integers(256, 1127)), int(rng.integers(256, 4097)), int(rng.integers(1000, 4001)))
              for _ in range(48)]
@@ -209,14 +214,14 @@ def batched_setup(name, nt=None):
 def run_batched(name, pick=None, nt=None, threads=None, log=print):
     """Every instance of a batched configuration in one batch on the GPU
     (ttifd.Batch: one launch per half-step for all of them), against the
-    reference program run alone for the instances `pick` (default: config2
-    shots 0, 31, 63; config4 the three smallest models); vx and vz traces
+    reference program run alone for the instances `pick` (default: shots64_1126x3000
+    shots 0, 31, 63; models48_uneven the three smallest models); vx and vz traces
     compared with the bounds of the plain runs."""
     import ttifd
 
     cfgs, model_of, models, inst = batched_setup(name, nt)
     if pick is None:
-        pick = [0, 31, 63] if name == "config2" else sorted(
+        pick = [0, 31, 63] if name == "shots64_1126x3000" else sorted(
             range(len(inst)), key=lambda i: cfgs[model_of[i]]["nz"] * cfgs[model_of[i]]["nx"])[:3]
     t0 = time.perf_counter()
     ours = {}
