@@ -235,8 +235,9 @@ SNAP_KINDS = {0: 0, 1: 2, 2: 1, 3: 3, 4: 2, 5: 2}  # wsave -> snapshot kinds per
 
 
 def measure_e2e(variant, K, rank, world, local_rank, reps=3):
-    """The whole public-API sequence from host buffers: create, upload +
-    device precompute, geometry, K steps with snapshots delivered to the host,
+    """The whole public-API sequence from host buffers: create, upload of the
+    physical model (tti_upload_model_physical: the rims are filled on the
+    device) + device precompute, geometry, K steps with snapshots delivered to the host,
     traces fetched, destroy (wall clock, max over ranks). The model, trace and
     snapshot buffers are page-locked host arrays (tti_host_alloc), allocated
     and filled once outside the timed region, as a service that models shot
@@ -246,9 +247,9 @@ def measure_e2e(variant, K, rank, world, local_rank, reps=3):
     import ttifd
 
     m = model()
-    pads = synthetic.padded(m, WORKLOAD["ealThick"])
-    pinned = [ttifd.host_empty(a.shape) for a in pads]
-    for d, a in zip(pinned, pads):
+    phys = m.arrays()  # the physical model; tti_upload_model_physical fills the rims on the device
+    pinned = [ttifd.host_empty(a.shape) for a in phys]
+    for d, a in zip(pinned, phys):
         d[...] = a
     sx, sz, gx, gz = geometry(rank)
     cfg_e = dict(WORKLOAD, variant=variant, nt=K)
@@ -266,7 +267,7 @@ def measure_e2e(variant, K, rank, world, local_rank, reps=3):
         t0 = time.perf_counter()
         with ttifd.Modeling(device=local_rank, **cfg_e) as he:
             phases["create"] = time.perf_counter() - t0
-            he.upload_model(*pinned)
+            he.upload_model_physical(*pinned)
             phases["upload"] = time.perf_counter() - t0 - sum(phases.values())
             he.set_source([sx], [sz], wav_e[None, :])
             for k in (0, 1, 2):
@@ -289,11 +290,12 @@ def measure_e2e(variant, K, rank, world, local_rank, reps=3):
     one()  # untimed: first use of the snapshot and transpose kernels in the process
     runs = sorted((one() for _ in range(reps)), key=lambda r: r[0])
     t_e2e, phases, cells, d2h = runs[len(runs) // 2]
-    h2d = sum(a.nbytes for a in pads) + wav_e.nbytes + 3 * 2 * gx.nbytes
+    h2d = sum(a.nbytes for a in phys) + wav_e.nbytes + 3 * 2 * gx.nbytes
     return {"value": cells * K * world / t_e2e / 1e9, "unit": "Gcell/s", "h2d_bytes_per_step": h2d / K,
             "d2h_bytes_per_step": d2h / K, "wall_s": t_e2e, "walls_s": [r[0] for r in runs], "phases_s": phases,
             "host_buffers": "page-locked (tti_host_alloc), allocated once outside the timed region",
-            "includes": "tti_create..tti_destroy: model upload + device precompute, geometry, K steps, "
+            "includes": "tti_create..tti_destroy: physical-model upload (rims padded on the device) + device "
+                        "precompute, geometry, K steps, "
                         "snapshots to host, traces; median of %d passes after one untimed pass" % reps}
 
 

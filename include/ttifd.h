@@ -135,6 +135,14 @@ int tti_grid(const tti_handle *h, int *Nz, int *Nx, int *E);
  * caller's, coord:362-415). */
 int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const float *rho, const float *epsilon,
                      const float *delta, const float *theta);
+/* The same from the physical model ([nx][nz], as the model files hold it,
+ * before padModel2d): the arrays cross the host link unpadded and the rims
+ * are filled on the device as padModel2d (padmod.c:33-59) fills them on the
+ * host, every rim cell taking the value of the nearest physical cell, so the
+ * result is tti_upload_model's on the padded arrays, bit for bit. On a
+ * 1126 x 7872 model it moves 12 % fewer bytes. */
+int tti_upload_model_physical(tti_handle *h, const float *vp, const float *vs, const float *rho,
+                              const float *epsilon, const float *delta, const float *theta);
 /* Copies one precomputed array ([Nx][Nz]) to host memory (setup dumps). */
 int tti_fetch_param(tti_handle *h, int which, float *out);
 

@@ -96,3 +96,54 @@ def test_snapshot_buffer_errors_and_abort(gpu_lib, pads):
         _shot(ttifd, pads, snapbuf=buf, abort_at=100)
     assert e.value.code == ttifd.ERR_CALLBACK
     assert "it=100" in str(e.value)
+
+
+@pytest.mark.parametrize("variant,fs", [("coordinate_rotation", 1), ("tensor_rotation", 0), ("bond_transformation", 1)])
+def test_physical_upload_matches_padded(gpu_lib, variant, fs):
+    """tti_upload_model_physical (unpadded arrays, rims filled on the device)
+    gives every precomputed parameter and every trace of tti_upload_model on
+    the host-padded arrays bit for bit, from pageable and from page-locked
+    arrays; a model whose edges vary along both axes, so every rim cell's
+    source cell matters."""
+    import ttifd
+
+    cfg = dict(CFG, variant=variant, freesurface=fs, nt=120, wsave=0)
+    m = synthetic.layered_model(cfg["nz"], cfg["nx"], seed=9)
+    m.theta[...] += np.linspace(-7.0, 9.0, cfg["nx"], dtype=np.float32)[:, None]  # varies along x too
+    phys = [np.array(a, np.float32) for a in m.arrays()]
+    pads = [np.array(a, np.float32) for a in synthetic.padded(m, cfg["ealThick"])]
+    pinned = [ttifd.host_empty(a.shape) for a in phys]
+    for d, a in zip(pinned, phys):
+        d[...] = a
+    w = synthetic.ricker(cfg["nt"], cfg["dt"], cfg["fpeak"])[None, :]
+    gx = np.arange(cfg["nx"], dtype=np.int32)
+
+    def shot(upload):
+        with ttifd.Modeling(**cfg) as h:
+            upload(h)
+            params = {}
+            for name in ttifd.PARAMS:
+                try:
+                    params[name] = h.fetch_param(name)
+                except ttifd.TTIError:
+                    pass  # not used by this formulation
+            h.set_source([45], [3], w)
+            for k in (0, 1, 2):
+                h.set_receivers(k, gx, 2)
+            h.run()
+            return params, [h.fetch_traces(k).copy() for k in (0, 1, 2)]
+
+    ref_par, ref_tr = shot(lambda h: h.upload_model(*pads))
+    assert {"vp", "coef1", "invrho", "c11"} <= set(ref_par)
+    for arrays in (phys, pinned):
+        par, tr = shot(lambda h: h.upload_model_physical(*arrays))
+        assert sorted(par) == sorted(ref_par)
+        for name in ref_par:
+            assert np.array_equal(par[name], ref_par[name]), name
+        for a, b in zip(tr, ref_tr):
+            assert np.array_equal(a, b)
+    with ttifd.Modeling(**cfg) as h:
+        with pytest.raises(ValueError):
+            h.upload_model_physical(*pads)  # padded arrays where physical ones are due
+        null = ttifd.load().tti_upload_model_physical(h._h, None, None, None, None, None, None)
+        assert null == ttifd.ERR_ARG

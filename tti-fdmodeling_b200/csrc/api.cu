@@ -406,20 +406,23 @@ int check_flag(tti_handle *h)
 // block c into one chunk while the DMA engine moves block c - 1 from the other
 // (TTIFD_UPLOAD=pageable: straight from the caller's pageable arrays, which
 // the driver stages itself, about 10.5 GB/s on B200 hosts).
-int upload_arrays(tti_handle *h, const float *const *src, float *const *dst, int na)
+// `na` dense host arrays of `ncol` columns of `sl` floats each into dense
+// device arrays (the padded model: Nx columns of Nz; the physical one: nx of nz).
+int upload_arrays(tti_handle *h, const float *const *src, float *const *dst, int na, int sl, int ncol)
 {
-  const Grid &g = h->g;
-  const size_t col = (size_t)g.Nz * sizeof(float);
+  const size_t col = (size_t)sl * sizeof(float);
+  auto copy = [&](int k, int x0, const float *from, int nx) {
+    return cudaMemcpyAsync(dst[k] + (size_t)x0 * sl, from, col * nx, cudaMemcpyHostToDevice, h->stream);
+  };
   bool pinned = true;  // all from page-locked memory: straight to the device
   for (int k = 0; k < na; ++k) pinned = pinned && is_pinned(src[k]);
   if (pinned) {
-    for (int k = 0; k < na; ++k)
-      CK(h, cudaMemcpyAsync(dst[k], src[k], col * g.Nx, cudaMemcpyHostToDevice, h->stream));
+    for (int k = 0; k < na; ++k) CK(h, copy(k, 0, src[k], ncol));
     return TTI_OK;
   }
   const char *mode = getenv("TTIFD_UPLOAD");
   const bool pageable = mode && strcmp(mode, "pageable") == 0;
-  const int per = (int)std::min<size_t>(g.Nx, PIN_CHUNK / g.Nz);  // columns per chunk
+  const int per = (int)std::min<size_t>(ncol, PIN_CHUNK / sl);  // columns per chunk
   float *pin[2] = {nullptr, nullptr};
   if (!pageable && per > 0) {
     pin[0] = pinned_chunk();
@@ -431,20 +434,19 @@ int upload_arrays(tti_handle *h, const float *const *src, float *const *dst, int
   if (!pin[0] || !pin[1]) {
     pinned_release(pin[0]);
     pinned_release(pin[1]);
-    for (int k = 0; k < na; ++k)
-      CK(h, cudaMemcpyAsync(dst[k], src[k], col * g.Nx, cudaMemcpyHostToDevice, h->stream));
+    for (int k = 0; k < na; ++k) CK(h, copy(k, 0, src[k], ncol));
     return TTI_OK;
   }
   cudaError_t e = cudaSuccess;
   bool pending[2] = {false, false};
   int c = 0;
   for (int k = 0; k < na && e == cudaSuccess; ++k)
-    for (int x0 = 0; x0 < g.Nx && e == cudaSuccess; x0 += per, ++c) {
-      const int nx = std::min(per, g.Nx - x0), b = c & 1;
+    for (int x0 = 0; x0 < ncol && e == cudaSuccess; x0 += per, ++c) {
+      const int nx = std::min(per, ncol - x0), b = c & 1;
       if (pending[b]) e = cudaEventSynchronize(h->pev[5 + b]);  // chunk b's previous DMA has drained
       if (e != cudaSuccess) break;
-      parallel_copy(pin[b], src[k] + (size_t)x0 * g.Nz, col * nx, 8);
-      e = cudaMemcpyAsync(dst[k] + (size_t)x0 * g.Nz, pin[b], col * nx, cudaMemcpyHostToDevice, h->stream);
+      parallel_copy(pin[b], src[k] + (size_t)x0 * sl, col * nx, 8);
+      e = copy(k, x0, pin[b], nx);
       if (e == cudaSuccess) e = cudaEventRecord(h->pev[5 + b], h->stream);
       pending[b] = true;
     }
@@ -675,30 +677,47 @@ int tti_grid(const tti_handle *h, int *Nz, int *Nx, int *E)
   return TTI_OK;
 }
 
-int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const float *rho, const float *epsilon,
-                     const float *delta, const float *theta)
+// tti_upload_model (padded arrays) and tti_upload_model_physical (physical
+// arrays, the rims filled on the device) from here on are one path.
+static int upload_model(tti_handle *h, const float *const *src, bool physical)
 {
-  if (!h || !vp || !vs || !rho || !epsilon || !delta || !theta) return set_err(h, TTI_ERR_ARG, "null model array");
+  for (int k = 0; k < 6; ++k)
+    if (!src[k]) return set_err(h, TTI_ERR_ARG, "null model array");
   if (h->owner) return set_err(h, TTI_ERR_STATE, "this handle shares the parameters of another; upload through it");
   CK(h, cudaSetDevice(h->device));
   const tti_config &c = h->cfg;
   const Grid &g = h->g;
   const size_t np = (size_t)g.Nz * g.Nx;
-  // Stability check on the unscaled padded vp (stable.c:217-246). Its host
-  // maximum runs on other threads while the arrays travel to the device;
-  // nothing is computed from them on the device before it has passed.
-  auto vmax_f = std::async(std::launch::async, [vp, np] { return host_max(vp, np, FLT_MIN); });
-  // raw model on the device (dense [Nx][Nz], one block of six arrays), freed after the precompute
-  float *raw[6] = {};
-  const float *src[6] = {vp, vs, rho, epsilon, delta, theta};
+  // Stability check on the unscaled padded vp (stable.c:217-246; the rims
+  // repeat physical values, so the physical maximum is the padded one). Its
+  // host maximum runs on other threads while the arrays travel to the
+  // device; nothing is computed from them on the device before it has passed.
+  const float *vp = src[0];
+  const size_t nv = physical ? (size_t)c.nz * c.nx : np;
+  auto vmax_f = std::async(std::launch::async, [vp, nv] { return host_max(vp, nv, FLT_MIN); });
+  // raw model on the device (dense [Nx][Nz], one block of six arrays), freed
+  // after the precompute; a physical model first lands densely after it (one
+  // contiguous copy per array: a pitched copy into the padded layout ran
+  // slower than the padded bytes it saves) and is expanded on the device
+  float *raw[6] = {}, *phys[6] = {};
   float *d_w = nullptr, *raw_block = nullptr;
   int rc = TTI_OK;
   {
-    cudaError_t e = pool_alloc(reinterpret_cast<void **>(&raw_block), 6 * np * sizeof(float), h->stream);
+    const size_t extra = physical ? 6 * nv : 0;
+    cudaError_t e = pool_alloc(reinterpret_cast<void **>(&raw_block), (6 * np + extra) * sizeof(float), h->stream);
     if (e != cudaSuccess) rc = set_err(h, TTI_ERR_NOMEM, "device allocation failed: %s", cudaGetErrorString(e));
   }
-  for (int k = 0; k < 6; ++k) raw[k] = raw_block + (size_t)k * np;
-  if (rc == TTI_OK) rc = upload_arrays(h, src, raw, 6);
+  for (int k = 0; k < 6; ++k) {
+    raw[k] = raw_block + (size_t)k * np;
+    phys[k] = raw_block + 6 * np + (size_t)k * nv;
+  }
+  if (rc == TTI_OK)
+    rc = physical ? upload_arrays(h, src, phys, 6, c.nz, c.nx)
+                  : upload_arrays(h, src, raw, 6, g.Nz, g.Nx);
+  if (rc == TTI_OK && physical) {
+    launch_expand_physical(phys[0], raw_block, 6, c.nz, c.nx, g.E, h->stream);
+    if (cudaGetLastError() != cudaSuccess) rc = set_err(h, TTI_ERR_CUDA, "model expansion kernel failed to launch");
+  }
   {
     const double vmax = vmax_f.get();
     const double csum = (double)rsg(0) + (double)rsg(2) + (double)rsg(4);
@@ -788,6 +807,22 @@ int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const floa
   }
   if (rc == TTI_OK) h->have_model = true;
   return rc;
+}
+
+int tti_upload_model(tti_handle *h, const float *vp, const float *vs, const float *rho, const float *epsilon,
+                     const float *delta, const float *theta)
+{
+  if (!h) return set_err(h, TTI_ERR_ARG, "null handle");
+  const float *src[6] = {vp, vs, rho, epsilon, delta, theta};
+  return upload_model(h, src, false);
+}
+
+int tti_upload_model_physical(tti_handle *h, const float *vp, const float *vs, const float *rho,
+                              const float *epsilon, const float *delta, const float *theta)
+{
+  if (!h) return set_err(h, TTI_ERR_ARG, "null handle");
+  const float *src[6] = {vp, vs, rho, epsilon, delta, theta};
+  return upload_model(h, src, true);
 }
 
 int tti_fetch_param(tti_handle *h, int which, float *out)

@@ -27,6 +27,10 @@ struct MealConst {
 };
 void launch_setup(const Grid &g, const SetupIn &in, const SetupOut &out, const MealConst &mc, int variant,
                   float scalar, int freesurface, cudaStream_t st);
+// Expands `na` dense physical [nx][nz] arrays (nz * nx floats apart) into
+// dense padded [Nx][Nz] arrays (Nz * Nx floats apart), the E-wide rims filled
+// as padModel2d fills them on the host.
+void launch_expand_physical(const float *phys, float *pad, int na, int nz, int nx, int E, cudaStream_t st);
 
 // ---------------- per-step ----------------
 // Source weight tables over the 11 x 11 window (offset (a, b) at a*11+b,

@@ -168,6 +168,23 @@ __global__ void k_setup_average(Grid g, const float *__restrict__ rho, const flo
   }
 }
 
+// `na` dense physical [nx][nz] arrays (phys, nz * nx floats apart) into dense
+// padded [Nx][Nz] arrays (pad, Nz * Nx floats apart, Nz = nz + 2E), as
+// padModel2d (padmod.c:33-59) pads them on the host: its first pass copies
+// row E (Nz - E - 1) up (down) in every physical column, its second copies
+// column E (Nx - E - 1) left (right) at full height, so every rim cell holds
+// the value of the physical cell at its clamped column and row.
+__global__ void k_expand_physical(const float *phys, float *pad, int na, int nz, int nx, int E)
+{
+  const int Nz = nz + 2 * E, Nx = nx + 2 * E;
+  const int iz = blockIdx.x * blockDim.x + threadIdx.x, ix = blockIdx.y;
+  if (iz >= Nz || ix >= Nx) return;
+  const int sx = min(max(ix - E, 0), nx - 1), sz = min(max(iz - E, 0), nz - 1);
+  const size_t np = (size_t)Nz * Nx, nq = (size_t)nz * nx;
+  const size_t d = (size_t)ix * Nz + iz, s = (size_t)sx * nz + sz;
+  for (int k = 0; k < na; ++k) pad[k * np + d] = phys[k * nq + s];
+}
+
 }  // namespace
 
 void launch_setup(const Grid &g, const SetupIn &in, const SetupOut &out, const MealConst &mc, int variant,
@@ -176,6 +193,12 @@ void launch_setup(const Grid &g, const SetupIn &in, const SetupOut &out, const M
   dim3 blk(128), grd((g.Nz + 127) / 128, g.Nx);
   k_setup_cell<<<grd, blk, 0, st>>>(g, in, out, mc, variant, scalar, freesurface);
   k_setup_average<<<grd, blk, 0, st>>>(g, out.rho, out.sn, out.cs, out.invrho, out.snv, out.csv);
+}
+
+void launch_expand_physical(const float *phys, float *pad, int na, int nz, int nx, int E, cudaStream_t st)
+{
+  const int Nz = nz + 2 * E, Nx = nx + 2 * E;
+  k_expand_physical<<<dim3((Nz + 127) / 128, Nx), 128, 0, st>>>(phys, pad, na, nz, nx, E);
 }
 
 }  // namespace ttifd

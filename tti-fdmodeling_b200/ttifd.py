@@ -87,6 +87,7 @@ _SIGNATURES = {
     "last_error": (C.c_char_p, [C.c_void_p]),
     "grid": (C.c_int, [C.c_void_p, _IP, _IP, _IP]),
     "upload_model": (C.c_int, [C.c_void_p] + [_FP] * 6),
+    "upload_model_physical": (C.c_int, [C.c_void_p] + [_FP] * 6),
     "fetch_param": (C.c_int, [C.c_void_p, C.c_int, _FP]),
     "set_source": (C.c_int, [C.c_void_p, C.c_int, _IP, _IP, _FP]),
     "set_receivers": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _IP, _IP]),
@@ -240,6 +241,16 @@ class Modeling:
             if a.shape != (self.Nx, self.Nz):
                 raise ValueError(f"model arrays must be padded (Nx, Nz) = {(self.Nx, self.Nz)}, got {a.shape}")
         self._call("upload_model", self._h, *[_f(a) for a in arrs])
+
+    def upload_model_physical(self, vp, vs, rho, epsilon, delta, theta):
+        """The unpadded model, (nx, nz) arrays; the rims are filled on the
+        device as padModel2d fills them (tti_upload_model_physical)."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (vp, vs, rho, epsilon, delta, theta)]
+        want = (self.cfg.nx, self.cfg.nz)
+        for a in arrs:
+            if a.shape != want:
+                raise ValueError(f"model arrays must be physical (nx, nz) = {want}, got {a.shape}")
+        self._call("upload_model_physical", self._h, *[_f(a) for a in arrs])
 
     def fetch_param(self, name) -> np.ndarray:
         out = np.empty((self.Nx, self.Nz), np.float32)
